@@ -1,0 +1,329 @@
+"""TEST INFRASTRUCTURE ONLY: ctypes bindings of the CPU oracle.
+
+See ``oracle/__init__.py``.  Each wrapper names the reference function it
+stands for; the C side (``vcbct_oracle.c`` / ``ref_driver.cpp``) cites the
+reference file and line of every step.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+import threading
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_LOCK = threading.Lock()
+_LIBS: dict[str, C.CDLL] = {}
+
+TIES_GPU = 0
+TIES_CPU = 1
+
+_dp = C.POINTER(C.c_double)
+_fp = C.POINTER(C.c_float)
+_ip = C.POINTER(C.c_int)
+_i64p = C.POINTER(C.c_int64)
+_u16p = C.POINTER(C.c_uint16)
+
+
+class OrcProjGeom(C.Structure):
+    _fields_ = [("N", C.c_int), ("Z", C.c_int), ("s", C.c_double), ("step", C.c_double),
+                ("W", C.c_int), ("H", C.c_int), ("V", C.c_int),
+                ("pdet", C.c_double), ("piso", C.c_double), ("sad", C.c_double),
+                ("dpn", C.c_double), ("x_reg", C.c_double), ("y_reg", C.c_double),
+                ("z_reg", C.c_double), ("nmat", C.c_int)]
+
+
+class OrcFdkConsts(C.Structure):
+    _fields_ = [("mpn", C.c_double), ("pdet", C.c_double), ("sad", C.c_double),
+                ("piso", C.c_double), ("cutoff", C.c_double), ("gamma_", C.c_double),
+                ("alpha", C.c_double)]
+
+
+def _ptr(a, t):
+    if a is None:
+        return None
+    return a.ctypes.data_as(t)
+
+
+def _load(name: str) -> C.CDLL:
+    with _LOCK:
+        if name in _LIBS:
+            return _LIBS[name]
+        path = os.path.join(HERE, name)
+        if not os.path.exists(path):
+            subprocess.run(["make", "-s", "-C", HERE], check=False)
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"oracle library {path} is not built")
+        lib = C.CDLL(path, mode=C.RTLD_LOCAL)
+        _LIBS[name] = lib
+        return lib
+
+
+def have_reference() -> bool:
+    """True when the reference's own CPU code (oracle/_ref) is built."""
+    return all(os.path.exists(os.path.join(HERE, "_ref", n))
+               for n in ("libref_proj.so", "libref_fdk.so"))
+
+
+def lib():
+    return _load("liboracle.so")
+
+
+# ----------------------------------------------------------------- geometry --
+
+def proj_geom(g) -> OrcProjGeom:
+    """Build the C struct from any object with the projector geometry fields."""
+    return OrcProjGeom(g.N, g.Z, g.s, g.step, g.W, g.H, g.V, g.pdet, g.piso, g.sad,
+                       g.dpn, g.x_reg, g.y_reg, g.z_reg, g.nmat)
+
+
+def trig_tables(W, H, angles_rad, xshift, yshift, pdet, dpn):
+    """P/misc.cpp:10-37 prepareTrigonometricTable (restated)."""
+    V = len(angles_rad)
+    a = np.ascontiguousarray(angles_rad, np.float64)
+    xs = np.ascontiguousarray(xshift, np.float64)
+    ys = np.ascontiguousarray(yshift, np.float64)
+    out = [np.zeros(V, np.float64) for _ in range(4)]
+    L = lib()
+    L.orc_trig_tables.restype = None
+    L.orc_trig_tables(C.c_int(W), C.c_int(H), C.c_int(V), _ptr(a, _dp), _ptr(xs, _dp),
+                      _ptr(ys, _dp), C.c_double(pdet), C.c_double(dpn),
+                      *[_ptr(o, _dp) for o in out])
+    return tuple(out)
+
+
+# -------------------------------------------------------------------- MBFPA --
+
+def mbfpa_forward(g, tables, vol, mu, pdf, xfactor, views=None, rows=None, cols=None,
+                  ties=TIES_GPU, with_leng=True, flip=True, exact=True, volf=None,
+                  want=("f",)):
+    """Restated reprojectionKernel + host energy loop (P/reprojectionOnGPU.cu:56-1056).
+
+    vol: uint16 [Z][nmat][N][N]; volf (float32, same layout) replaces it.
+    mu: float32 [nmat][NE]; pdf: float32 [NE].
+    want: any of "f" (float-summed reference output), "d" (FP64), "L" (per
+    element path integrals), "nb"/"nm" (segment counts).  Returns a dict.
+    """
+    gc = proj_geom(g)
+    V, H, W = g.V, g.H, g.W
+    cosT, sinT, Xc, Yc = [np.ascontiguousarray(t, np.float64) for t in tables]
+    views = np.arange(V, dtype=np.int32) if views is None else np.ascontiguousarray(views, np.int32)
+    j0, j1 = (0, H) if rows is None else rows
+    c0, c1 = (0, W) if cols is None else cols
+    mu = np.ascontiguousarray(mu, np.float32)
+    pdf = np.ascontiguousarray(pdf, np.float32)
+    NE = int(pdf.shape[0])
+    res = {}
+    if "f" in want:
+        res["f"] = np.zeros((V, H, W), np.float32)
+    if "d" in want:
+        res["d"] = np.zeros((V, H, W), np.float64)
+    if "L" in want:
+        res["L"] = np.zeros((V, H, W, g.nmat), np.float64)
+    if "nb" in want:
+        res["nb"] = np.zeros((V, H, W), np.int64)
+    if "nm" in want:
+        res["nm"] = np.zeros((V, H, W), np.int64)
+    vol_p = None if vol is None else _ptr(np.ascontiguousarray(vol, np.uint16), _u16p)
+    volf_c = None if volf is None else np.ascontiguousarray(volf, np.float32)
+    L = lib()
+    L.orc_mbfpa_forward.restype = C.c_int
+    rc = L.orc_mbfpa_forward(
+        C.byref(gc), _ptr(cosT, _dp), _ptr(sinT, _dp), _ptr(Xc, _dp), _ptr(Yc, _dp),
+        vol_p, _ptr(volf_c, _fp), _ptr(mu, _fp), _ptr(pdf, _fp), C.c_int(NE),
+        C.c_double(xfactor), _ptr(views, _ip), C.c_int(len(views)),
+        C.c_int(j0), C.c_int(j1), C.c_int(c0), C.c_int(c1), C.c_int(ties),
+        C.c_int(int(with_leng)), C.c_int(int(flip)), C.c_int(int(exact)),
+        _ptr(res.get("f"), _fp), _ptr(res.get("d"), _dp), _ptr(res.get("L"), _dp),
+        _ptr(res.get("nb"), _i64p), _ptr(res.get("nm"), _i64p))
+    if rc != 0:
+        raise ValueError(f"orc_mbfpa_forward failed ({rc})")
+    return res
+
+
+def mbfpa_adjoint(g, tables, volf, mu, pdf, xfactor, resid):
+    """FP64 gradient of sum(resid * I) w.r.t. float element volumes."""
+    gc = proj_geom(g)
+    cosT, sinT, Xc, Yc = [np.ascontiguousarray(t, np.float64) for t in tables]
+    volf = np.ascontiguousarray(volf, np.float32)
+    grad = np.zeros(volf.shape, np.float64)
+    resid = np.ascontiguousarray(resid, np.float64)
+    mu = np.ascontiguousarray(mu, np.float32)
+    pdf = np.ascontiguousarray(pdf, np.float32)
+    L = lib()
+    L.orc_mbfpa_adjoint.restype = C.c_int
+    rc = L.orc_mbfpa_adjoint(C.byref(gc), _ptr(cosT, _dp), _ptr(sinT, _dp), _ptr(Xc, _dp),
+                             _ptr(Yc, _dp), _ptr(volf, _fp), _ptr(mu, _fp), _ptr(pdf, _fp),
+                             C.c_int(int(pdf.shape[0])), C.c_double(xfactor),
+                             _ptr(resid, _dp), _ptr(grad, _dp))
+    if rc != 0:
+        raise ValueError("orc_mbfpa_adjoint failed")
+    return grad
+
+
+# ---------------------------------------------------------------------- FDK --
+
+def fdk_consts(piso, mpn=800.0, pdet=0.05, sad=100.0, cutoff=1.6, gamma_=1.0, alpha=0.5):
+    return OrcFdkConsts(mpn, pdet, sad, piso, cutoff, gamma_, alpha)
+
+
+def const_map(W, consts):
+    """R/filterSinogram.cpp:10-65 prepareConstMap (restated)."""
+    h = np.zeros((W, W), np.float64)
+    L = lib()
+    L.orc_const_map.restype = None
+    L.orc_const_map(C.c_int(W), C.byref(consts), _ptr(h, _dp))
+    return h
+
+
+def filter_coeff(W, consts):
+    L = lib()
+    L.orc_filter_coeff.restype = C.c_double
+    return L.orc_filter_coeff(C.c_int(W), C.byref(consts))
+
+
+def filter_sinogram(proj, xshift, yshift, consts, mode=0, h=None):
+    """R/filterSinogram.cpp:67-131 (restated).  mode 0: float accumulation
+    (reference), mode 1: FP64 accumulation (returns float64)."""
+    proj = np.ascontiguousarray(proj, np.float32)
+    V, H, W = proj.shape
+    if h is None:
+        h = const_map(W, consts)
+    xs = np.ascontiguousarray(xshift, np.float64)
+    ys = np.ascontiguousarray(yshift, np.float64)
+    out_f = np.zeros(proj.shape, np.float32) if mode == 0 else None
+    out_d = np.zeros(proj.shape, np.float64) if mode == 1 else None
+    L = lib()
+    L.orc_filter.restype = None
+    L.orc_filter(C.c_int(V), C.c_int(H), C.c_int(W), _ptr(proj, _fp),
+                 _ptr(np.ascontiguousarray(h, np.float64), _dp), _ptr(xs, _dp), _ptr(ys, _dp),
+                 C.byref(consts), C.c_int(mode), _ptr(out_f, _fp), _ptr(out_d, _dp))
+    return out_f if mode == 0 else out_d
+
+
+def mask(N):
+    m = np.zeros((N, N), np.int8)
+    L = lib()
+    L.orc_mask.restype = None
+    L.orc_mask(C.c_int(N), m.ctypes.data_as(C.c_char_p))
+    return m
+
+
+def backproject(N, Z, zstart, step, scale, filt, xfactor, angles, xshift, consts,
+                vol=None):
+    """R/reconstructImage.cpp:10-184 (restated); returns the double volume."""
+    filt_f = filt_d = None
+    if filt.dtype == np.float64:
+        filt_d = np.ascontiguousarray(filt)
+    else:
+        filt_f = np.ascontiguousarray(filt, np.float32)
+    V, H, W = filt.shape
+    angles = np.ascontiguousarray(angles, np.float64)
+    cosT = np.cos(angles)
+    sinT = np.sin(angles)
+    xs = np.ascontiguousarray(xshift, np.float64)
+    m = mask(N)
+    out = np.zeros((Z, N, N), np.float64) if vol is None else np.ascontiguousarray(vol, np.float64)
+    L = lib()
+    L.orc_backproject.restype = None
+    L.orc_backproject(C.c_int(N), C.c_int(Z), C.c_int(zstart), C.c_double(step),
+                      C.c_double(scale), _ptr(out, _dp), m.ctypes.data_as(C.c_char_p),
+                      C.c_int(H), C.c_int(W), C.c_int(V), _ptr(filt_f, _fp), _ptr(filt_d, _dp),
+                      C.c_int(int(xfactor)), _ptr(angles, _dp), _ptr(cosT, _dp), _ptr(sinT, _dp),
+                      _ptr(xs, _dp), C.byref(consts))
+    return out
+
+
+# -------------------------------------------------- the reference's own code --
+
+def ref_proj():
+    return _load(os.path.join("_ref", "libref_proj.so"))
+
+
+def ref_fdk():
+    return _load(os.path.join("_ref", "libref_fdk.so"))
+
+
+def ref_mbfpa_views(g, tables, vol, mu, pdf, xfactor, views, bins, nthreads=0):
+    """Reference CPU twin reprojection() (P/reprojection.cpp:10) driven per
+    (view, bin); returns (float [V][H][W] un-flipped, no cos^3, seconds)."""
+    L = ref_proj()
+    L.ref_mbfpa_views.restype = C.c_double
+    cosT, sinT, Xc, Yc = [np.ascontiguousarray(t, np.float64) for t in tables]
+    vol = np.ascontiguousarray(vol, np.uint16)
+    mu = np.ascontiguousarray(mu, np.float32)
+    pdf = np.ascontiguousarray(pdf, np.float32)
+    views = np.ascontiguousarray(views, np.int32)
+    bins = np.ascontiguousarray(bins, np.int32)
+    out = np.zeros((g.V, g.H, g.W), np.float32)
+    secs = L.ref_mbfpa_views(
+        C.c_int(g.N), C.c_int(g.Z), _ptr(vol, _u16p), C.c_double(g.s), C.c_double(g.step),
+        C.c_int(g.W), C.c_int(g.H), _ptr(cosT, _dp), _ptr(sinT, _dp), _ptr(Xc, _dp),
+        _ptr(Yc, _dp), C.c_double(xfactor), C.c_double(g.pdet), C.c_double(g.piso),
+        C.c_double(g.sad), C.c_double(g.dpn), C.c_double(g.x_reg), C.c_double(g.y_reg),
+        C.c_double(g.z_reg), _ptr(mu, _fp), _ptr(pdf, _fp), C.c_int(g.nmat),
+        C.c_int(int(pdf.shape[0])), _ptr(views, _ip), C.c_int(len(views)), _ptr(bins, _ip),
+        C.c_int(len(bins)), C.c_int(nthreads), _ptr(out, _fp))
+    return out, secs
+
+
+def ref_attenuation(workdir, spectrum, nmat, mat_type="human"):
+    """Reference attenuation_coefficient (P/prior_weight_production.cpp:200)."""
+    L = ref_proj()
+    L.ref_attenuation.restype = C.c_int
+    mu = np.zeros(1024 * nmat, np.float32)
+    pdf = np.zeros(1024, np.float32)
+    NE = L.ref_attenuation(workdir.encode(), spectrum.encode(), C.c_int(nmat),
+                           mat_type.encode(), _ptr(mu, _fp), _ptr(pdf, _fp))
+    if NE <= 0:
+        raise RuntimeError("reference attenuation_coefficient failed")
+    return mu[: nmat * NE].reshape(nmat, NE).copy(), pdf[:NE].copy()
+
+
+def ref_filter(proj, xshift, yshift, piso, nthreads=0):
+    """Reference filterSinogram (R/filterSinogram.cpp:67); (out, seconds)."""
+    L = ref_fdk()
+    L.ref_filter.restype = C.c_double
+    proj = np.ascontiguousarray(proj, np.float32)
+    V, H, W = proj.shape
+    out = np.zeros_like(proj)
+    secs = L.ref_filter(C.c_int(V), C.c_int(H), C.c_int(W), _ptr(proj, _fp), _ptr(out, _fp),
+                        _ptr(np.ascontiguousarray(xshift, np.float64), _dp),
+                        _ptr(np.ascontiguousarray(yshift, np.float64), _dp),
+                        C.c_double(piso), C.c_int(nthreads))
+    return out, secs
+
+
+def ref_backproject(N, Z, zstart, step, scale, filt, xfactor, angles, xshift, piso,
+                    nthreads=0):
+    """Reference reconstructImage (R/reconstructImage.cpp:10); (vol, seconds)."""
+    L = ref_fdk()
+    L.ref_backproject.restype = C.c_double
+    filt = np.ascontiguousarray(filt, np.float32)
+    V, H, W = filt.shape
+    vol = np.zeros((Z, N, N), np.float64)
+    secs = L.ref_backproject(C.c_int(N), C.c_int(Z), C.c_int(zstart), C.c_double(step),
+                             C.c_double(scale), _ptr(vol, _dp), C.c_int(H), C.c_int(W),
+                             C.c_int(V), _ptr(filt, _fp), C.c_int(int(xfactor)),
+                             _ptr(np.ascontiguousarray(angles, np.float64), _dp),
+                             _ptr(np.ascontiguousarray(xshift, np.float64), _dp),
+                             C.c_double(piso), C.c_int(nthreads))
+    return vol, secs
+
+
+def ref_const_map(W, piso):
+    L = ref_fdk()
+    L.ref_const_map.restype = None
+    h = np.zeros((W, W), np.float64)
+    L.ref_const_map(C.c_int(W), C.c_double(piso), _ptr(h, _dp))
+    return h
+
+
+def ref_mask(N):
+    L = ref_fdk()
+    L.ref_mask.restype = None
+    m = np.zeros((N, N), np.int8)
+    L.ref_mask(C.c_int(N), m.ctypes.data_as(C.c_char_p))
+    return m
