@@ -1,0 +1,232 @@
+/*
+ * vcbct.h -- C ABI of libvcbct, the B200 (sm_100a) implementation of
+ * VirtualCBCT's two hot paths:
+ *
+ *   MBFPA  material-based polychromatic ray-driven forward projection
+ *   FDK    cosine weighting + ramp filter + voxel-driven cone-beam
+ *          backprojection
+ *
+ * Two layers are exported.
+ *
+ *  1. Reference-named entry points with the reference's exact signatures, so
+ *     that a main.cpp-style driver of hagaakihiro/VirtualCBCT links unchanged
+ *     (see INTEGRATION.md).  Each cites the declaration it replaces.
+ *  2. vcbct_* entry points: explicit geometry structs, host or device
+ *     buffers, a CUDA stream (passed as void*, 0 = legacy default stream) and
+ *     an int status (VCBCT_OK = 0).  vcbct_last_error() gives the message of
+ *     the last failure on the calling thread.  Nothing here calls exit().
+ *
+ * All arrays are dense, C order.  Layouts follow the reference:
+ *   element volume   uint16 [Z][nmat][N][N]   (projectionData.cpp:192-215)
+ *   projections      float  [V][H][W]          (reprojectionOnGPU.cu:106)
+ *   reconstruction   short / float / double [Z][N][N] (R/main.cpp:47-49)
+ *   attenuation      float  [nmat][NE] (cm^2/g), pdf float [NE]
+ */
+#ifndef VCBCT_H
+#define VCBCT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------ status codes */
+enum {
+    VCBCT_OK = 0,
+    VCBCT_ERR_ARG = 1,     /* invalid argument (size, NULL, range) */
+    VCBCT_ERR_CUDA = 2,    /* a CUDA runtime call failed */
+    VCBCT_ERR_LIMIT = 3,   /* a size exceeds a documented limit */
+    VCBCT_ERR_STATE = 4,   /* object not ready (e.g. no volume loaded) */
+    VCBCT_ERR_IO = 5,      /* file could not be read or written */
+    VCBCT_ERR_DEVICE = 6   /* a kernel reported a runtime fault flag */
+};
+
+/* Limits of this build. */
+#define VCBCT_MAX_MATERIALS 8   /* element planes per voxel */
+#define VCBCT_MAX_BINS 1024     /* energy bins (reference arrays are 1024) */
+
+const char* vcbct_last_error(void);
+const char* vcbct_version(void);
+
+/* ------------------------------------------------------------------ MBFPA */
+
+/* Projection geometry = the arguments of initializeGPU
+ * (Release_CBCT_Projection_CM/reprojectionOnGPU.h:2-8). */
+typedef struct {
+    int recon_size;          /* N: voxels along x and y */
+    int recon_slices;        /* Z */
+    double recon_scale;      /* voxel pitch in x/y [cm] */
+    double recon_step;       /* slice pitch [cm] */
+    int proj_width;          /* W */
+    int proj_height;         /* H */
+    int n_views;             /* V */
+    double det_pitch_cm;     /* DETECTOR_PITCH_CM */
+    double det_pitch_iso_cm; /* DETECTOR_PITCH_CM_AT_ISO_CENT */
+    double sad_cm;           /* DIST_BTWN_SRC_AND_ISOCENT_CM */
+    double det_pixel_num;    /* DETECTOR_PIXEL_NUM */
+    double x_reg, y_reg, z_reg;
+    int num_material;        /* <= VCBCT_MAX_MATERIALS */
+} vcbct_proj_geometry;
+
+typedef struct vcbct_projector vcbct_projector;
+
+/* Replaces initializeGPU (reprojectionOnGPU.h:2-8): per-view tables are the
+ * outputs of prepareTrigonometricTable (misc.cpp:10-37), n_views entries. */
+int vcbct_projector_create(const vcbct_proj_geometry* g, const double* cos_table,
+                           const double* sin_table, const double* xcenter_shift,
+                           const double* ycenter_shift, vcbct_projector** out);
+/* Replaces terminateGPU (reprojectionOnGPU.h:10). */
+int vcbct_projector_destroy(vcbct_projector* p);
+
+/* Spectrum: Attenuation float [nmat][NE] and pdf_pe float [NE] as produced by
+ * attenuation_coefficient (prior_weight_production.cpp:200-523); xfactor is
+ * the density factor of the input txt (projectionData.cpp:164). */
+int vcbct_projector_set_spectrum(vcbct_projector* p, const float* attenuation,
+                                 const float* pdf, int n_bins, double xfactor);
+
+/* Element volume uint16 [Z][nmat][N][N] (the matVolume of projectionData.cpp),
+ * from host memory (on_device = 0) or device memory (on_device = 1).  The
+ * values are kept unaltered; the device copy is re-laid out once into the
+ * z-fastest packed form the projector reads. */
+int vcbct_projector_load_volume(vcbct_projector* p, const uint16_t* volume, int on_device,
+                                void* stream);
+
+/* Same, from float element volumes [Z][nmat][N][N] (densities x1000, the
+ * differentiable path; no reference counterpart). */
+int vcbct_projector_load_volume_f32(vcbct_projector* p, const float* volume, int on_device,
+                                    void* stream);
+
+/* The spectral projection of reprojectionOnGPU (reprojectionOnGPU.cu:838-1056):
+ * out float [V][H][W] (row H-1-j holds detector row j, as :106), host or
+ * device.  One fused launch marches every ray once and forms the spectral sum
+ * in-kernel instead of one launch + D2H copy per energy bin. */
+int vcbct_projector_forward(vcbct_projector* p, float* out, int out_on_device, void* stream);
+
+/* Per-ray element path integrals L[V][H][W][nmat] (float, cm x density
+ * units) -- the decomposition state; device pointer. */
+int vcbct_projector_path_integrals(vcbct_projector* p, float* d_L, void* stream);
+
+/* Segment counter (diagnostics and the Gseg/s metric): number of in-volume,
+ * in-cylinder segments of every ray, summed; device-side count. */
+int vcbct_projector_count_segments(vcbct_projector* p, unsigned long long* total, void* stream);
+
+/* Adjoint (no reference counterpart; nearest analogue lengthproj.cpp:10-131):
+ * given d(loss)/d(out) as float [V][H][W] on the device, accumulate
+ * d(loss)/d(volume) into d_grad float [Z][nmat][N][N] (+=).  Requires a float
+ * volume (vcbct_projector_load_volume_f32).  Per-ray spectral state is
+ * recomputed, not stored. */
+int vcbct_projector_adjoint(vcbct_projector* p, const float* d_grad_out, float* d_grad,
+                            void* stream);
+
+/* Reference-named entry points (Release_CBCT_Projection_CM/reprojectionOnGPU.h).
+ * Same argument lists and meaning, including the ignored ones (ite,
+ * reprojection_float, npf_double, projVolume, anglesRad, xalpha,
+ * startProjNumber).  reprojectionOnGPU writes "<outputname>.raw" as the
+ * reference does.  Errors are printed to stderr and leave the state
+ * unchanged (the reference exits with status 0 instead). */
+void initializeGPU(int reconSize, double reconScale, int reconSlices, double reconStep,
+                   int projImgHeight, int projImgWidth, int totalProjNumber, double* cosTable,
+                   double* sinTable, double* XcenterShift, double* YcenterShift, double x_reg,
+                   double y_reg, double z_reg, double DETECTOR_PITCH_CM,
+                   double DETECTOR_PITCH_CM_AT_ISO_CENT, double DIST_BTWN_SRC_AND_ISOCENT_CM,
+                   double DETECTOR_PIXEL_NUM, int num_material);
+void terminateGPU(void);
+void reprojectionOnGPU(int ite, int reconSize, int reconSlices, unsigned short* reconImageshort,
+                       float* reprojection_float, float* npf_double, float* projVolume,
+                       double reconScale, double reconStep, int projImgWidth,
+                       int projImgHeight, int startProjNumber, int endProjNumber,
+                       double* anglesRad, double* cosTable, double* sinTable,
+                       double* XcenterShift, double* YcenterShift, double xfactor,
+                       double* xalpha, double DETECTOR_PITCH_CM,
+                       double DETECTOR_PITCH_CM_AT_ISO_CENT,
+                       double DIST_BTWN_SRC_AND_ISOCENT_CM, double DETECTOR_PIXEL_NUM,
+                       double x_reg, double y_reg, double z_reg, float* Attenuation,
+                       float* pdf_pe, int num_material, int NE, char* outputname);
+
+/* Host helpers of the projector's input preparation. */
+/* misc.cpp:10-37 prepareTrigonometricTable (outputs caller-allocated). */
+int vcbct_proj_trig_tables(int proj_width, int proj_height, int n_views,
+                           const double* angles_rad, const double* xshift,
+                           const double* yshift, double det_pitch_cm, double det_pixel_num,
+                           double* cos_table, double* sin_table, double* xcenter_shift,
+                           double* ycenter_shift);
+/* prior_weight_production.cpp:200-523 attenuation_coefficient: parse the
+ * spectrum CSV and look up photo+Compton+Rayleigh (cm^2/g) per element at
+ * each bin midpoint in the x-ray DB directory (photo_/comp_/rayl_5keVto150keV
+ * .csv).  mu: nmat*VCBCT_MAX_BINS floats, pdf: VCBCT_MAX_BINS floats. */
+int vcbct_attenuation_table(const char* spectrum_csv, const char* xraydb_dir, int num_material,
+                            int nthin, float* mu, float* pdf, int* n_bins);
+
+/* -------------------------------------------------------------------- FDK */
+
+/* Geometry of filterSinogram / reconstructImage.  The reference fixes
+ * MAX_PIC_NUM, DETECTOR_PITCH_CM, DIST_BTWN_SRC_AND_ISOCENT_CM and the filter
+ * shape at compile time (R/physParams.h:22-41); here they are fields, and
+ * vcbct_fdk_default_geometry() fills the reference's values. */
+typedef struct {
+    int proj_width;          /* W */
+    int proj_height;         /* H */
+    int n_views;             /* V (usedProjNumber) */
+    int recon_size;          /* N */
+    int recon_slices;        /* Z */
+    int zstart;              /* reconOffset [cm], an int in the reference */
+    double recon_step;       /* [cm] */
+    double recon_scale;      /* [cm] */
+    int xfactor;             /* CT-value factor (int, R/projectionDataMVkV.h:26) */
+    double det_pitch_iso_cm; /* DETECTOR_PITCH_CM_AT_ISO_CENT */
+    double det_pitch_cm;     /* DETECTOR_PITCH_CM */
+    double max_pic_num;      /* MAX_PIC_NUM */
+    double sad_cm;           /* DIST_BTWN_SRC_AND_ISOCENT_CM */
+    double cutoff;           /* CUTOFF_FREQ */
+    double gamma;            /* GAMMA */
+    double alpha;            /* ALPHA */
+    int redundancy;          /* 0: none (reference); 1: Parker/half-fan weights */
+} vcbct_fdk_geometry;
+
+void vcbct_fdk_default_geometry(vcbct_fdk_geometry* g);
+
+enum {
+    VCBCT_FILTER_DIRECT_F32 = 0, /* FP32 direct Toeplitz product (parity path) */
+    VCBCT_FILTER_BF16X3 = 1      /* tcgen05 BF16 3-term split GEMM, FP32 accumulate */
+};
+
+typedef struct vcbct_fdk vcbct_fdk;
+
+/* angles_rad / xshift / yshift: per view, in the order the projections are
+ * stored (the caller applies the reference's CW reversal,
+ * projectionDataMVkV.cpp:184-197, as loadData does). */
+int vcbct_fdk_create(const vcbct_fdk_geometry* g, const double* angles_rad,
+                     const double* xshift, const double* yshift, vcbct_fdk** out);
+int vcbct_fdk_destroy(vcbct_fdk* f);
+/* Optional: replace the ramp kernel h[W][W] (prepareConstMap layout). */
+int vcbct_fdk_set_kernel(vcbct_fdk* f, const double* h);
+/* filterSinogram (R/filterSinogram.cpp:67-131): proj, filtered float [V][H][W]. */
+int vcbct_fdk_filter(vcbct_fdk* f, const float* proj, float* filtered, int on_device,
+                     int method, void* stream);
+/* reconstructImage (R/reconstructImage.cpp:10-184) over filtered [V][H][W]:
+ * vol_f32 float [Z][N][N] (may be NULL) and vol_i16 short [Z][N][N] (the
+ * (short) cast of R/main.cpp:179-185; may be NULL).  Overwrites. */
+int vcbct_fdk_backproject(vcbct_fdk* f, const float* filtered, float* vol_f32, short* vol_i16,
+                          int on_device, void* stream);
+
+/* Reference-named FDK entry points (R/filterSinogram.h:2-6,
+ * R/reconstructImage.h:2-5).  Arrays are VOLUME-ONE style pointer tables over
+ * contiguous storage (mallocMD.cpp:69-109).  prepareConstMap returns a
+ * pointer table the caller frees with vcbct_free_const_map. */
+double** prepareConstMap(int projWidth, double DETECTOR_PITCH_CM_AT_ISO_CENT);
+void vcbct_free_const_map(double** constMap, int projWidth);
+void filterSinogram(int projHeight, int projWidth, int sngrmHeight, float*** projVolume,
+                    float*** fltdVoxData, double** constMap, double* xshift, double* yshift,
+                    double DETECTOR_PITCH_CM_AT_ISO_CENT);
+void reconstructImage(int reconSize, int reconSlices, int zstart, double reconStep,
+                      double reconScale, double*** reconVoxData, char** maskData,
+                      int projHeight, int projWidth, int sngrmHeight, float*** sngrmVoxData,
+                      int xfactor, double* anglesRad, double* cosTable, double* sinTable,
+                      double* xshift, double DETECTOR_PITCH_CM_AT_ISO_CENT);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* VCBCT_H */

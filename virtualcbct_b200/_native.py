@@ -1,0 +1,124 @@
+"""ctypes binding of libvcbct.so (the C ABI declared in include/vcbct.h).
+
+The library is built in-tree by ``virtualcbct_b200/csrc/Makefile`` (see
+``__graft_entry__.build``).  There is no fallback: if the library is missing,
+``lib()`` raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libvcbct.so")
+
+VCBCT_OK = 0
+ERRORS = {1: "invalid argument", 2: "CUDA error", 3: "limit exceeded", 4: "bad state",
+          5: "I/O error", 6: "device fault flag"}
+
+MAX_MATERIALS = 8
+MAX_BINS = 1024
+
+FILTER_DIRECT_F32 = 0
+FILTER_BF16X3 = 1
+
+
+class VcbctError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"vcbct error {code} ({ERRORS.get(code, '?')}): {msg}")
+        self.code = code
+
+
+class ProjGeometryC(C.Structure):
+    _fields_ = [("recon_size", C.c_int), ("recon_slices", C.c_int),
+                ("recon_scale", C.c_double), ("recon_step", C.c_double),
+                ("proj_width", C.c_int), ("proj_height", C.c_int), ("n_views", C.c_int),
+                ("det_pitch_cm", C.c_double), ("det_pitch_iso_cm", C.c_double),
+                ("sad_cm", C.c_double), ("det_pixel_num", C.c_double),
+                ("x_reg", C.c_double), ("y_reg", C.c_double), ("z_reg", C.c_double),
+                ("num_material", C.c_int)]
+
+
+class FdkGeometryC(C.Structure):
+    _fields_ = [("proj_width", C.c_int), ("proj_height", C.c_int), ("n_views", C.c_int),
+                ("recon_size", C.c_int), ("recon_slices", C.c_int), ("zstart", C.c_int),
+                ("recon_step", C.c_double), ("recon_scale", C.c_double), ("xfactor", C.c_int),
+                ("det_pitch_iso_cm", C.c_double), ("det_pitch_cm", C.c_double),
+                ("max_pic_num", C.c_double), ("sad_cm", C.c_double), ("cutoff", C.c_double),
+                ("gamma", C.c_double), ("alpha", C.c_double), ("redundancy", C.c_int)]
+
+
+_vp = C.c_void_p
+_dp = C.POINTER(C.c_double)
+_fp = C.POINTER(C.c_float)
+_ip = C.POINTER(C.c_int)
+
+# Every extern "C" symbol of include/vcbct.h with its ctypes signature.
+SIGNATURES = {
+    "vcbct_last_error": (C.c_char_p, []),
+    "vcbct_version": (C.c_char_p, []),
+    "vcbct_projector_create": (C.c_int, [C.POINTER(ProjGeometryC), _dp, _dp, _dp, _dp, C.POINTER(_vp)]),
+    "vcbct_projector_destroy": (C.c_int, [_vp]),
+    "vcbct_projector_set_spectrum": (C.c_int, [_vp, _fp, _fp, C.c_int, C.c_double]),
+    "vcbct_projector_load_volume": (C.c_int, [_vp, _vp, C.c_int, _vp]),
+    "vcbct_projector_load_volume_f32": (C.c_int, [_vp, _vp, C.c_int, _vp]),
+    "vcbct_projector_forward": (C.c_int, [_vp, _vp, C.c_int, _vp]),
+    "vcbct_projector_path_integrals": (C.c_int, [_vp, _vp, _vp]),
+    "vcbct_projector_count_segments": (C.c_int, [_vp, C.POINTER(C.c_ulonglong), _vp]),
+    "vcbct_projector_adjoint": (C.c_int, [_vp, _vp, _vp, _vp]),
+    "vcbct_proj_trig_tables": (C.c_int, [C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, C.c_double,
+                                         C.c_double, _dp, _dp, _dp, _dp]),
+    "vcbct_attenuation_table": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int, C.c_int, _fp, _fp, _ip]),
+    "vcbct_fdk_default_geometry": (None, [C.POINTER(FdkGeometryC)]),
+    "vcbct_fdk_create": (C.c_int, [C.POINTER(FdkGeometryC), _dp, _dp, _dp, C.POINTER(_vp)]),
+    "vcbct_fdk_destroy": (C.c_int, [_vp]),
+    "vcbct_fdk_set_kernel": (C.c_int, [_vp, _dp]),
+    "vcbct_fdk_filter": (C.c_int, [_vp, _vp, _vp, C.c_int, C.c_int, _vp]),
+    "vcbct_fdk_backproject": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int, _vp]),
+    # reference-named entry points
+    "initializeGPU": (None, [C.c_int, C.c_double, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int,
+                             _dp, _dp, _dp, _dp, C.c_double, C.c_double, C.c_double, C.c_double,
+                             C.c_double, C.c_double, C.c_double, C.c_int]),
+    "terminateGPU": (None, []),
+    "reprojectionOnGPU": (None, [C.c_int, C.c_int, C.c_int, _vp, _fp, _fp, _fp, C.c_double,
+                                 C.c_double, C.c_int, C.c_int, C.c_int, C.c_int, _dp, _dp, _dp,
+                                 _dp, _dp, C.c_double, _dp, C.c_double, C.c_double, C.c_double,
+                                 C.c_double, C.c_double, C.c_double, C.c_double, _fp, _fp,
+                                 C.c_int, C.c_int, C.c_char_p]),
+    "prepareConstMap": (C.POINTER(_dp), [C.c_int, C.c_double]),
+    "vcbct_free_const_map": (None, [C.POINTER(_dp), C.c_int]),
+    "filterSinogram": (None, [C.c_int, C.c_int, C.c_int, _vp, _vp, C.POINTER(_dp), _dp, _dp,
+                              C.c_double]),
+    "reconstructImage": (None, [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, _vp, _vp,
+                                C.c_int, C.c_int, C.c_int, _vp, C.c_int, _dp, _dp, _dp, _dp,
+                                C.c_double]),
+}
+
+_lock = threading.Lock()
+_lib: C.CDLL | None = None
+
+
+def lib() -> C.CDLL:
+    """Load libvcbct.so (once).  Raises if it has not been built."""
+    global _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(
+                f"{LIB_PATH} is missing: build it with `make -C virtualcbct_b200/csrc` "
+                "(or __graft_entry__.build()); there is no CPU fallback")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+        return L
+
+
+def check(rc: int) -> None:
+    if rc != VCBCT_OK:
+        msg = lib().vcbct_last_error()
+        raise VcbctError(rc, msg.decode() if msg else "")

@@ -1,0 +1,881 @@
+// capi.cpp -- the C ABI of libvcbct (declared in include/vcbct.h): projector
+// and FDK objects, the reference-named entry points, and host-side input
+// preparation.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "internal.h"
+
+namespace vcbct {
+
+static thread_local std::string g_last_error;
+
+void set_error(const std::string& msg) { g_last_error = msg; }
+
+int fail(int code, const std::string& msg)
+{
+    set_error(msg);
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char* what)
+{
+    return fail(VCBCT_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// Grow-only device buffer.
+struct DevBuf {
+    void* p = nullptr;
+    size_t n = 0;
+    cudaError_t ensure(size_t bytes)
+    {
+        if (bytes <= n) return cudaSuccess;
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+        cudaError_t e = cudaMalloc(&p, bytes);
+        if (e == cudaSuccess) n = bytes;
+        return e;
+    }
+    void release()
+    {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    template <class T>
+    T* as() const { return static_cast<T*>(p); }
+};
+
+static const double kPi = 3.141592653589793238462643383279;
+
+}  // namespace vcbct
+
+using namespace vcbct;
+
+// ===================================================================== MBFPA
+
+struct vcbct_projector {
+    vcbct_proj_geometry g;
+    ProjParams pp;
+    DevBuf views;      // ViewGeom[V]
+    DevBuf vol_u16;    // packed
+    DevBuf vol_f32;    // packed
+    DevBuf stage;      // staging for host inputs / outputs
+    DevBuf spec_mu;    // float4 [NE][2]
+    DevBuf spec_pdf;   // float [NE]
+    DevBuf grad_pk;    // packed float gradient accumulator
+    DevBuf counter;    // unsigned long long + int err flag
+    int NE = 0;
+    int have_u16 = 0, have_f32 = 0;
+    int cols_per_block = 4;
+};
+
+extern "C" const char* vcbct_last_error(void) { return g_last_error.c_str(); }
+extern "C" const char* vcbct_version(void) { return "vcbct-b200 0.1 (sm_100a)"; }
+
+static int check_geom(const vcbct_proj_geometry* g)
+{
+    if (!g) return fail(VCBCT_ERR_ARG, "geometry is NULL");
+    if (g->recon_size <= 0 || g->recon_slices <= 0 || g->proj_width <= 0 || g->proj_height <= 0 ||
+        g->n_views <= 0)
+        return fail(VCBCT_ERR_ARG, "geometry sizes must be positive");
+    if (g->num_material <= 0 || g->num_material > VCBCT_MAX_MATERIALS)
+        return fail(VCBCT_ERR_LIMIT, "num_material must be in [1, 8]");
+    if (!(g->recon_scale > 0) || !(g->recon_step > 0) || !(g->sad_cm > 0) ||
+        !(g->det_pitch_cm > 0) || !(g->det_pitch_iso_cm > 0) || !(g->det_pixel_num > 0))
+        return fail(VCBCT_ERR_ARG, "geometry pitches and distances must be positive");
+    if ((double)g->recon_size * g->recon_size * g->recon_slices > 2.0e9)
+        return fail(VCBCT_ERR_LIMIT, "volume exceeds 2e9 voxels");
+    if ((double)g->proj_width * g->proj_height * g->n_views > 2.0e9)
+        return fail(VCBCT_ERR_LIMIT, "projection stack exceeds 2e9 pixels");
+    return VCBCT_OK;
+}
+
+extern "C" int vcbct_projector_create(const vcbct_proj_geometry* g, const double* cos_table,
+                                      const double* sin_table, const double* xcs,
+                                      const double* ycs, vcbct_projector** out)
+{
+    if (!out) return fail(VCBCT_ERR_ARG, "out is NULL");
+    *out = nullptr;
+    int rc = check_geom(g);
+    if (rc) return rc;
+    if (!cos_table || !sin_table || !xcs || !ycs) return fail(VCBCT_ERR_ARG, "view tables are NULL");
+    auto* p = new vcbct_projector();
+    p->g = *g;
+    p->pp = ProjParams{g->recon_size, g->recon_slices, g->proj_width, g->proj_height, g->n_views,
+                       g->num_material, g->recon_scale, g->recon_step, g->det_pitch_cm,
+                       g->det_pitch_iso_cm, g->sad_cm, g->det_pixel_num, g->x_reg, g->y_reg,
+                       g->z_reg};
+    std::vector<ViewGeom> vg(g->n_views);
+    for (int i = 0; i < g->n_views; i++) vg[i] = ViewGeom{cos_table[i], sin_table[i], xcs[i], ycs[i]};
+    cudaError_t e = p->views.ensure(sizeof(ViewGeom) * vg.size());
+    if (e == cudaSuccess) e = cudaMemcpy(p->views.p, vg.data(), sizeof(ViewGeom) * vg.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = p->counter.ensure(64);
+    if (e == cudaSuccess) e = cudaMemset(p->counter.p, 0, 64);
+    if (e != cudaSuccess) {
+        delete p;
+        return cuda_fail(e, "vcbct_projector_create");
+    }
+    if (const char* c = std::getenv("VCBCT_COLS_PER_BLOCK")) {
+        int v = std::atoi(c);
+        if (v == 1 || v == 2 || v == 4 || v == 8) p->cols_per_block = v;
+    }
+    *out = p;
+    return VCBCT_OK;
+}
+
+extern "C" int vcbct_projector_destroy(vcbct_projector* p)
+{
+    if (!p) return VCBCT_OK;
+    p->views.release();
+    p->vol_u16.release();
+    p->vol_f32.release();
+    p->stage.release();
+    p->spec_mu.release();
+    p->spec_pdf.release();
+    p->grad_pk.release();
+    p->counter.release();
+    delete p;
+    return VCBCT_OK;
+}
+
+extern "C" int vcbct_projector_set_spectrum(vcbct_projector* p, const float* mu, const float* pdf,
+                                            int NE, double xfactor)
+{
+    if (!p || !mu || !pdf) return fail(VCBCT_ERR_ARG, "NULL argument");
+    if (NE <= 0 || NE > VCBCT_MAX_BINS) return fail(VCBCT_ERR_LIMIT, "n_bins must be in [1, 1024]");
+    if (!(xfactor != 0.0) || !std::isfinite(xfactor)) return fail(VCBCT_ERR_ARG, "xfactor must be finite and non-zero");
+    std::vector<float> tab((size_t)NE * 8, 0.0f);
+    for (int e = 0; e < NE; e++)
+        for (int k = 0; k < p->g.num_material; k++)
+            tab[(size_t)e * 8 + k] = (float)((double)mu[(size_t)k * NE + e] / xfactor);
+    VCBCT_CUDA_TRY(p->spec_mu.ensure(tab.size() * sizeof(float)));
+    VCBCT_CUDA_TRY(p->spec_pdf.ensure((size_t)NE * sizeof(float)));
+    VCBCT_CUDA_TRY(cudaMemcpy(p->spec_mu.p, tab.data(), tab.size() * sizeof(float), cudaMemcpyHostToDevice));
+    VCBCT_CUDA_TRY(cudaMemcpy(p->spec_pdf.p, pdf, (size_t)NE * sizeof(float), cudaMemcpyHostToDevice));
+    p->NE = NE;
+    return VCBCT_OK;
+}
+
+static size_t vol_elems(const vcbct_proj_geometry& g)
+{
+    return (size_t)g.recon_slices * g.num_material * g.recon_size * g.recon_size;
+}
+
+extern "C" int vcbct_projector_load_volume(vcbct_projector* p, const uint16_t* vol, int on_device,
+                                           void* stream)
+{
+    if (!p || !vol) return fail(VCBCT_ERR_ARG, "NULL argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    const auto& g = p->g;
+    const uint16_t* src = vol;
+    if (!on_device) {
+        VCBCT_CUDA_TRY(p->stage.ensure(vol_elems(g) * sizeof(uint16_t)));
+        VCBCT_CUDA_TRY(cudaMemcpyAsync(p->stage.p, vol, vol_elems(g) * sizeof(uint16_t), cudaMemcpyHostToDevice, st));
+        src = p->stage.as<uint16_t>();
+    }
+    VCBCT_CUDA_TRY(p->vol_u16.ensure(packed_u16_bytes(g.recon_size, g.recon_slices)));
+    VCBCT_CUDA_TRY(launch_pack_u16(src, g.recon_size, g.recon_slices, g.num_material, p->vol_u16.as<uint4>(), st));
+    p->have_u16 = 1;
+    p->have_f32 = 0;
+    return VCBCT_OK;
+}
+
+extern "C" int vcbct_projector_load_volume_f32(vcbct_projector* p, const float* vol, int on_device,
+                                               void* stream)
+{
+    if (!p || !vol) return fail(VCBCT_ERR_ARG, "NULL argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    const auto& g = p->g;
+    const float* src = vol;
+    if (!on_device) {
+        VCBCT_CUDA_TRY(p->stage.ensure(vol_elems(g) * sizeof(float)));
+        VCBCT_CUDA_TRY(cudaMemcpyAsync(p->stage.p, vol, vol_elems(g) * sizeof(float), cudaMemcpyHostToDevice, st));
+        src = p->stage.as<float>();
+    }
+    VCBCT_CUDA_TRY(p->vol_f32.ensure(packed_f32_bytes(g.recon_size, g.recon_slices)));
+    VCBCT_CUDA_TRY(launch_pack_f32(src, g.recon_size, g.recon_slices, g.num_material, p->vol_f32.as<float4>(), st));
+    p->have_f32 = 1;
+    p->have_u16 = 0;
+    return VCBCT_OK;
+}
+
+static int make_fwd_args(vcbct_projector* p, ForwardArgs& a)
+{
+    if (!p->have_u16 && !p->have_f32) return fail(VCBCT_ERR_STATE, "no volume loaded");
+    if (p->NE <= 0) return fail(VCBCT_ERR_STATE, "no spectrum set");
+    a = ForwardArgs{};
+    a.p = p->pp;
+    a.views = p->views.as<ViewGeom>();
+    a.spec = SpectrumDev{p->spec_mu.as<float4>(), p->spec_pdf.as<float>(), p->NE};
+    a.vol_u16 = p->have_u16 ? p->vol_u16.as<uint4>() : nullptr;
+    a.vol_f32 = p->have_f32 ? p->vol_f32.as<float4>() : nullptr;
+    a.err_flag = reinterpret_cast<int*>(p->counter.as<char>() + 8);
+    a.cols_per_block = p->cols_per_block;
+    return VCBCT_OK;
+}
+
+extern "C" int vcbct_projector_forward(vcbct_projector* p, float* out, int out_on_device, void* stream)
+{
+    if (!p || !out) return fail(VCBCT_ERR_ARG, "NULL argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    ForwardArgs a;
+    int rc = make_fwd_args(p, a);
+    if (rc) return rc;
+    const size_t nout = (size_t)p->g.n_views * p->g.proj_height * p->g.proj_width;
+    float* dout = out;
+    if (!out_on_device) {
+        // the staging buffer may hold the host volume of load_volume: use a
+        // region after it
+        VCBCT_CUDA_TRY(p->grad_pk.ensure(nout * sizeof(float)));
+        dout = p->grad_pk.as<float>();
+    }
+    a.out = dout;
+    VCBCT_CUDA_TRY(launch_forward(a, st));
+    if (!out_on_device) {
+        VCBCT_CUDA_TRY(cudaMemcpyAsync(out, dout, nout * sizeof(float), cudaMemcpyDeviceToHost, st));
+        VCBCT_CUDA_TRY(cudaStreamSynchronize(st));
+    }
+    return VCBCT_OK;
+}
+
+extern "C" int vcbct_projector_path_integrals(vcbct_projector* p, float* d_L, void* stream)
+{
+    if (!p || !d_L) return fail(VCBCT_ERR_ARG, "NULL argument");
+    ForwardArgs a;
+    int rc = make_fwd_args(p, a);
+    if (rc) return rc;
+    a.L_out = d_L;
+    VCBCT_CUDA_TRY(launch_forward(a, (cudaStream_t)stream));
+    return VCBCT_OK;
+}
+
+extern "C" int vcbct_projector_count_segments(vcbct_projector* p, unsigned long long* total, void* stream)
+{
+    if (!p || !total) return fail(VCBCT_ERR_ARG, "NULL argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    ForwardArgs a;
+    int rc = make_fwd_args(p, a);
+    if (rc) return rc;
+    unsigned long long* cnt = p->counter.as<unsigned long long>();
+    VCBCT_CUDA_TRY(cudaMemsetAsync(cnt, 0, sizeof(unsigned long long), st));
+    a.seg_count = cnt;
+    VCBCT_CUDA_TRY(launch_forward(a, st));
+    VCBCT_CUDA_TRY(cudaMemcpyAsync(total, cnt, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+    VCBCT_CUDA_TRY(cudaStreamSynchronize(st));
+    return VCBCT_OK;
+}
+
+extern "C" int vcbct_projector_adjoint(vcbct_projector* p, const float* d_grad_out, float* d_grad,
+                                       void* stream)
+{
+    if (!p || !d_grad_out || !d_grad) return fail(VCBCT_ERR_ARG, "NULL argument");
+    if (!p->have_f32) return fail(VCBCT_ERR_STATE, "the adjoint needs a float volume (load_volume_f32)");
+    if (p->NE <= 0) return fail(VCBCT_ERR_STATE, "no spectrum set");
+    cudaStream_t st = (cudaStream_t)stream;
+    const auto& g = p->g;
+    const size_t pk = packed_f32_bytes(g.recon_size, g.recon_slices);
+    VCBCT_CUDA_TRY(p->grad_pk.ensure(pk));
+    VCBCT_CUDA_TRY(cudaMemsetAsync(p->grad_pk.p, 0, pk, st));
+    AdjointArgs a{};
+    a.p = p->pp;
+    a.views = p->views.as<ViewGeom>();
+    a.spec = SpectrumDev{p->spec_mu.as<float4>(), p->spec_pdf.as<float>(), p->NE};
+    a.vol_f32 = p->vol_f32.as<float4>();
+    a.grad_out = d_grad_out;
+    a.grad_packed = p->grad_pk.as<float4>();
+    a.err_flag = reinterpret_cast<int*>(p->counter.as<char>() + 8);
+    a.cols_per_block = p->cols_per_block;
+    VCBCT_CUDA_TRY(launch_adjoint(a, st));
+    VCBCT_CUDA_TRY(launch_unpack_grad(p->grad_pk.as<float4>(), g.recon_size, g.recon_slices, g.num_material, d_grad, st));
+    return VCBCT_OK;
+}
+
+// ------------------------------------------------------------ host helpers --
+
+extern "C" int vcbct_proj_trig_tables(int W, int H, int V, const double* angles, const double* xs,
+                                      const double* ys, double pdet, double dpn, double* c,
+                                      double* s, double* xc, double* yc)
+{
+    (void)W;
+    if (V <= 0 || H <= 0 || !angles || !xs || !ys || !c || !s || !xc || !yc)
+        return fail(VCBCT_ERR_ARG, "invalid argument");
+    // misc.cpp:22-32: the projector's shifts are scaled by 10 and use the
+    // detector height for both axes.
+    for (int i = 0; i < V; i++) {
+        c[i] = std::cos(angles[i]);
+        s[i] = std::sin(angles[i]);
+        xc[i] = -H / 2.0 - xs[i] * 10.0 / (pdet * (dpn / H));
+        yc[i] = -H / 2.0 - ys[i] * 10.0 / (pdet * (dpn / H));
+    }
+    return VCBCT_OK;
+}
+
+// Spectrum + x-ray DB lookup, following attenuation_coefficient
+// (prior_weight_production.cpp:200-523): bin midpoints in MeV (float sum of
+// the CSV's lo/hi), optional merging of nthin bins, pdf normalised in float,
+// and for each element the photo + Compton + Rayleigh mass attenuation of the
+// DB row whose energy matches the midpoint within 0.03 eV.
+extern "C" int vcbct_attenuation_table(const char* spectrum_csv, const char* dbdir, int nmat,
+                                       int nthin, float* mu, float* pdf, int* n_bins)
+{
+    if (!spectrum_csv || !dbdir || !mu || !pdf || !n_bins) return fail(VCBCT_ERR_ARG, "NULL argument");
+    if (nmat <= 0 || nmat > 6) return fail(VCBCT_ERR_LIMIT, "the x-ray DB holds 6 elements (H,C,N,O,P,Ca)");
+    if (nthin <= 0) return fail(VCBCT_ERR_ARG, "nthin must be positive");
+    FILE* fp = std::fopen(spectrum_csv, "r");
+    if (!fp) return fail(VCBCT_ERR_IO, std::string("cannot open spectrum ") + spectrum_csv);
+    char row[1024];
+    std::vector<double> energy;
+    std::vector<float> frac;
+    if (!std::fgets(row, sizeof row, fp)) {
+        std::fclose(fp);
+        return fail(VCBCT_ERR_IO, "empty spectrum file");
+    }
+    while (std::fgets(row, sizeof row, fp)) {
+        float lo, hi, fr;
+        if (std::sscanf(row, "%f,%f,%f", &lo, &hi, &fr) != 3) continue;
+        energy.push_back((hi + lo) * 0.5);
+        frac.push_back(fr);
+        if (energy.size() > 1024) break;
+    }
+    std::fclose(fp);
+    // merge nthin consecutive bins (:231-248)
+    std::vector<float> pdf_t, e_t;
+    double psum = 0.0, esum = 0.0, sum_t = 0.0;
+    for (size_t i = 0; i < energy.size(); i++) {
+        psum += frac[i];
+        esum += energy[i];
+        const long q = (long)i - nthin + 1;
+        if (q >= 0 && q % nthin == 0) {
+            pdf_t.push_back((float)psum);
+            e_t.push_back((float)(esum / nthin));
+            sum_t += psum;
+            psum = 0.0;
+            esum = 0.0;
+        }
+    }
+    const int NE = (int)pdf_t.size();
+    if (NE <= 0 || NE > VCBCT_MAX_BINS) return fail(VCBCT_ERR_LIMIT, "spectrum has no bins or more than 1024");
+    const float sum = (float)sum_t;
+    for (int i = 0; i < NE; i++) pdf[i] = pdf_t[i] / sum;
+
+    const char* names[3] = {"photo_5keVto150keV.csv", "comp_5keVto150keV.csv", "rayl_5keVto150keV.csv"};
+    std::vector<double> db_e;
+    std::vector<double> db[3];
+    for (int t = 0; t < 3; t++) {
+        std::string path = std::string(dbdir) + "/" + names[t];
+        FILE* f = std::fopen(path.c_str(), "r");
+        if (!f) return fail(VCBCT_ERR_IO, "cannot open " + path);
+        char line[512];
+        if (!std::fgets(line, sizeof line, f)) {
+            std::fclose(f);
+            return fail(VCBCT_ERR_IO, "empty " + path);
+        }
+        while (std::fgets(line, sizeof line, f)) {
+            double v[7];
+            if (std::sscanf(line, "%lf,%lf,%lf,%lf,%lf,%lf,%lf", &v[0], &v[1], &v[2], &v[3], &v[4], &v[5], &v[6]) != 7) continue;
+            for (int k = 0; k < 6; k++) db[t].push_back(v[k]);
+            if (t == 0) db_e.push_back(v[6] / 1000 / 1000);
+        }
+        std::fclose(f);
+    }
+    const size_t nrow = db_e.size();
+    if (nrow == 0 || db[1].size() != 6 * nrow || db[2].size() != 6 * nrow)
+        return fail(VCBCT_ERR_IO, "x-ray DB tables are inconsistent");
+    for (int k = 0; k < nmat; k++) {
+        for (int i = 0; i < NE; i++) {
+            const double E = (double)e_t[i];
+            long hit = -1;
+            for (size_t r = 0; r < nrow; r++) {
+                const double aaa = db_e[r] * 1000 * 1000 * 1000 - E * 1000 * 1000 * 1000;
+                if (-30 < aaa && aaa < 30) hit = (long)r;  // the last match wins, as :471-501
+            }
+            if (hit < 0) return fail(VCBCT_ERR_ARG, "spectrum bin midpoint not on the 5 eV DB grid");
+            mu[(size_t)k * NE + i] = (float)(db[0][hit * 6 + k] + db[1][hit * 6 + k] + db[2][hit * 6 + k] + 0.0);
+        }
+    }
+    *n_bins = NE;
+    return VCBCT_OK;
+}
+
+// ------------------------------------------------ reference-named MBFPA API --
+
+namespace {
+std::mutex g_ref_mu;
+vcbct_projector* g_ref_proj = nullptr;
+}  // namespace
+
+extern "C" void initializeGPU(int reconSize, double reconScale, int reconSlices, double reconStep,
+                              int projImgHeight, int projImgWidth, int totalProjNumber,
+                              double* cosTable, double* sinTable, double* XcenterShift,
+                              double* YcenterShift, double x_reg, double y_reg, double z_reg,
+                              double DETECTOR_PITCH_CM, double DETECTOR_PITCH_CM_AT_ISO_CENT,
+                              double DIST_BTWN_SRC_AND_ISOCENT_CM, double DETECTOR_PIXEL_NUM,
+                              int num_material)
+{
+    std::lock_guard<std::mutex> lk(g_ref_mu);
+    vcbct_proj_geometry g{reconSize, reconSlices, reconScale, reconStep, projImgWidth,
+                          projImgHeight, totalProjNumber, DETECTOR_PITCH_CM,
+                          DETECTOR_PITCH_CM_AT_ISO_CENT, DIST_BTWN_SRC_AND_ISOCENT_CM,
+                          DETECTOR_PIXEL_NUM, x_reg, y_reg, z_reg, num_material};
+    vcbct_projector* p = nullptr;
+    int rc = vcbct_projector_create(&g, cosTable, sinTable, XcenterShift, YcenterShift, &p);
+    if (rc) {
+        std::fprintf(stderr, "initializeGPU: %s\n", vcbct_last_error());
+        return;
+    }
+    if (g_ref_proj) vcbct_projector_destroy(g_ref_proj);
+    g_ref_proj = p;
+}
+
+extern "C" void terminateGPU(void)
+{
+    std::lock_guard<std::mutex> lk(g_ref_mu);
+    vcbct_projector_destroy(g_ref_proj);
+    g_ref_proj = nullptr;
+}
+
+extern "C" void reprojectionOnGPU(int ite, int reconSize, int reconSlices, unsigned short* reconImageshort,
+                                  float* reprojection_float, float* npf_double, float* projVolume,
+                                  double reconScale, double reconStep, int projImgWidth,
+                                  int projImgHeight, int startProjNumber, int endProjNumber,
+                                  double* anglesRad, double* cosTable, double* sinTable,
+                                  double* XcenterShift, double* YcenterShift, double xfactor,
+                                  double* xalpha, double DETECTOR_PITCH_CM,
+                                  double DETECTOR_PITCH_CM_AT_ISO_CENT,
+                                  double DIST_BTWN_SRC_AND_ISOCENT_CM, double DETECTOR_PIXEL_NUM,
+                                  double x_reg, double y_reg, double z_reg, float* Attenuation,
+                                  float* pdf_pe, int num_material, int NE, char* outputname)
+{
+    (void)ite; (void)reprojection_float; (void)npf_double; (void)projVolume; (void)startProjNumber;
+    (void)anglesRad; (void)xalpha; (void)reconScale; (void)reconStep; (void)cosTable;
+    (void)sinTable; (void)XcenterShift; (void)YcenterShift; (void)DETECTOR_PITCH_CM;
+    (void)DETECTOR_PITCH_CM_AT_ISO_CENT; (void)DIST_BTWN_SRC_AND_ISOCENT_CM;
+    (void)DETECTOR_PIXEL_NUM; (void)x_reg; (void)y_reg; (void)z_reg;
+    std::lock_guard<std::mutex> lk(g_ref_mu);
+    vcbct_projector* p = g_ref_proj;
+    if (!p) {
+        std::fprintf(stderr, "reprojectionOnGPU: initializeGPU was not called\n");
+        return;
+    }
+    // the geometry set by initializeGPU is the one used (as the reference's
+    // __constant__ memory); the counts here must agree with it
+    if (reconSize != p->g.recon_size || reconSlices != p->g.recon_slices ||
+        projImgWidth != p->g.proj_width || projImgHeight != p->g.proj_height ||
+        num_material != p->g.num_material || endProjNumber <= 0 || endProjNumber > p->g.n_views) {
+        std::fprintf(stderr, "reprojectionOnGPU: arguments disagree with initializeGPU\n");
+        return;
+    }
+    const int V = endProjNumber;  // views 0..endProjNumber-1, as the launch grid (:976)
+    const int saveV = p->g.n_views;
+    p->g.n_views = V;
+    p->pp.V = V;
+    int rc = vcbct_projector_set_spectrum(p, Attenuation, pdf_pe, NE, xfactor);
+    if (!rc) rc = vcbct_projector_load_volume(p, reconImageshort, 0, nullptr);
+    std::vector<float> out((size_t)V * projImgHeight * projImgWidth);
+    if (!rc) rc = vcbct_projector_forward(p, out.data(), 0, nullptr);
+    p->g.n_views = saveV;
+    p->pp.V = saveV;
+    if (rc) {
+        std::fprintf(stderr, "reprojectionOnGPU: %s\n", vcbct_last_error());
+        return;
+    }
+    char fname[512];
+    std::snprintf(fname, sizeof fname, "%s.raw", outputname ? outputname : "reprojection");
+    FILE* f = std::fopen(fname, "wb");
+    if (!f) {
+        std::fprintf(stderr, "reprojectionOnGPU: cannot write %s\n", fname);
+        return;
+    }
+    std::fwrite(out.data(), sizeof(float), out.size(), f);
+    std::fclose(f);
+}
+
+// ======================================================================= FDK
+
+struct vcbct_fdk {
+    vcbct_fdk_geometry g;
+    FdkParams fp;
+    std::vector<double> angles, xs, ys, h;  // host copies
+    DevBuf hT;        // float [W][W]
+    DevBuf fviews;    // FilterView[V]
+    DevBuf bviews;    // BpView[V]
+    DevBuf wts;       // float [V][W] redundancy weights (optional)
+    DevBuf in, mid, outv, outs, work;
+    int have_wts = 0;
+};
+
+extern "C" void vcbct_fdk_default_geometry(vcbct_fdk_geometry* g)
+{
+    if (!g) return;
+    std::memset(g, 0, sizeof *g);
+    // R/physParams.h:22-41 and the shipped FDK txt (FDK_36pro_water20cm.txt)
+    g->proj_width = 400;
+    g->proj_height = 400;
+    g->n_views = 36;
+    g->recon_size = 270;
+    g->recon_slices = 50;
+    g->zstart = -5;
+    g->recon_step = 0.2;
+    g->recon_scale = 0.1;
+    g->xfactor = 1000;
+    g->det_pitch_iso_cm = 0.032509752;
+    g->det_pitch_cm = 0.05;
+    g->max_pic_num = 800;
+    g->sad_cm = 100.0;
+    g->cutoff = 1.60;
+    g->gamma = 1.00;
+    g->alpha = 0.50;
+    g->redundancy = 0;
+}
+
+// Ramp kernel h[m][n] of prepareConstMap (filterSinogram.cpp:21-62): a
+// band-limited Ram-Lak/Hamming-type kernel with cutoff CUTOFF_FREQ and
+// window ALPHA, GAMMA; zero on the diagonal.
+static void ramp_kernel(int W, double piso, double mpn, double cutoff, double gam, double alpha,
+                        double* h)
+{
+    const double c0 = 1.0 / (8.0 * kPi * kPi * piso * mpn / W);
+    const double gc = gam * cutoff, pc = kPi * cutoff, oma = 1.0 - alpha;
+    const double om = kPi / gam, co = std::cos(om), so = std::sin(om);
+    for (int m = 0; m < W; m++)
+        for (int n = 0; n < W; n++) {
+            if (m == n) {
+                h[(size_t)m * W + n] = 0.0;
+                continue;
+            }
+            const double d = (double)(m - n);
+            const double th = pc * d, de = gc * d;
+            const double eta = 1.0 / (1.0 - 1.0 / de), xi = 1.0 / (1.0 + 1.0 / de);
+            const double ct = std::cos(th), st = std::sin(th);
+            h[(size_t)m * W + n] = c0 / d / d *
+                (2.0 * alpha * th * st + 2.0 * alpha * (ct - 1.0) +
+                 xi * oma * th * (st * co + ct * so) + eta * oma * th * (st * co - ct * so) +
+                 xi * xi * oma * (ct * co - st * so - 1.0) +
+                 eta * eta * oma * (ct * co + st * so - 1.0));
+        }
+}
+
+static double filter_coeff(const vcbct_fdk_geometry& g)
+{
+    // filterSinogram.cpp:79-80
+    const double om = kPi / g.gamma;
+    return g.cutoff * g.cutoff / 4.0 / (g.det_pitch_iso_cm * g.max_pic_num / g.proj_width) *
+           (g.alpha * 0.5 + (1.0 - g.alpha) * (1.0 / om * std::sin(om) + 1.0 / om / om * (std::cos(om) - 1.0)));
+}
+
+static int upload_kernel(vcbct_fdk* f)
+{
+    const int W = f->g.proj_width;
+    const double coeff = filter_coeff(f->g);
+    std::vector<float> hT((size_t)W * W);
+    for (int k = 0; k < W; k++)
+        for (int m = 0; m < W; m++)
+            hT[(size_t)k * W + m] = (float)(f->h[(size_t)m * W + k] + (m == k ? coeff : 0.0));
+    VCBCT_CUDA_TRY(f->hT.ensure(hT.size() * sizeof(float)));
+    VCBCT_CUDA_TRY(cudaMemcpy(f->hT.p, hT.data(), hT.size() * sizeof(float), cudaMemcpyHostToDevice));
+    return VCBCT_OK;
+}
+
+// Redundancy weights for an offset (half-fan) detector over a full rotation
+// (Wang, Med. Phys. 29 (2002) 1464): with u the lateral column position at
+// the isocentre and u0 the half-width of the band seen from both sides of the
+// rotation axis, w = 2 sin^2(pi/4 (1 + u/u0)) inside the band, 2 on the long
+// side beyond it and 0 beyond the short edge, so conjugate rays sum to 2 and
+// the 2*pi angular integral stays normalised.  Not in the reference, which
+// has only the offset terms of Cm and UUU.
+static void halffan_weights(const vcbct_fdk& f, std::vector<float>& w)
+{
+    const int W = f.g.proj_width, V = f.g.n_views;
+    const double pitch = f.g.det_pitch_iso_cm * f.g.max_pic_num / W;
+    const double px = f.g.det_pitch_cm * f.g.max_pic_num / W;
+    w.assign((size_t)V * W, 1.0f);
+    for (int v = 0; v < V; v++) {
+        const double xcs = -W / 2.0 - f.xs[v] / px - 1;
+        const double umin = xcs * pitch, umax = (xcs + W - 1) * pitch;
+        const double u0 = std::fmin(-umin, umax);
+        if (!(u0 > 0)) continue;
+        const double side = (umax >= -umin) ? 1.0 : -1.0;  // +1: long side at +u
+        for (int m = 0; m < W; m++) {
+            const double x = side * (xcs + m) * pitch / u0;
+            double wt;
+            if (x >= 1.0) wt = 2.0;
+            else if (x <= -1.0) wt = 0.0;
+            else {
+                const double sn = std::sin(kPi / 4.0 * (1.0 + x));
+                wt = 2.0 * sn * sn;
+            }
+            w[(size_t)v * W + m] = (float)wt;
+        }
+    }
+}
+
+extern "C" int vcbct_fdk_create(const vcbct_fdk_geometry* g, const double* angles,
+                                const double* xshift, const double* yshift, vcbct_fdk** out)
+{
+    if (!out) return fail(VCBCT_ERR_ARG, "out is NULL");
+    *out = nullptr;
+    if (!g || !angles || !xshift || !yshift) return fail(VCBCT_ERR_ARG, "NULL argument");
+    if (g->proj_width <= 1 || g->proj_height <= 1 || g->n_views < 2 || g->recon_size <= 0 ||
+        g->recon_slices <= 0)
+        return fail(VCBCT_ERR_ARG, "FDK sizes must be positive (at least 2 views)");
+    if (!(g->det_pitch_iso_cm > 0) || !(g->det_pitch_cm > 0) || !(g->max_pic_num > 0) || !(g->sad_cm > 0))
+        return fail(VCBCT_ERR_ARG, "FDK pitches and distances must be positive");
+    auto* f = new vcbct_fdk();
+    f->g = *g;
+    const int V = g->n_views, W = g->proj_width;
+    f->angles.assign(angles, angles + V);
+    f->xs.assign(xshift, xshift + V);
+    f->ys.assign(yshift, yshift + V);
+    f->fp = FdkParams{g->proj_width, g->proj_height, V, g->recon_size, g->recon_slices, g->zstart,
+                      g->xfactor, g->redundancy, g->recon_step, g->recon_scale, g->det_pitch_iso_cm,
+                      g->det_pitch_cm, g->max_pic_num, g->sad_cm};
+    f->h.resize((size_t)W * W);
+    ramp_kernel(W, g->det_pitch_iso_cm, g->max_pic_num, g->cutoff, g->gamma, g->alpha, f->h.data());
+    int rc = upload_kernel(f);
+    if (rc) {
+        delete f;
+        return rc;
+    }
+    std::vector<FilterView> fv(V);
+    std::vector<BpView> bv(V);
+    const double px = g->det_pitch_cm * g->max_pic_num / W;
+    for (int th = 0; th < V; th++) {
+        // filterSinogram.cpp:86-87 (the height shift also uses the width)
+        fv[th].xcs = (float)(-W / 2.0 - f->xs[th] / px - 1);
+        fv[th].ycs = (float)(-W / 2.0 - f->ys[th] / px - 1);
+        // reconstructImage.cpp:37-72
+        double dbeta;
+        if (th == 0) dbeta = std::fabs(angles[1] - angles[0]) / 2;
+        else if (th == V - 1) dbeta = std::fabs(angles[th] - angles[th - 1]) / 2;
+        else {
+            const double t0 = angles[th - 1], t2 = angles[th + 1];
+            double t1 = angles[th + 1] - 2 * kPi;
+            if (t2 < 0) t1 = angles[th + 1] + 2 * kPi;
+            dbeta = std::fabs(t2 - t0) / 2;
+            if (dbeta > kPi / 2) dbeta = std::fabs(t1 - t0) / 2;
+        }
+        bv[th].cs = std::cos(angles[th]);
+        bv[th].sn = std::sin(angles[th]);
+        bv[th].ushift = (double)(W / 2) + f->xs[th] / px - 0.5;
+        bv[th].dbeta = (float)dbeta;
+        bv[th].pad = 0.0f;
+    }
+    cudaError_t e = f->fviews.ensure(sizeof(FilterView) * V);
+    if (e == cudaSuccess) e = cudaMemcpy(f->fviews.p, fv.data(), sizeof(FilterView) * V, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = f->bviews.ensure(sizeof(BpView) * V);
+    if (e == cudaSuccess) e = cudaMemcpy(f->bviews.p, bv.data(), sizeof(BpView) * V, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && g->redundancy == 1) {
+        std::vector<float> w;
+        halffan_weights(*f, w);
+        e = f->wts.ensure(w.size() * sizeof(float));
+        if (e == cudaSuccess) e = cudaMemcpy(f->wts.p, w.data(), w.size() * sizeof(float), cudaMemcpyHostToDevice);
+        f->have_wts = 1;
+    }
+    if (e != cudaSuccess) {
+        delete f;
+        return cuda_fail(e, "vcbct_fdk_create");
+    }
+    *out = f;
+    return VCBCT_OK;
+}
+
+extern "C" int vcbct_fdk_destroy(vcbct_fdk* f)
+{
+    if (!f) return VCBCT_OK;
+    f->hT.release(); f->fviews.release(); f->bviews.release(); f->wts.release();
+    f->in.release(); f->mid.release(); f->outv.release(); f->outs.release(); f->work.release();
+    delete f;
+    return VCBCT_OK;
+}
+
+extern "C" int vcbct_fdk_set_kernel(vcbct_fdk* f, const double* h)
+{
+    if (!f || !h) return fail(VCBCT_ERR_ARG, "NULL argument");
+    f->h.assign(h, h + (size_t)f->g.proj_width * f->g.proj_width);
+    return upload_kernel(f);
+}
+
+extern "C" int vcbct_fdk_filter(vcbct_fdk* f, const float* proj, float* filtered, int on_device,
+                                int method, void* stream)
+{
+    if (!f || !proj || !filtered) return fail(VCBCT_ERR_ARG, "NULL argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    const auto& g = f->g;
+    const size_t n = (size_t)g.n_views * g.proj_height * g.proj_width;
+    const float* din = proj;
+    float* dout = filtered;
+    if (!on_device) {
+        VCBCT_CUDA_TRY(f->in.ensure(n * sizeof(float)));
+        VCBCT_CUDA_TRY(f->mid.ensure(n * sizeof(float)));
+        VCBCT_CUDA_TRY(cudaMemcpyAsync(f->in.p, proj, n * sizeof(float), cudaMemcpyHostToDevice, st));
+        din = f->in.as<float>();
+        dout = f->mid.as<float>();
+    }
+    const float pitch = (float)(g.det_pitch_iso_cm * g.max_pic_num / g.proj_width);
+    const float* w = f->have_wts ? f->wts.as<float>() : nullptr;
+    if (method == VCBCT_FILTER_DIRECT_F32) {
+        VCBCT_CUDA_TRY(launch_filter_direct(din, dout, f->hT.as<float>(), f->fviews.as<FilterView>(), w,
+                                            pitch, (float)g.sad_cm, g.n_views, g.proj_height,
+                                            g.proj_width, st));
+    } else if (method == VCBCT_FILTER_BF16X3) {
+        VCBCT_CUDA_TRY(f->work.ensure(ramp_gemm_workspace_bytes(g.n_views, g.proj_height, g.proj_width)));
+        VCBCT_CUDA_TRY(launch_ramp_gemm_bf16x3(din, dout, f->hT.as<float>(), f->fviews.as<FilterView>(), w,
+                                               pitch, (float)g.sad_cm, g.n_views, g.proj_height,
+                                               g.proj_width, f->work.p, st));
+    } else {
+        return fail(VCBCT_ERR_ARG, "unknown filter method");
+    }
+    if (!on_device) {
+        VCBCT_CUDA_TRY(cudaMemcpyAsync(filtered, dout, n * sizeof(float), cudaMemcpyDeviceToHost, st));
+        VCBCT_CUDA_TRY(cudaStreamSynchronize(st));
+    }
+    return VCBCT_OK;
+}
+
+extern "C" int vcbct_fdk_backproject(vcbct_fdk* f, const float* filtered, float* vol_f32,
+                                     short* vol_i16, int on_device, void* stream)
+{
+    if (!f || !filtered || (!vol_f32 && !vol_i16)) return fail(VCBCT_ERR_ARG, "NULL argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    const auto& g = f->g;
+    const size_t np = (size_t)g.n_views * g.proj_height * g.proj_width;
+    const size_t nv = (size_t)g.recon_slices * g.recon_size * g.recon_size;
+    const float* din = filtered;
+    float* df = vol_f32;
+    short* di = vol_i16;
+    if (!on_device) {
+        VCBCT_CUDA_TRY(f->in.ensure(np * sizeof(float)));
+        VCBCT_CUDA_TRY(cudaMemcpyAsync(f->in.p, filtered, np * sizeof(float), cudaMemcpyHostToDevice, st));
+        din = f->in.as<float>();
+        if (vol_f32) {
+            VCBCT_CUDA_TRY(f->outv.ensure(nv * sizeof(float)));
+            df = f->outv.as<float>();
+        }
+        if (vol_i16) {
+            VCBCT_CUDA_TRY(f->outs.ensure(nv * sizeof(short)));
+            di = f->outs.as<short>();
+        }
+    }
+    VCBCT_CUDA_TRY(launch_backproject(f->fp, f->bviews.as<BpView>(), din, df, di, st));
+    if (!on_device) {
+        if (vol_f32) VCBCT_CUDA_TRY(cudaMemcpyAsync(vol_f32, df, nv * sizeof(float), cudaMemcpyDeviceToHost, st));
+        if (vol_i16) VCBCT_CUDA_TRY(cudaMemcpyAsync(vol_i16, di, nv * sizeof(short), cudaMemcpyDeviceToHost, st));
+        VCBCT_CUDA_TRY(cudaStreamSynchronize(st));
+    }
+    return VCBCT_OK;
+}
+
+// ------------------------------------------------- reference-named FDK API --
+
+extern "C" double** prepareConstMap(int projWidth, double piso)
+{
+    if (projWidth <= 0) {
+        std::fprintf(stderr, "ERROR: invalid projWidth for prepareConstMap\n");
+        return nullptr;
+    }
+    // VOLUME-ONE 2D layout (mallocMD.cpp:47-67): contiguous data + row table
+    double* data = (double*)std::calloc((size_t)projWidth * projWidth, sizeof(double));
+    double** rows = (double**)std::malloc(sizeof(double*) * projWidth);
+    if (!data || !rows) {
+        std::free(data);
+        std::free(rows);
+        std::fprintf(stderr, "ERROR: not enough memory for prepareConstMap\n");
+        return nullptr;
+    }
+    for (int j = 0; j < projWidth; j++) rows[j] = data + (size_t)j * projWidth;
+    vcbct_fdk_geometry g;
+    vcbct_fdk_default_geometry(&g);
+    ramp_kernel(projWidth, piso, g.max_pic_num, g.cutoff, g.gamma, g.alpha, data);
+    return rows;
+}
+
+extern "C" void vcbct_free_const_map(double** m, int projWidth)
+{
+    (void)projWidth;
+    if (!m) return;
+    std::free(m[0]);
+    std::free(m);
+}
+
+extern "C" void filterSinogram(int projHeight, int projWidth, int sngrmHeight, float*** projVolume,
+                               float*** fltdVoxData, double** constMap, double* xshift,
+                               double* yshift, double piso)
+{
+    if (!fltdVoxData || !projVolume || !constMap) {
+        std::fprintf(stderr, "ERROR: fltdVoxData is NULL\n");
+        return;
+    }
+    vcbct_fdk_geometry g;
+    vcbct_fdk_default_geometry(&g);
+    g.proj_width = projWidth;
+    g.proj_height = projHeight;
+    g.n_views = sngrmHeight;
+    g.det_pitch_iso_cm = piso;
+    std::vector<double> ang(sngrmHeight > 1 ? sngrmHeight : 2, 0.0);
+    for (size_t i = 0; i < ang.size(); i++) ang[i] = (double)i;  // unused by the filter
+    std::vector<double> ys(yshift, yshift + sngrmHeight), xs(xshift, xshift + sngrmHeight);
+    if (sngrmHeight < 2) { xs.resize(2, 0.0); ys.resize(2, 0.0); g.n_views = 2; }
+    vcbct_fdk* f = nullptr;
+    int rc = vcbct_fdk_create(&g, ang.data(), xs.data(), ys.data(), &f);
+    if (!rc) rc = vcbct_fdk_set_kernel(f, constMap[0]);
+    if (!rc) {
+        f->g.n_views = sngrmHeight;
+        f->fp.V = sngrmHeight;
+        rc = vcbct_fdk_filter(f, &projVolume[0][0][0], &fltdVoxData[0][0][0], 0, VCBCT_FILTER_DIRECT_F32, nullptr);
+    }
+    if (rc) std::fprintf(stderr, "filterSinogram: %s\n", vcbct_last_error());
+    vcbct_fdk_destroy(f);
+}
+
+extern "C" void reconstructImage(int reconSize, int reconSlices, int zstart, double reconStep,
+                                 double reconScale, double*** reconVoxData, char** maskData,
+                                 int projHeight, int projWidth, int sngrmHeight,
+                                 float*** sngrmVoxData, int xfactor, double* anglesRad,
+                                 double* cosTable, double* sinTable, double* xshift, double piso)
+{
+    (void)cosTable; (void)sinTable;
+    if (!reconVoxData) {
+        std::fprintf(stderr, "ERROR: reconVoxData is NULL\n");
+        return;
+    }
+    vcbct_fdk_geometry g;
+    vcbct_fdk_default_geometry(&g);
+    g.proj_width = projWidth;
+    g.proj_height = projHeight;
+    g.n_views = sngrmHeight;
+    g.recon_size = reconSize;
+    g.recon_slices = reconSlices;
+    g.zstart = zstart;
+    g.recon_step = reconStep;
+    g.recon_scale = reconScale;
+    g.xfactor = xfactor;
+    g.det_pitch_iso_cm = piso;
+    std::vector<double> ys(sngrmHeight, 0.0);
+    vcbct_fdk* f = nullptr;
+    int rc = vcbct_fdk_create(&g, anglesRad, xshift, ys.data(), &f);
+    const size_t nv = (size_t)reconSlices * reconSize * reconSize;
+    std::vector<float> vol(nv);
+    if (!rc) rc = vcbct_fdk_backproject(f, &sngrmVoxData[0][0][0], vol.data(), nullptr, 0, nullptr);
+    vcbct_fdk_destroy(f);
+    if (rc) {
+        std::fprintf(stderr, "reconstructImage: %s\n", vcbct_last_error());
+        return;
+    }
+    double* dst = &reconVoxData[0][0][0];
+    for (int z = 0; z < reconSlices; z++)
+        for (int y = 0; y < reconSize; y++)
+            for (int x = 0; x < reconSize; x++) {
+                if (maskData && maskData[y][x] == 0) continue;
+                const size_t o = ((size_t)z * reconSize + y) * reconSize + x;
+                dst[o] += (double)vol[o];
+            }
+}

@@ -1,0 +1,199 @@
+// fdk.cu -- FDK ramp filter (direct FP32 path) and voxel-driven cone-beam
+// backprojection on sm_100a.
+//
+// Reference: Release_recon_from_forward_pro_float_CM/filterSinogram.cpp:67-131
+// and reconstructImage.cpp:10-184 (OpenMP CPU code).
+#include "internal.h"
+
+#include <climits>
+
+namespace vcbct {
+namespace {
+
+// ------------------------------------------------------------------ filter --
+// out[r][m] = Cm(v, n, m) * sum_k hT[k][m] * g[r][k],  g = -logf(p),  r = v*H + n,
+// where hT already holds the diagonal coefficient (filterSinogram.cpp:103) and
+// the ramp kernel (:106-110).  A 64x64 output tile per block, K tiles of 32;
+// each thread computes 4x4 outputs.  -logf is applied while staging the A tile
+// (the reference's log of a float is the float overload, :103/:108).
+constexpr int FT_M = 64, FT_N = 64, FT_K = 32;
+
+__global__ void __launch_bounds__(256) filter_direct_kernel(
+    const float* __restrict__ proj, float* __restrict__ out, const float* __restrict__ hT,
+    const FilterView* __restrict__ views, const float* __restrict__ wts, float pitch, float sad,
+    int V, int H, int W)
+{
+    __shared__ float As[FT_K][FT_M + 4];
+    __shared__ float Bs[FT_K][FT_N + 4];
+    const int M = V * H;
+    const int r0 = blockIdx.y * FT_M, c0 = blockIdx.x * FT_N;
+    const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+    float acc[4][4] = {};
+    for (int k0 = 0; k0 < W; k0 += FT_K) {
+        // stage A: 64 rows x 32 k  (g = -logf(p))
+        for (int i = threadIdx.x; i < FT_M * FT_K; i += 256) {
+            const int rr = i / FT_K, kk = i % FT_K;
+            const int r = r0 + rr, k = k0 + kk;
+            float g = 0.0f;
+            if (r < M && k < W) {
+                g = -logf(__ldg(proj + (size_t)r * W + k));
+                if (wts) g *= __ldg(wts + (size_t)(r / H) * W + k);
+            }
+            As[kk][rr] = g;
+        }
+        // stage B: 32 k x 64 cols of hT
+        for (int i = threadIdx.x; i < FT_K * FT_N; i += 256) {
+            const int kk = i / FT_N, cc = i % FT_N;
+            const int k = k0 + kk, c = c0 + cc;
+            Bs[kk][cc] = (k < W && c < W) ? __ldg(hT + (size_t)k * W + c) : 0.0f;
+        }
+        __syncthreads();
+#pragma unroll 8
+        for (int kk = 0; kk < FT_K; kk++) {
+            float a[4], b[4];
+#pragma unroll
+            for (int i = 0; i < 4; i++) a[i] = As[kk][ty * 4 + i];
+#pragma unroll
+            for (int i = 0; i < 4; i++) b[i] = Bs[kk][tx * 4 + i];
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+#pragma unroll
+                for (int jn = 0; jn < 4; jn++) acc[i][jn] = fmaf(a[i], b[jn], acc[i][jn]);
+        }
+        __syncthreads();
+    }
+    // epilogue: cosine factor Cm = D / sqrt(D^2 + pos1^2 + pos2^2) (:92-99)
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        const int r = r0 + ty * 4 + i;
+        if (r >= M) continue;
+        const int v = r / H, n = r - v * H;
+        const FilterView sh = views[v];
+        const float pos2 = fabsf(sh.ycs + (float)n) * pitch;
+#pragma unroll
+        for (int jn = 0; jn < 4; jn++) {
+            const int m = c0 + tx * 4 + jn;
+            if (m >= W) continue;
+            const float pos1 = fabsf(sh.xcs + (float)m) * pitch;
+            const float cm = sad / sqrtf(sad * sad + pos1 * pos1 + pos2 * pos2);
+            out[(size_t)r * W + m] = acc[i][jn] * cm;
+        }
+    }
+}
+
+// ----------------------------------------------------------- backprojection --
+// One thread per (x, y) voxel column and a chunk of ZB slices (register
+// accumulators).  Per (x, y, view) the detector column coordinate U, its
+// interpolation weight and the magnification are formed in FP64 (the floor
+// of U decides which two detector columns are read and must agree with the
+// reference); per slice the row coordinate ZETA is an exact integer base plus
+// an FP32 fractional offset.  Bilinear interpolation is manual FP32 with the
+// reference's edge rules and its weight quirk (the column weight is frac(U),
+// not frac(UUU), reconstructImage.cpp:80-83).
+template <int ZB>
+__global__ void __launch_bounds__(256) backproject_kernel(
+    FdkParams f, const BpView* __restrict__ views, const float* __restrict__ filt,
+    float* __restrict__ vol_f32, short* __restrict__ vol_i16)
+{
+    const int x = blockIdx.x * 32 + threadIdx.x;
+    const int y = blockIdx.y * 8 + threadIdx.y;
+    const int z0 = blockIdx.z * ZB;
+    if (x >= f.N || y >= f.N) return;
+    const double R = (double)(f.N - 1) / 2.0;
+    const bool inmask = ((double)y - R) * ((double)y - R) + ((double)x - R) * ((double)x - R) <= R * R;
+    float acc[ZB];
+#pragma unroll
+    for (int i = 0; i < ZB; i++) acc[i] = 0.0f;
+    if (inmask) {
+        const double cp = (double)f.N / 2.0 - 0.5;
+        const double xx = (x - cp) * f.scale;
+        const double yy = -(y - cp) * f.scale;
+        const double pitch = f.piso * f.mpn / f.W;
+        const double zz0 = f.zstart + z0 * f.step;
+        const int W = f.W, H = f.H;
+        for (int th = 0; th < f.V; th++) {
+            const BpView bv = views[th];
+            const double cs = bv.cs, sn = bv.sn;
+            // FP64 detector coordinates of this column (:76-83)
+            const double X = xx * cs + yy * sn;
+            const double Y = -xx * sn + yy * cs;
+            const double L2 = 1.0 - Y / f.sad;
+            const double g = 1.0 / (L2 * pitch);
+            const double U = X * g;
+            const double Uf = floor(U);
+            const float wu = (float)(U - Uf);
+            const double UUU = bv.ushift + U;
+            const int UU = (int)floor(UUU);
+            const double zeta0 = (double)(H / 2) + zz0 * g;
+            const double zf = floor(zeta0);
+            const int Zi = (int)zf;
+            const float Zf = (float)(zeta0 - zf);
+            const float dz = (float)(f.step * g);
+            const float w2 = (float)(1.0 / L2 / L2) * bv.dbeta * (float)f.xfactor;
+            if (UU < 0 || UU > W - 1) continue;
+            const bool lastc = (UU == W - 1);
+            const float cw0 = lastc ? 1.0f : 1.0f - wu;
+            const float cw1 = lastc ? 0.0f : wu;
+            const int UU1 = lastc ? UU : UU + 1;
+            const float* pv = filt + (size_t)th * H * W;
+#pragma unroll
+            for (int i = 0; i < ZB; i++) {
+                const float zfrac = fmaf((float)i, dz, Zf);
+                const float fl = floorf(zfrac);
+                const int NZ = Zi + (int)fl;
+                const float wz = zfrac - fl;
+                if (NZ < 0 || NZ > H - 1 || z0 + i >= f.Z) continue;
+                const bool lastr = (NZ == H - 1);
+                const float rw0 = lastr ? 1.0f : 1.0f - wz;
+                const float rw1 = lastr ? 0.0f : wz;
+                const int NZ1 = lastr ? NZ : NZ + 1;
+                const float* r0p = pv + (size_t)NZ * W;
+                const float* r1p = pv + (size_t)NZ1 * W;
+                const float s0 = fmaf(cw1, __ldg(r0p + UU1), cw0 * __ldg(r0p + UU));
+                const float s1 = fmaf(cw1, __ldg(r1p + UU1), cw0 * __ldg(r1p + UU));
+                acc[i] = fmaf(fmaf(rw1, s1, rw0 * s0), w2, acc[i]);
+            }
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < ZB; i++) {
+        const int z = z0 + i;
+        if (z >= f.Z) break;
+        const size_t o = ((size_t)z * f.N + y) * f.N + x;
+        if (vol_f32) vol_f32[o] = acc[i];
+        if (vol_i16) {
+            // (short) of the reconstructed value: truncation toward zero
+            // (R/main.cpp:184), saturated to the short range.
+            float a = fminf(fmaxf(acc[i], -32768.0f), 32767.0f);
+            vol_i16[o] = (short)__float2int_rz(a);
+        }
+    }
+}
+
+}  // namespace
+
+}  // namespace vcbct
+
+namespace vcbct {
+
+cudaError_t launch_filter_direct(const float* proj, float* out, const float* hT,
+                                 const FilterView* views, const float* wts, float pitch,
+                                 float sad, int V, int H, int W, cudaStream_t st)
+{
+    const int M = V * H;
+    dim3 grid((W + FT_N - 1) / FT_N, (M + FT_M - 1) / FT_M);
+    filter_direct_kernel<<<grid, 256, 0, st>>>(proj, out, hT, views, wts, pitch, sad, V, H, W);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_backproject(const FdkParams& f, const BpView* d_views, const float* filt,
+                               float* vol_f32, short* vol_i16, cudaStream_t st)
+{
+    constexpr int ZB = 16;
+    dim3 block(32, 8);
+    dim3 grid((f.N + 31) / 32, (f.N + 7) / 8, (f.Z + ZB - 1) / ZB);
+    backproject_kernel<ZB><<<grid, block, 0, st>>>(f, d_views, filt, vol_f32, vol_i16);
+    return cudaGetLastError();
+}
+
+}  // namespace vcbct

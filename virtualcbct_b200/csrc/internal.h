@@ -1,0 +1,114 @@
+// internal.h -- shared declarations of libvcbct's CUDA translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <string>
+
+#include "vcbct.h"
+
+namespace vcbct {
+
+// Thread-local error message behind vcbct_last_error().
+void set_error(const std::string& msg);
+int fail(int code, const std::string& msg);
+int cuda_fail(cudaError_t e, const char* what);
+
+#define VCBCT_CUDA_TRY(call)                                  \
+    do {                                                      \
+        cudaError_t e__ = (call);                             \
+        if (e__ != cudaSuccess) return ::vcbct::cuda_fail(e__, #call); \
+    } while (0)
+
+// Per-view geometry the projector kernels read (double, from the host
+// tables of prepareTrigonometricTable, misc.cpp:10-37).
+struct ViewGeom {
+    double cs, sn, xc, yc;
+};
+
+// Scalar projection geometry passed by value to the kernels.
+struct ProjParams {
+    int N, Z, W, H, V, nmat;
+    double s, step, pdet, piso, sad, dpn, xr, yr, zr;
+};
+
+// ---------------------------------------------------------------- MBFPA --
+// Packed volume: voxel (x, y, z) at index (y*N + x)*Z + z, one 16-byte record
+// of 8 uint16 element values (u16 form) or two 16-byte records of 8 floats
+// (f32 form).  Elements beyond nmat are zero.
+size_t packed_u16_bytes(int N, int Z);
+size_t packed_f32_bytes(int N, int Z);
+
+cudaError_t launch_pack_u16(const uint16_t* src, int N, int Z, int nmat, uint4* dst,
+                            cudaStream_t st);
+cudaError_t launch_pack_f32(const float* src, int N, int Z, int nmat, float4* dst,
+                            cudaStream_t st);
+cudaError_t launch_unpack_grad(const float4* packed, int N, int Z, int nmat, float* dst,
+                               cudaStream_t st);
+
+// Spectral table: per bin 8 floats mu_k(E)/xfactor (zero padded) + pdf.
+struct SpectrumDev {
+    const float4* mu8;  // [NE][2] float4
+    const float* pdf;   // [NE]
+    int NE;
+};
+
+struct ForwardArgs {
+    ProjParams p;
+    const ViewGeom* views;   // device [V]
+    SpectrumDev spec;
+    const uint4* vol_u16;    // packed (or nullptr)
+    const float4* vol_f32;   // packed (or nullptr)
+    float* out;              // [V][H][W] intensities (or nullptr)
+    float* L_out;            // [V][H][W][nmat] path integrals (or nullptr)
+    unsigned long long* seg_count;  // (or nullptr)
+    int* err_flag;           // device fault flag
+    int cols_per_block;
+};
+cudaError_t launch_forward(const ForwardArgs& a, cudaStream_t st);
+
+struct AdjointArgs {
+    ProjParams p;
+    const ViewGeom* views;
+    SpectrumDev spec;
+    const float4* vol_f32;   // packed float volume
+    const float* grad_out;   // [V][H][W] d loss / d intensity
+    float4* grad_packed;     // packed [..][8] float accumulator
+    int* err_flag;
+    int cols_per_block;
+};
+cudaError_t launch_adjoint(const AdjointArgs& a, cudaStream_t st);
+
+// ------------------------------------------------------------------ FDK --
+struct FdkParams {
+    int W, H, V, N, Z, zstart, xfactor, redundancy;
+    double step, scale, piso, pdet, mpn, sad;
+};
+
+// Per-view filter constants: detector centre shifts of filterSinogram.cpp:86-87.
+struct FilterView {
+    float xcs, ycs;
+};
+// Direct FP32 ramp filter.  hT: [W][W] float, hT[k][m] = h[m][k] + coeff*(m==k).
+// wts: optional [V][W] redundancy weights applied to -log(p) before filtering.
+cudaError_t launch_filter_direct(const float* proj, float* out, const float* hT,
+                                 const FilterView* views, const float* wts, float pitch,
+                                 float sad, int V, int H, int W, cudaStream_t st);
+
+struct BpView {
+    double cs, sn;   // cos / sin of the view angle
+    double ushift;   // W/2 - 0.5 + xshift in pixels (reconstructImage.cpp:83)
+    float dbeta;     // half the neighbouring angular gap (:45-71)
+    float pad;
+};
+cudaError_t launch_backproject(const FdkParams& f, const BpView* d_views, const float* filt,
+                               float* vol_f32, short* vol_i16, cudaStream_t st);
+
+// BF16 3-term split tensor-core ramp filter (tcgen05).
+size_t ramp_gemm_workspace_bytes(int V, int H, int W);
+cudaError_t launch_ramp_gemm_bf16x3(const float* proj, float* out, const float* hT,
+                                    const FilterView* views, const float* wts, float pitch,
+                                    float sad, int V, int H, int W, void* workspace,
+                                    cudaStream_t st);
+
+}  // namespace vcbct

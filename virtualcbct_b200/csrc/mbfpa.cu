@@ -1,0 +1,761 @@
+// mbfpa.cu -- material-based polychromatic forward projection (MBFPA) on sm_100a.
+//
+// Reference: Release_CBCT_Projection_CM/reprojectionOnGPU.cu (reprojectionKernel,
+// :56-690, launched once per energy bin from :1004-1056).  This file keeps its
+// per-ray semantics -- the Siddon-style march with its discrete rules -- and
+// changes how the work maps to the GPU:
+//
+//  * one launch marches every ray once and accumulates the six per-element
+//    path integrals L_k; the spectral sum  leng * sum_E pdf_E exp(-sum_k
+//    mu_k(E) L_k / xfactor)  is formed in the same kernel (the reference
+//    re-marches every ray for each of ~100 bins and copies the whole stack to
+//    the host after each);
+//  * a warp is 32 consecutive detector rows of one column: those rays share
+//    their xy trajectory, so trip counts and x/y plane crossings are
+//    warp-uniform and only z crossings diverge;
+//  * the volume is re-laid out once into z-fastest 16-byte voxel records
+//    (all elements of a voxel in one vector load); the warp's loads at a step
+//    fall in one contiguous run of a z column;
+//  * FP64 is used only for the per-ray source/detector geometry, the
+//    entry/exit and loop-bound computation, and the parametric positions
+//    (Siddon alphas) of plane crossings.  The march itself is FP32, with
+//    voxel cells carried as integers plus a small fractional offset so that no
+//    FP32 value has to resolve a large coordinate near a plane.
+#include "internal.h"
+
+#include <cfloat>
+#include <climits>
+
+namespace vcbct {
+
+size_t packed_u16_bytes(int N, int Z) { return (size_t)N * N * Z * sizeof(uint4); }
+size_t packed_f32_bytes(int N, int Z) { return (size_t)N * N * Z * 2 * sizeof(float4); }
+
+namespace {
+
+// ---------------------------------------------------------------- FP64 ops --
+// Explicitly rounded double operations: nvcc may not contract these into
+// FMAs, so the setup reproduces the reference's double arithmetic bitwise.
+__device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double ddiv(double a, double b) { return __ddiv_rn(a, b); }
+__device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a, b); }
+
+// (a - a0)/(a1 - a0)*(b1 - b0) + b0, the reference's line evaluation (:159).
+__device__ __forceinline__ double line_at(double a, double a0, double a1, double b0, double b1)
+{
+    return dadd(dmul(ddiv(dsub(a, a0), dsub(a1, a0)), dsub(b1, b0)), b0);
+}
+
+// (int) cast of a double made total (non-finite / out of range -> INT_MIN).
+__device__ __forceinline__ int d2i(double v)
+{
+    if (!(v > -2147483648.0 && v < 2147483647.0)) return INT_MIN;
+    return __double2int_rz(v);
+}
+
+constexpr float kInf = 3.0e38f;
+
+// One axis of the march: value(t) = I + F + slope * (t - ta), in voxel (or
+// slice) units.  I is an integer cell base, F a small fraction.
+struct Axis {
+    int I;
+    float F;
+    float slope;
+    float ta;
+};
+
+__device__ __forceinline__ float axis_frac(const Axis& a, float t)
+{
+    return fmaf(a.slope, t - a.ta, a.F);
+}
+
+// Everything the FP32 march needs about one ray, produced by ray_setup().
+struct RayPlan {
+    int active;      // emits at least one segment
+    int d;           // dominant axis (0: x, 1: y)
+    int pha;         // +1 / -1 along the dominant axis
+    int kstar;       // last iteration index (iterations 0..kstar)
+    int klo, khi;    // iterations that can contribute (inclusive)
+    float tI;        // entry point parameter (<= 0)
+    float Lt;        // cm per unit of t
+    float leng;      // cos^3 factor (reprojectionOnGPU.cu:141-150)
+    double D0;       // dominant coordinate / s at t = 0
+    double O0, O1;   // other in-plane coordinate / s:  O0 + O1 t
+    double Z0, Z1;   // z / step:                        Z0 + Z1 t
+};
+
+// Per-ray FP64 setup: reprojectionOnGPU.cu:128-212, mirrored operation for
+// operation.  Rays that hit the xy square fewer than twice are defined to miss
+// (the reference reads uninitialised entries there).
+__device__ void ray_setup(const ProjParams& P, const ViewGeom& vg, int j, int jj, RayPlan& R)
+{
+    const double s = P.s, step = P.step;
+    const int nxm = (int)(P.N * 0.5), nym = (int)(P.N * 0.5), nzm = (int)(P.Z * 0.5);
+    double S[3], Pp[3];
+    S[0] = dadd(dmul(-P.sad, vg.sn), P.xr);
+    S[1] = dadd(dmul(P.sad, vg.cs), P.yr);
+    S[2] = P.zr;
+    const double bin = ddiv(P.dpn, (double)P.H);
+    Pp[2] = dadd(dmul(dmul(-dadd(vg.yc, (double)j), P.piso), bin), ddiv(dmul(P.zr, P.piso), P.pdet));
+    const double pr = dmul(dmul(P.piso, dadd(vg.xc, (double)jj)), bin);
+    Pp[0] = dadd(dmul(pr, vg.cs), ddiv(dmul(P.xr, P.piso), P.pdet));
+    Pp[1] = dadd(dmul(pr, vg.sn), ddiv(dmul(P.yr, P.piso), P.pdet));
+    {
+        const double d2 = dmul(P.sad, P.sad);
+        double l = ddiv(d2, dadd(d2, dadd(dmul(pr, pr), dmul(Pp[2], Pp[2]))));
+        R.leng = (float)dmul(l, __dsqrt_rn(l));
+    }
+    R.active = 0;
+    R.klo = INT_MAX;
+    R.khi = -1;
+
+    // entry / exit against the four side planes (:154-183)
+    const double hx = dmul((double)nxm, s), hy = dmul((double)nym, s);
+    double xx[4], yy[4], zz[4];
+    int m = 0;
+    yy[m] = hy;
+    if (fabs(line_at(yy[m], S[1], Pp[1], S[0], Pp[0])) < hx) {
+        xx[m] = line_at(yy[m], S[1], Pp[1], S[0], Pp[0]);
+        zz[m] = line_at(yy[m], S[1], Pp[1], S[2], Pp[2]);
+        m++;
+    }
+    yy[m] = -hy;
+    if (fabs(line_at(yy[m], S[1], Pp[1], S[0], Pp[0])) < hx) {
+        xx[m] = line_at(yy[m], S[1], Pp[1], S[0], Pp[0]);
+        zz[m] = line_at(yy[m], S[1], Pp[1], S[2], Pp[2]);
+        m++;
+    }
+    if (m < 4) {
+        xx[m] = hx;
+        if (fabs(line_at(xx[m], S[0], Pp[0], S[1], Pp[1])) < hy) {
+            yy[m] = line_at(xx[m], S[0], Pp[0], S[1], Pp[1]);
+            zz[m] = line_at(xx[m], S[0], Pp[0], S[2], Pp[2]);
+            m++;
+        }
+    }
+    if (m < 4) {
+        xx[m] = -hx;
+        if (fabs(line_at(xx[m], S[0], Pp[0], S[1], Pp[1])) < hy) {
+            yy[m] = line_at(xx[m], S[0], Pp[0], S[1], Pp[1]);
+            zz[m] = line_at(xx[m], S[0], Pp[0], S[2], Pp[2]);
+            m++;
+        }
+    }
+    if (m < 2) return;
+
+    double I[3], F[3];
+    {
+        double e0 = dadd(dadd(dmul(dsub(xx[0], S[0]), dsub(xx[0], S[0])),
+                              dmul(dsub(yy[0], S[1]), dsub(yy[0], S[1]))),
+                         dmul(dsub(zz[0], S[2]), dsub(zz[0], S[2])));
+        double e1 = dadd(dadd(dmul(dsub(xx[1], S[0]), dsub(xx[1], S[0])),
+                              dmul(dsub(yy[1], S[1]), dsub(yy[1], S[1]))),
+                         dmul(dsub(zz[1], S[2]), dsub(zz[1], S[2])));
+        const int f = (e0 < e1) ? 0 : 1;
+        I[0] = xx[f]; I[1] = yy[f]; I[2] = zz[f];
+        F[0] = xx[1 - f]; F[1] = yy[1 - f]; F[2] = zz[1 - f];
+    }
+    // dominant axis, GPU twin rule (:198)
+    const int d = (fabs(dsub(I[0], F[0])) > fabs(dsub(I[1], F[1]))) ? 0 : 1;
+    const int o = 1 - d;
+    const double dF = dsub(F[d], I[d]);
+    const double pha = ddiv(dF, fabs(dsub(I[d], F[d])));
+    if (!(pha == 1.0 || pha == -1.0)) return;
+    int ain;
+    if ((I[d] < 0 && dF < 0) || (I[d] > 0 && dF > 0))
+        ain = d2i(dadd((double)d2i(I[d]), ddiv(dF, fabs(dF))));
+    else
+        ain = d2i(I[d]);
+    if (ain == INT_MIN) return;
+
+    const double h = hx;  // hx == hy (both from reconSize)
+    auto inb = [&](double k) {
+        double a = dadd((double)ain, dmul(dmul(pha, k), s));
+        double ov = line_at(a, S[d], Pp[d], S[o], Pp[o]);
+        return a <= h && a >= -h && ov <= h && ov >= -h;
+    };
+    if (!inb(0.0)) return;
+
+    // first iteration whose step point leaves the box; the loop of the
+    // reference (:212) executes it and stops.
+    const double go = ddiv(dsub(Pp[o], S[o]), dsub(Pp[d], S[d]));
+    const double gz = ddiv(dsub(Pp[2], S[2]), dsub(Pp[d], S[d]));
+    const double o0 = line_at((double)ain, S[d], Pp[d], S[o], Pp[o]);
+    const double z0 = line_at((double)ain, S[d], Pp[d], S[2], Pp[2]);
+    double kd = floor((h - pha * ain) / s) + 1.0;
+    double ko = 1e30;
+    const double vo = go * pha * s;
+    if (vo > 0) ko = floor((h - o0) / vo) + 1.0;
+    else if (vo < 0) ko = floor((-h - o0) / vo) + 1.0;
+    double ke = fmin(kd, ko);
+    const int kcap = 4 * (P.N + 4) + (int)(8.0 / s) + 64;
+    if (!(ke >= 1.0)) ke = 1.0;
+    if (ke > kcap) ke = kcap;
+    int ks = (int)ke;
+    while (ks > 1 && !inb((double)(ks - 1))) ks--;
+    int guard = 0;
+    while (inb((double)ks) && guard < kcap) { ks++; guard++; }
+    R.kstar = ks;
+
+    R.d = d;
+    R.pha = (int)pha;
+    R.D0 = (double)ain / s;
+    R.O0 = o0 / s;
+    R.O1 = go * pha;
+    R.Z0 = z0 / step;
+    R.Z1 = gz * pha * s / step;
+    R.Lt = (float)(s * sqrt(1.0 + go * go + gz * gz));
+    R.tI = (float)((I[d] - (double)ain) / (pha * s));
+
+    // iterations whose segments can pass the cylinder mask and the z bounds
+    const double Rv = P.N * 0.5;
+    double A = 1.0 + R.O1 * R.O1;
+    double B = 2.0 * (R.D0 * pha + R.O0 * R.O1);
+    double C = R.D0 * R.D0 + R.O0 * R.O0 - Rv * Rv;
+    double disc = B * B - 4.0 * A * C;
+    if (!(disc > 0.0)) return;
+    double sq = sqrt(disc);
+    double tl = (-B - sq) / (2.0 * A), th = (-B + sq) / (2.0 * A);
+    const double zlo = (double)(nzm - P.Z), zhi = (double)(nzm + 1);  // (int) of zmc in [0, Z-1]
+    if (R.Z1 > 0) {
+        tl = fmax(tl, (zlo - R.Z0) / R.Z1);
+        th = fmin(th, (zhi - R.Z0) / R.Z1);
+    } else if (R.Z1 < 0) {
+        tl = fmax(tl, (zhi - R.Z0) / R.Z1);
+        th = fmin(th, (zlo - R.Z0) / R.Z1);
+    } else if (!(R.Z0 > zlo && R.Z0 < zhi)) {
+        return;
+    }
+    if (!(th > tl)) return;
+    int klo = (int)fmax(0.0, floor(tl) - 1.0);
+    int khi = (int)fmin((double)ks, floor(th) + 2.0);
+    if (khi < klo) return;
+    R.klo = klo;
+    R.khi = khi;
+    R.active = 1;
+}
+
+// Map a cell index to the reference's (int)-truncated voxel index: the value
+// lies in (q, q+1); q >= 0 -> q, q == -1 -> 0 (truncation toward zero), else
+// out of range.  Returns -1 when out of [0, size).
+__device__ __forceinline__ int trunc_index(int q, int size)
+{
+    return ((unsigned)(q + 1) <= (unsigned)size) ? max(q, 0) : -1;
+}
+
+// Anchor of an axis at parameter t (FP64 value v = c0 + c1 t).
+__device__ __forceinline__ Axis make_axis(double c0, double c1, double t)
+{
+    double v = c0 + c1 * t;
+    double fl = floor(v);
+    Axis a;
+    a.I = (int)fl;
+    a.F = (float)(v - fl);
+    a.slope = (float)c1;
+    a.ta = (float)t;
+    return a;
+}
+
+// Parameter of the crossing of plane `m` (FP64 Siddon alpha, as float).
+__device__ __forceinline__ float cross_t(double c0, double inv1, int m)
+{
+    return (float)(((double)m - c0) * inv1);
+}
+
+// The FP32 march of one ray (reprojectionOnGPU.cu:200-429 and its y-dominant
+// mirror :441-666).  `visit(ix, iy, iz, len)` is called for every segment
+// that passes the voxel-bounds test and the cylinder mask.
+template <class Visit>
+__device__ __forceinline__ void march(const ProjParams& P, const RayPlan& R, int Klo, int Khi,
+                                      Visit& visit)
+{
+    const int nxm = (int)(P.N * 0.5), nym = (int)(P.N * 0.5), nzm = (int)(P.Z * 0.5);
+    const float R2 = (float)(P.N * 0.5) * (float)(P.N * 0.5);
+    const int d = R.d;
+    const float fpha = (float)R.pha;
+    const double Dfl = floor(R.D0);
+    const int Id0 = (int)Dfl;
+    const float Fd = (float)(R.D0 - Dfl);
+
+    // o / z crossing bookkeeping (FP64 alphas)
+    const int diro = (R.O1 > 0) ? 1 : ((R.O1 < 0) ? -1 : 0);
+    const int dirz = (R.Z1 > 0) ? 1 : ((R.Z1 < 0) ? -1 : 0);
+    const double invO1 = diro ? 1.0 / R.O1 : 0.0;
+    const double invZ1 = dirz ? 1.0 / R.Z1 : 0.0;
+
+    const int ks = max(Klo, 1);
+    const double t0s = (double)(ks - 1);
+    Axis ao = make_axis(R.O0, R.O1, t0s);
+    Axis az = make_axis(R.Z0, R.Z1, t0s);
+    int mo = 0, mz = 0;
+    float to_next = kInf, tz_next = kInf;
+    if (diro) {
+        double v = R.O0 + R.O1 * t0s;
+        mo = (diro > 0) ? (int)floor(v) + 1 : (int)ceil(v) - 1;
+        to_next = cross_t(R.O0, invO1, mo);
+    }
+    if (dirz) {
+        double v = R.Z0 + R.Z1 * t0s;
+        mz = (dirz > 0) ? (int)floor(v) + 1 : (int)ceil(v) - 1;
+        if (mz == 0) mz += dirz;  // z = 0 is never a split plane (:237-238)
+        tz_next = cross_t(R.Z0, invZ1, mz);
+    }
+
+    // One segment [ta, tb] within the step whose start is t = tbase, where the
+    // dominant cell base is Idk.
+    auto segment = [&](float ta, float tb, float tbase, int Idk) {
+        const float tm = 0.5f * (ta + tb);
+        const float ud = fmaf(fpha, tm - tbase, Fd);
+        const float uo = axis_frac(ao, tm);
+        const float uz = axis_frac(az, tm);
+        const int cd = Idk + __float2int_rd(ud);
+        const int co = ao.I + __float2int_rd(uo);
+        const int cz = az.I + __float2int_rd(uz);
+        const float vd = (float)Idk + ud;
+        const float vo = (float)ao.I + uo;
+        const int cx = d ? co : cd;
+        const int cy = d ? cd : co;
+        const int ix = trunc_index(nxm + cx, P.N);
+        const int iy = trunc_index(nym - 1 - cy, P.N);
+        const int iz = trunc_index(nzm - 1 - cz, P.Z);
+        if ((ix | iy | iz) < 0) return;
+        if (!(fmaf(vd, vd, vo * vo) < R2)) return;
+        visit(ix, iy, iz, fabsf(tb - ta) * R.Lt);
+    };
+
+    if (Klo == 0 && R.kstar >= 0) {
+        // iteration 0: one unsplit segment from the entry point to the first
+        // step point (:405-427 with ik == 0)
+        segment(R.tI, 0.0f, 0.0f, Id0);
+    }
+    const int kcap = Khi;
+    for (int k = ks; k <= kcap; k++) {
+        const float tk = (float)k;
+        const float t0 = tk - 1.0f;
+        const int Idk = Id0 + R.pha * (k - 1);
+        const bool eo = to_next <= tk;
+        const bool ez = tz_next <= tk;
+        float tY = 0.0f, tZ = 0.0f;
+        if (eo) {
+            tY = to_next;
+            ao.I = mo; ao.F = 0.0f; ao.ta = tY;
+            mo += diro;
+            to_next = cross_t(R.O0, invO1, mo);
+        }
+        if (ez) {
+            // the reference splits only at the last z plane crossed in a step
+            int guard = 0;
+            do {
+                tZ = tz_next;
+                az.I = mz; az.F = 0.0f; az.ta = tZ;
+                mz += dirz;
+                if (mz == 0) mz += dirz;
+                tz_next = cross_t(R.Z0, invZ1, mz);
+            } while (tz_next <= tk && ++guard < 64);
+        }
+        // order of the split points: the one farther from the step point first
+        // (chz > chy, :249-404)
+        int ns = 0;
+        float a1 = tk, a2 = tk;
+        if (eo && ez) {
+            const float dY = tk - tY, dZ = tk - tZ;
+            if (dZ > dY) { a1 = tZ; a2 = tY; ns = 2; }
+            else if (dZ < dY) { a1 = tY; a2 = tZ; ns = 2; }
+        } else if (eo) {
+            if (tY != tk) { a1 = tY; ns = 1; }
+        } else if (ez) {
+            if (tZ != tk) { a1 = tZ; ns = 1; }
+        }
+        segment(t0, ns > 0 ? a1 : tk, t0, Idk);
+        if (ns > 0) segment(a1, ns > 1 ? a2 : tk, t0, Idk);
+        if (ns > 1) segment(a2, tk, t0, Idk);
+    }
+}
+
+// -------------------------------------------------------------- visitors --
+template <int M>
+struct AccumU16 {
+    const uint4* __restrict__ vol;
+    int N, Z;
+    float L[M];
+    float Lp[M];
+    unsigned nseg;
+    __device__ __forceinline__ void operator()(int ix, int iy, int iz, float len)
+    {
+        const uint4 v = __ldg(vol + ((size_t)(iy * N + ix) * Z + iz));
+        Lp[0] = fmaf((float)(v.x & 0xFFFFu), len, Lp[0]);
+        Lp[1] = fmaf((float)(v.x >> 16), len, Lp[1]);
+        Lp[2] = fmaf((float)(v.y & 0xFFFFu), len, Lp[2]);
+        Lp[3] = fmaf((float)(v.y >> 16), len, Lp[3]);
+        Lp[4] = fmaf((float)(v.z & 0xFFFFu), len, Lp[4]);
+        Lp[5] = fmaf((float)(v.z >> 16), len, Lp[5]);
+        if (M > 6) {
+            Lp[6 % M] = fmaf((float)(v.w & 0xFFFFu), len, Lp[6 % M]);
+            Lp[7 % M] = fmaf((float)(v.w >> 16), len, Lp[7 % M]);
+        }
+        nseg++;
+    }
+};
+
+template <int M>
+struct AccumF32 {
+    const float4* __restrict__ vol;
+    int N, Z;
+    float L[M];
+    float Lp[M];
+    unsigned nseg;
+    __device__ __forceinline__ void operator()(int ix, int iy, int iz, float len)
+    {
+        const float4* p = vol + 2 * ((size_t)(iy * N + ix) * Z + iz);
+        const float4 a = __ldg(p), b = __ldg(p + 1);
+        Lp[0] = fmaf(a.x, len, Lp[0]);
+        Lp[1] = fmaf(a.y, len, Lp[1]);
+        Lp[2] = fmaf(a.z, len, Lp[2]);
+        Lp[3] = fmaf(a.w, len, Lp[3]);
+        Lp[4] = fmaf(b.x, len, Lp[4]);
+        Lp[5] = fmaf(b.y, len, Lp[5]);
+        if (M > 6) {
+            Lp[6 % M] = fmaf(b.z, len, Lp[6 % M]);
+            Lp[7 % M] = fmaf(b.w, len, Lp[7 % M]);
+        }
+        nseg++;
+    }
+};
+
+struct Scatter {
+    float4* __restrict__ grad;
+    int N, Z;
+    float g[8];
+    __device__ __forceinline__ void operator()(int ix, int iy, int iz, float len)
+    {
+        float4* p = grad + 2 * ((size_t)(iy * N + ix) * Z + iz);
+        atomicAdd(p, make_float4(g[0] * len, g[1] * len, g[2] * len, g[3] * len));
+        atomicAdd(p + 1, make_float4(g[4] * len, g[5] * len, g[6] * len, g[7] * len));
+    }
+};
+
+// Two-level summation: the visitor accumulates into Lp; every 32 iterations
+// the partials are folded into L (bounds the FP32 error growth).
+template <class Acc, int M>
+__device__ __forceinline__ void march_accumulate(const ProjParams& P, const RayPlan& R, int Klo,
+                                                 int Khi, Acc& acc)
+{
+#pragma unroll
+    for (int i = 0; i < M; i++) { acc.L[i] = 0.0f; acc.Lp[i] = 0.0f; }
+    for (int k0 = Klo; k0 <= Khi; k0 += 32) {
+        const int k1 = min(Khi, k0 + 31);
+        march(P, R, k0, k1, acc);
+#pragma unroll
+        for (int i = 0; i < M; i++) { acc.L[i] += acc.Lp[i]; acc.Lp[i] = 0.0f; }
+    }
+}
+
+__device__ __forceinline__ void load_spectrum(const SpectrumDev& sp, float4* s_mu, float* s_pdf)
+{
+    for (int e = threadIdx.x + threadIdx.y * blockDim.x; e < sp.NE; e += blockDim.x * blockDim.y) {
+        s_mu[2 * e] = sp.mu8[2 * e];
+        s_mu[2 * e + 1] = sp.mu8[2 * e + 1];
+        s_pdf[e] = sp.pdf[e];
+    }
+}
+
+template <int M>
+__device__ __forceinline__ float spectral_sum(const float4* s_mu, const float* s_pdf, int NE,
+                                              const float* L)
+{
+    float acc = 0.0f;
+    for (int e = 0; e < NE; e++) {
+        const float4 a = s_mu[2 * e], b = s_mu[2 * e + 1];
+        float T = a.x * L[0];
+        T = fmaf(a.y, L[1], T);
+        T = fmaf(a.z, L[2], T);
+        T = fmaf(a.w, L[3], T);
+        T = fmaf(b.x, L[4], T);
+        T = fmaf(b.y, L[5], T);
+        if (M > 6) {
+            T = fmaf(b.z, L[6 % M], T);
+            T = fmaf(b.w, L[7 % M], T);
+        }
+        acc = fmaf(s_pdf[e], expf(-T), acc);
+    }
+    return acc;
+}
+
+// Warp-uniform iteration range: the union over the warp's lanes.
+__device__ __forceinline__ void warp_range(const RayPlan& R, bool valid, int& Klo, int& Khi)
+{
+    const int lo = (valid && R.active) ? R.klo : INT_MAX;
+    const int hi = (valid && R.active) ? R.khi : -1;
+    Klo = __reduce_min_sync(0xffffffffu, lo);
+    Khi = __reduce_max_sync(0xffffffffu, hi);
+}
+
+// grid: (ceil(W / cols_per_block), ceil(H / 32), V); block: (32, cols_per_block).
+template <int M, bool F32VOL, bool COUNT>
+__global__ void __launch_bounds__(256) forward_kernel(ForwardArgs a)
+{
+    extern __shared__ float4 smem[];
+    float4* s_mu = smem;
+    float* s_pdf = reinterpret_cast<float*>(smem + 2 * a.spec.NE);
+    load_spectrum(a.spec, s_mu, s_pdf);
+    __syncthreads();
+
+    const ProjParams& P = a.p;
+    const int lane = threadIdx.x;
+    const int jj = blockIdx.x * blockDim.y + threadIdx.y;  // detector column
+    if (jj >= P.W) return;                                 // whole warp exits together
+    const int j = blockIdx.y * 32 + lane;                  // detector row
+    const int v = blockIdx.z;
+    const bool valid = j < P.H;
+
+    const ViewGeom vg = a.views[v];
+    RayPlan R;
+    ray_setup(P, vg, j, jj, R);
+    int Klo, Khi;
+    warp_range(R, valid, Klo, Khi);
+
+    float L[M];
+    unsigned nseg = 0;
+    if (F32VOL) {
+        AccumF32<M> acc{a.vol_f32, P.N, P.Z, {}, {}, 0u};
+        if (Klo <= Khi && R.active) march_accumulate<AccumF32<M>, M>(P, R, Klo, Khi, acc);
+        else for (int i = 0; i < M; i++) acc.L[i] = 0.0f;
+#pragma unroll
+        for (int i = 0; i < M; i++) L[i] = acc.L[i];
+        nseg = acc.nseg;
+    } else {
+        AccumU16<M> acc{a.vol_u16, P.N, P.Z, {}, {}, 0u};
+        if (Klo <= Khi && R.active) march_accumulate<AccumU16<M>, M>(P, R, Klo, Khi, acc);
+        else for (int i = 0; i < M; i++) acc.L[i] = 0.0f;
+#pragma unroll
+        for (int i = 0; i < M; i++) L[i] = acc.L[i];
+        nseg = acc.nseg;
+    }
+    if (COUNT) {
+        unsigned tot = __reduce_add_sync(0xffffffffu, valid ? nseg : 0u);
+        if (lane == 0 && tot) atomicAdd(a.seg_count, (unsigned long long)tot);
+    }
+    if (!valid) return;
+    const size_t o = ((size_t)v * P.H + (P.H - 1 - j)) * P.W + jj;
+    if (a.L_out) {
+        for (int i = 0; i < P.nmat; i++) a.L_out[o * P.nmat + i] = L[i];
+    }
+    if (a.out) a.out[o] = spectral_sum<M>(s_mu, s_pdf, a.spec.NE, L) * R.leng;
+}
+
+template <int M>
+__global__ void __launch_bounds__(256) adjoint_kernel(AdjointArgs a)
+{
+    extern __shared__ float4 smem[];
+    float4* s_mu = smem;
+    float* s_pdf = reinterpret_cast<float*>(smem + 2 * a.spec.NE);
+    load_spectrum(a.spec, s_mu, s_pdf);
+    __syncthreads();
+
+    const ProjParams& P = a.p;
+    const int lane = threadIdx.x;
+    const int jj = blockIdx.x * blockDim.y + threadIdx.y;
+    if (jj >= P.W) return;
+    const int j = blockIdx.y * 32 + lane;
+    const int v = blockIdx.z;
+    const bool valid = j < P.H;
+    const ViewGeom vg = a.views[v];
+    RayPlan R;
+    ray_setup(P, vg, j, jj, R);
+    float r = 0.0f;
+    if (valid) r = a.grad_out[((size_t)v * P.H + (P.H - 1 - j)) * P.W + jj];
+    int Klo, Khi;
+    // rays with a zero residual do not scatter
+    warp_range(R, valid && r != 0.0f, Klo, Khi);
+    if (Klo > Khi) return;
+
+    // pass 1: recompute the per-element path integrals of this ray
+    AccumF32<M> acc{a.vol_f32, P.N, P.Z, {}, {}, 0u};
+    if (R.active) march_accumulate<AccumF32<M>, M>(P, R, Klo, Khi, acc);
+    else for (int i = 0; i < M; i++) acc.L[i] = 0.0f;
+
+    // d I / d L_k = -leng * sum_E pdf_E mu'_k(E) exp(-sum_k mu'_k(E) L_k)
+    float g[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int e = 0; e < a.spec.NE; e++) {
+        const float4 m0 = s_mu[2 * e], m1 = s_mu[2 * e + 1];
+        float T = m0.x * acc.L[0];
+        T = fmaf(m0.y, acc.L[1], T);
+        T = fmaf(m0.z, acc.L[2], T);
+        T = fmaf(m0.w, acc.L[3], T);
+        T = fmaf(m1.x, acc.L[4], T);
+        T = fmaf(m1.y, acc.L[5], T);
+        if (M > 6) {
+            T = fmaf(m1.z, acc.L[6 % M], T);
+            T = fmaf(m1.w, acc.L[7 % M], T);
+        }
+        const float w = s_pdf[e] * expf(-T);
+        g[0] = fmaf(w, m0.x, g[0]); g[1] = fmaf(w, m0.y, g[1]);
+        g[2] = fmaf(w, m0.z, g[2]); g[3] = fmaf(w, m0.w, g[3]);
+        g[4] = fmaf(w, m1.x, g[4]); g[5] = fmaf(w, m1.y, g[5]);
+        g[6] = fmaf(w, m1.z, g[6]); g[7] = fmaf(w, m1.w, g[7]);
+    }
+    const float scale = -R.leng * r;
+    Scatter sc{a.grad_packed, P.N, P.Z, {}};
+#pragma unroll
+    for (int i = 0; i < 8; i++) sc.g[i] = g[i] * scale;
+    // pass 2: scatter along the same segments (lanes with r == 0 add zeros)
+    if (R.active && r != 0.0f) march(P, R, Klo, Khi, sc);
+}
+
+// ------------------------------------------------------- layout kernels --
+// Reference layout [Z][nmat][N][N] -> packed z-fastest records.
+// grid (ceil(N/32), N, ceil(Z/32)), block (32, 8).
+__global__ void pack_u16_kernel(const uint16_t* __restrict__ src, int N, int Z, int nmat,
+                                uint4* __restrict__ dst)
+{
+    __shared__ uint16_t tile[32][8][33];
+    const int x0 = blockIdx.x * 32, y = blockIdx.y, z0 = blockIdx.z * 32;
+    const size_t NN = (size_t)N * N;
+    for (int zz = threadIdx.y; zz < 32; zz += 8) {
+        const int z = z0 + zz, x = x0 + threadIdx.x;
+        for (int m = 0; m < 8; m++) {
+            uint16_t v = 0;
+            if (m < nmat && z < Z && x < N) v = src[((size_t)z * nmat + m) * NN + (size_t)y * N + x];
+            tile[zz][m][threadIdx.x] = v;
+        }
+    }
+    __syncthreads();
+    for (int xx = threadIdx.y; xx < 32; xx += 8) {
+        const int x = x0 + xx, z = z0 + threadIdx.x;
+        if (x >= N || z >= Z) continue;
+        const int zz = threadIdx.x;
+        uint4 r;
+        r.x = (uint32_t)tile[zz][0][xx] | ((uint32_t)tile[zz][1][xx] << 16);
+        r.y = (uint32_t)tile[zz][2][xx] | ((uint32_t)tile[zz][3][xx] << 16);
+        r.z = (uint32_t)tile[zz][4][xx] | ((uint32_t)tile[zz][5][xx] << 16);
+        r.w = (uint32_t)tile[zz][6][xx] | ((uint32_t)tile[zz][7][xx] << 16);
+        dst[((size_t)y * N + x) * Z + z] = r;
+    }
+}
+
+__global__ void pack_f32_kernel(const float* __restrict__ src, int N, int Z, int nmat,
+                                float4* __restrict__ dst)
+{
+    __shared__ float tile[32][8][33];
+    const int x0 = blockIdx.x * 32, y = blockIdx.y, z0 = blockIdx.z * 32;
+    const size_t NN = (size_t)N * N;
+    for (int zz = threadIdx.y; zz < 32; zz += 8) {
+        const int z = z0 + zz, x = x0 + threadIdx.x;
+        for (int m = 0; m < 8; m++) {
+            float v = 0.0f;
+            if (m < nmat && z < Z && x < N) v = src[((size_t)z * nmat + m) * NN + (size_t)y * N + x];
+            tile[zz][m][threadIdx.x] = v;
+        }
+    }
+    __syncthreads();
+    for (int xx = threadIdx.y; xx < 32; xx += 8) {
+        const int x = x0 + xx, z = z0 + threadIdx.x;
+        if (x >= N || z >= Z) continue;
+        const int zz = threadIdx.x;
+        float4* p = dst + 2 * (((size_t)y * N + x) * Z + z);
+        p[0] = make_float4(tile[zz][0][xx], tile[zz][1][xx], tile[zz][2][xx], tile[zz][3][xx]);
+        p[1] = make_float4(tile[zz][4][xx], tile[zz][5][xx], tile[zz][6][xx], tile[zz][7][xx]);
+    }
+}
+
+// packed float records -> [Z][nmat][N][N], accumulated (+=).
+__global__ void unpack_grad_kernel(const float4* __restrict__ src, int N, int Z, int nmat,
+                                   float* __restrict__ dst)
+{
+    __shared__ float tile[32][8][33];
+    const int x0 = blockIdx.x * 32, y = blockIdx.y, z0 = blockIdx.z * 32;
+    const size_t NN = (size_t)N * N;
+    for (int xx = threadIdx.y; xx < 32; xx += 8) {
+        const int x = x0 + xx, z = z0 + threadIdx.x;
+        float4 a = make_float4(0, 0, 0, 0), b = a;
+        if (x < N && z < Z) {
+            const float4* p = src + 2 * (((size_t)y * N + x) * Z + z);
+            a = p[0];
+            b = p[1];
+        }
+        const int zz = threadIdx.x;
+        tile[zz][0][xx] = a.x; tile[zz][1][xx] = a.y; tile[zz][2][xx] = a.z; tile[zz][3][xx] = a.w;
+        tile[zz][4][xx] = b.x; tile[zz][5][xx] = b.y; tile[zz][6][xx] = b.z; tile[zz][7][xx] = b.w;
+    }
+    __syncthreads();
+    for (int zz = threadIdx.y; zz < 32; zz += 8) {
+        const int z = z0 + zz, x = x0 + threadIdx.x;
+        if (z >= Z || x >= N) continue;
+        for (int m = 0; m < nmat; m++) dst[((size_t)z * nmat + m) * NN + (size_t)y * N + x] += tile[zz][m][threadIdx.x];
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_pack_u16(const uint16_t* src, int N, int Z, int nmat, uint4* dst, cudaStream_t st)
+{
+    dim3 grid((N + 31) / 32, N, (Z + 31) / 32), block(32, 8);
+    pack_u16_kernel<<<grid, block, 0, st>>>(src, N, Z, nmat, dst);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pack_f32(const float* src, int N, int Z, int nmat, float4* dst, cudaStream_t st)
+{
+    dim3 grid((N + 31) / 32, N, (Z + 31) / 32), block(32, 8);
+    pack_f32_kernel<<<grid, block, 0, st>>>(src, N, Z, nmat, dst);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_unpack_grad(const float4* packed, int N, int Z, int nmat, float* dst, cudaStream_t st)
+{
+    dim3 grid((N + 31) / 32, N, (Z + 31) / 32), block(32, 8);
+    unpack_grad_kernel<<<grid, block, 0, st>>>(packed, N, Z, nmat, dst);
+    return cudaGetLastError();
+}
+
+template <int M, bool F32VOL, bool COUNT>
+static cudaError_t launch_fwd_t(const ForwardArgs& a, cudaStream_t st)
+{
+    const int cpb = a.cols_per_block;
+    dim3 block(32, cpb);
+    dim3 grid((a.p.W + cpb - 1) / cpb, (a.p.H + 31) / 32, a.p.V);
+    size_t shm = (size_t)a.spec.NE * (2 * sizeof(float4) + sizeof(float));
+    auto k = forward_kernel<M, F32VOL, COUNT>;
+    if (shm > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
+        if (e != cudaSuccess) return e;
+    }
+    k<<<grid, block, shm, st>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_forward(const ForwardArgs& a, cudaStream_t st)
+{
+    const bool f32 = a.vol_f32 != nullptr;
+    const bool cnt = a.seg_count != nullptr;
+    if (a.p.nmat <= 6) {
+        if (f32) return cnt ? launch_fwd_t<6, true, true>(a, st) : launch_fwd_t<6, true, false>(a, st);
+        return cnt ? launch_fwd_t<6, false, true>(a, st) : launch_fwd_t<6, false, false>(a, st);
+    }
+    if (f32) return cnt ? launch_fwd_t<8, true, true>(a, st) : launch_fwd_t<8, true, false>(a, st);
+    return cnt ? launch_fwd_t<8, false, true>(a, st) : launch_fwd_t<8, false, false>(a, st);
+}
+
+template <int M>
+static cudaError_t launch_adj_t(const AdjointArgs& a, cudaStream_t st)
+{
+    const int cpb = a.cols_per_block;
+    dim3 block(32, cpb);
+    dim3 grid((a.p.W + cpb - 1) / cpb, (a.p.H + 31) / 32, a.p.V);
+    size_t shm = (size_t)a.spec.NE * (2 * sizeof(float4) + sizeof(float));
+    auto k = adjoint_kernel<M>;
+    if (shm > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
+        if (e != cudaSuccess) return e;
+    }
+    k<<<grid, block, shm, st>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_adjoint(const AdjointArgs& a, cudaStream_t st)
+{
+    return a.p.nmat <= 6 ? launch_adj_t<6>(a, st) : launch_adj_t<8>(a, st);
+}
+
+}  // namespace vcbct

@@ -1,0 +1,145 @@
+"""Host mirror of the MBFPA projector interface.
+
+``Projector`` owns a ``vcbct_projector`` handle (the state the reference keeps
+in file-scope globals after ``initializeGPU``, reprojectionOnGPU.cu:710-825)
+and exposes the forward projection, per-element path integrals, segment count
+and adjoint.  Buffers are numpy arrays (host) or CUDA torch tensors (device);
+device calls run on the current torch stream.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _native as N
+from .geometry import ProjGeometry
+
+
+def _is_torch_cuda(x) -> bool:
+    return hasattr(x, "is_cuda") and bool(x.is_cuda)
+
+
+def _stream_ptr(stream=None):
+    import torch
+    s = torch.cuda.current_stream() if stream is None else stream
+    return C.c_void_p(s.cuda_stream)
+
+
+def _dp(a):
+    return np.ascontiguousarray(a, np.float64).ctypes.data_as(C.POINTER(C.c_double))
+
+
+class Projector:
+    """Polychromatic material-based forward projector on one GPU."""
+
+    def __init__(self, geom: ProjGeometry, cos_table, sin_table, xcenter, ycenter):
+        self.geom = geom
+        self._keep = [np.ascontiguousarray(t, np.float64) for t in (cos_table, sin_table, xcenter, ycenter)]
+        for t in self._keep:
+            if t.shape[0] < geom.V:
+                raise ValueError("view tables shorter than the number of views")
+        h = C.c_void_p()
+        gc = geom.to_c()
+        L = N.lib()
+        N.check(L.vcbct_projector_create(C.byref(gc), *[t.ctypes.data_as(C.POINTER(C.c_double)) for t in self._keep],
+                                         C.byref(h)))
+        self._h = h
+        self.NE = 0
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            N.lib().vcbct_projector_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ------------------------------------------------------------- inputs --
+    def set_spectrum(self, mu, pdf, xfactor: float):
+        mu = np.ascontiguousarray(mu, np.float32)
+        pdf = np.ascontiguousarray(pdf, np.float32)
+        if mu.ndim != 2 or mu.shape[0] != self.geom.nmat or mu.shape[1] != pdf.shape[0]:
+            raise ValueError("mu must be [nmat][NE] and pdf [NE]")
+        N.check(N.lib().vcbct_projector_set_spectrum(self._h, mu.ctypes.data_as(C.POINTER(C.c_float)),
+                                                     pdf.ctypes.data_as(C.POINTER(C.c_float)),
+                                                     int(pdf.shape[0]), float(xfactor)))
+        self.NE = int(pdf.shape[0])
+
+    def _check_vol(self, vol, dtype_name):
+        g = self.geom
+        shape = (g.Z, g.nmat, g.N, g.N)
+        if tuple(vol.shape) != shape:
+            raise ValueError(f"volume must be {dtype_name} {shape}, got {tuple(vol.shape)}")
+
+    def load_volume(self, vol, stream=None):
+        """uint16 [Z][nmat][N][N] element volume (host numpy or CUDA torch)."""
+        self._check_vol(vol, "uint16")
+        L = N.lib()
+        if _is_torch_cuda(vol):
+            import torch
+            if vol.dtype not in (torch.uint16, torch.int16):
+                raise ValueError("device volume must be uint16/int16 bits")
+            v = vol.contiguous()
+            N.check(L.vcbct_projector_load_volume(self._h, C.c_void_p(v.data_ptr()), 1, _stream_ptr(stream)))
+            self._vol_ref = v
+        else:
+            v = np.ascontiguousarray(vol, np.uint16)
+            N.check(L.vcbct_projector_load_volume(self._h, C.c_void_p(v.ctypes.data), 0, None))
+
+    def load_volume_f32(self, vol, stream=None):
+        """float32 [Z][nmat][N][N] element volume (host numpy or CUDA torch)."""
+        self._check_vol(vol, "float32")
+        L = N.lib()
+        if _is_torch_cuda(vol):
+            v = vol.contiguous()
+            N.check(L.vcbct_projector_load_volume_f32(self._h, C.c_void_p(v.data_ptr()), 1, _stream_ptr(stream)))
+            self._vol_ref = v
+        else:
+            v = np.ascontiguousarray(vol, np.float32)
+            N.check(L.vcbct_projector_load_volume_f32(self._h, C.c_void_p(v.ctypes.data), 0, None))
+
+    # ------------------------------------------------------------ outputs --
+    def forward(self, out=None, stream=None):
+        """Spectral projection float [V][H][W].  With a CUDA torch ``out`` (or
+        out=None and torch available) the result stays on the device; with a
+        numpy ``out`` it is copied to the host."""
+        g = self.geom
+        L = N.lib()
+        if out is None:
+            import torch
+            out = torch.empty((g.V, g.H, g.W), dtype=torch.float32, device="cuda")
+        if _is_torch_cuda(out):
+            N.check(L.vcbct_projector_forward(self._h, C.c_void_p(out.data_ptr()), 1, _stream_ptr(stream)))
+        else:
+            if out.dtype != np.float32 or not out.flags.c_contiguous or out.size != g.V * g.H * g.W:
+                raise ValueError("host out must be contiguous float32 [V][H][W]")
+            N.check(L.vcbct_projector_forward(self._h, C.c_void_p(out.ctypes.data), 0, None))
+        return out
+
+    def path_integrals(self, stream=None):
+        import torch
+        g = self.geom
+        Lb = torch.empty((g.V, g.H, g.W, g.nmat), dtype=torch.float32, device="cuda")
+        N.check(N.lib().vcbct_projector_path_integrals(self._h, C.c_void_p(Lb.data_ptr()), _stream_ptr(stream)))
+        return Lb
+
+    def count_segments(self, stream=None) -> int:
+        tot = C.c_ulonglong(0)
+        N.check(N.lib().vcbct_projector_count_segments(self._h, C.byref(tot), _stream_ptr(stream)))
+        return int(tot.value)
+
+    def adjoint(self, grad_out, grad=None, stream=None):
+        """Accumulate d loss / d volume (float [Z][nmat][N][N], device) for a
+        device d loss / d projection ``grad_out`` [V][H][W]."""
+        import torch
+        g = self.geom
+        if grad is None:
+            grad = torch.zeros((g.Z, g.nmat, g.N, g.N), dtype=torch.float32, device="cuda")
+        go = grad_out.contiguous()
+        N.check(N.lib().vcbct_projector_adjoint(self._h, C.c_void_p(go.data_ptr()),
+                                                C.c_void_p(grad.data_ptr()), _stream_ptr(stream)))
+        return grad
