@@ -79,7 +79,9 @@ static void emit_segment(seg_ctx* c, const double* b0, const double* b1)
     double r = sqrt((b0[0] + b1[0]) * (b0[0] + b1[0]) +
                     (-b0[1] - b1[1]) * (-b0[1] - b1[1])) * 0.5;
     double ph = (r >= c->rmax) ? 0.0 : 1.0;
-    if (ph != 0.0) c->nm++;
+    /* the throughput unit: a segment that reads voxel data and contributes
+     * (zero-length segments, emitted at exact plane ties, are not counted) */
+    if (ph != 0.0 && rr > 0.0) c->nm++;
     const int64_t NN = (int64_t)g->N * g->N;
     for (int mat = 0; mat < g->nmat; mat++) {
         int64_t vnum = xmc + (int64_t)ymc * g->N + ((int64_t)zmc * g->nmat + mat) * NN;

@@ -68,7 +68,7 @@ enum {
  *   L_out    double [V][H][W][nmat] per-element path integrals, may be NULL
  *   nseg_bounds / nseg_mask  int64 per ray [V][H][W] (GPU layout index) of
  *            segments that passed the voxel-bounds test / also the cylinder
- *            mask, may be NULL
+ *            mask and have non-zero length (the throughput unit), may be NULL
  * Returns 0 on success.
  */
 int orc_mbfpa_forward(const orc_proj_geom* g,
@@ -133,8 +133,6 @@ void orc_mask(int N, char* mask);
 /*
  * reconstructImage.cpp:10-184.  vol double [Z][N][N] is accumulated (+=).
  * filt float [V][H][W] (filt_d double, used instead when non-NULL).
- * weights optional double [V][W] per-view, per-column multiplier (the
- * redundancy weights extension; NULL reproduces the reference).
  */
 void orc_backproject(int N, int Z, int zstart, double step, double scale,
                      double* vol, const char* mask, int H, int W, int V,

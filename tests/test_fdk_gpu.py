@@ -1,0 +1,73 @@
+"""FDK parity: the CUDA filter and backprojector (through the C ABI) against
+the reference's own filterSinogram / reconstructImage (oracle/_ref) and the
+FP64 oracle restatement, on seeded projections."""
+import numpy as np
+import pytest
+
+import oracle as O
+from virtualcbct_b200 import FILTER_DIRECT_F32, Fdk, FdkGeometry
+
+pytestmark = pytest.mark.gpu
+
+
+def _case(V=6, H=40, W=48, seed=0, N=27, Z=8, span=360.0, xshift=0.0):
+    rng = np.random.default_rng(seed)
+    # smooth positive "projections" in (0, 1]: a blurred random field
+    base = rng.uniform(0.05, 1.0, size=(V, H, W)).astype(np.float32)
+    k = np.ones(5) / 5
+    for ax in (1, 2):
+        base = np.apply_along_axis(lambda r: np.convolve(r, k, mode="same"), ax, base)
+    proj = np.clip(base, 0.02, 1.0).astype(np.float32)
+    ang = np.deg2rad(-180.0001 + np.arange(V) * span / V)
+    g = FdkGeometry(W=W, H=H, V=V, N=N, Z=Z, zstart=-3, step=0.5, scale=0.4)
+    xs = np.full(V, xshift)
+    return g, proj, ang, xs
+
+
+def test_filter_matches_reference(cuda):
+    if not O.have_reference():
+        pytest.skip("reference CPU objects not built")
+    g, proj, ang, xs = _case()
+    f = Fdk(g, ang, xs, np.zeros(g.V))
+    gpu = f.filter(proj, method=FILTER_DIRECT_F32)
+    ref, _ = O.ref_filter(proj, xs, np.zeros(g.V), g.piso)
+    d64 = O.filter_sinogram(proj, xs, np.zeros(g.V), O.fdk_consts(g.piso), mode=1)
+    scale = np.abs(d64).max()
+    # the reference itself accumulates in float; both sit within 1e-5 of the
+    # output scale of the FP64 filter
+    assert np.abs(ref - d64).max() <= 1e-5 * scale
+    assert np.abs(gpu - d64).max() <= 1e-5 * scale
+
+
+def test_filter_with_offset_detector(cuda):
+    g, proj, ang, xs = _case(xshift=3.0)
+    f = Fdk(g, ang, xs, np.zeros(g.V))
+    gpu = f.filter(proj)
+    d64 = O.filter_sinogram(proj, xs, np.zeros(g.V), O.fdk_consts(g.piso), mode=1)
+    assert np.abs(gpu - d64).max() <= 1e-5 * np.abs(d64).max()
+
+
+@pytest.mark.parametrize("xshift", [0.0, 2.0])
+def test_backprojection_matches_reference(cuda, xshift):
+    if not O.have_reference():
+        pytest.skip("reference CPU objects not built")
+    g, proj, ang, xs = _case(V=12, xshift=xshift)
+    filt, _ = O.ref_filter(proj, xs, np.zeros(g.V), g.piso)
+    f = Fdk(g, ang, xs, np.zeros(g.V))
+    vf, vi = f.backproject(filt)
+    ref, _ = O.ref_backproject(g.N, g.Z, g.zstart, g.step, g.scale, filt, g.xfactor, ang, xs, g.piso)
+    ref_i16 = ref.astype(np.int16)  # (short) truncation toward zero (R/main.cpp:184)
+    assert np.abs(vf - ref).max() <= 1e-5 * max(1.0, np.abs(ref).max())
+    assert np.abs(vi.astype(np.int32) - ref_i16.astype(np.int32)).max() <= 1
+
+
+def test_fdk_chain_short_volume_within_one_lsb(cuda):
+    if not O.have_reference():
+        pytest.skip("reference CPU objects not built")
+    g, proj, ang, xs = _case(V=24, H=48, W=64, N=40, Z=10, seed=3)
+    f = Fdk(g, ang, xs, np.zeros(g.V))
+    _, vi = f.reconstruct(proj)
+    filt, _ = O.ref_filter(proj, xs, np.zeros(g.V), g.piso)
+    ref, _ = O.ref_backproject(g.N, g.Z, g.zstart, g.step, g.scale, filt, g.xfactor, ang, xs, g.piso)
+    d = np.abs(vi.astype(np.int32) - ref.astype(np.int16).astype(np.int32))
+    assert d.max() <= 1, f"{(d > 1).sum()} voxels differ by more than 1 LSB"

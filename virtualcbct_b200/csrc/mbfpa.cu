@@ -76,8 +76,9 @@ struct RayPlan {
     int d;           // dominant axis (0: x, 1: y)
     int pha;         // +1 / -1 along the dominant axis
     int kstar;       // last iteration index (iterations 0..kstar)
-    int klo, khi;    // iterations that can contribute (inclusive)
-    float tI;        // entry point parameter (<= 0)
+    int klo, khi;    // iterations k >= 1 that can contribute (inclusive)
+    int first_idx;   // packed voxel of the first segment, or -1
+    float first_len; // its length [cm]
     float Lt;        // cm per unit of t
     float leng;      // cos^3 factor (reprojectionOnGPU.cu:141-150)
     double D0;       // dominant coordinate / s at t = 0
@@ -109,6 +110,8 @@ __device__ void ray_setup(const ProjParams& P, const ViewGeom& vg, int j, int jj
     R.active = 0;
     R.klo = INT_MAX;
     R.khi = -1;
+    R.first_idx = -1;
+    R.first_len = 0.0f;
 
     // entry / exit against the four side planes (:154-183)
     const double hx = dmul((double)nxm, s), hy = dmul((double)nym, s);
@@ -206,7 +209,34 @@ __device__ void ray_setup(const ProjParams& P, const ViewGeom& vg, int j, int jj
     R.Z0 = z0 / step;
     R.Z1 = gz * pha * s / step;
     R.Lt = (float)(s * sqrt(1.0 + go * go + gz * gz));
-    R.tI = (float)((I[d] - (double)ain) / (pha * s));
+    R.active = 1;
+
+    // Iteration 0 emits one unsplit segment from the entry point to the first
+    // step point (:405-427 with ik == 0).  It can span many voxels and its
+    // midpoint often lies exactly on a voxel plane (entry through a face), so
+    // its voxel, length and mask are evaluated in FP64 exactly as the
+    // reference does.
+    {
+        double b1[3];
+        b1[d] = (double)ain;
+        b1[o] = o0;
+        b1[2] = z0;
+        const double* b0 = I;
+        const double rr = __dsqrt_rn(dadd(dadd(dmul(dsub(b0[0], b1[0]), dsub(b0[0], b1[0])),
+                                               dmul(dsub(b0[1], b1[1]), dsub(b0[1], b1[1]))),
+                                          dmul(dsub(b0[2], b1[2]), dsub(b0[2], b1[2]))));
+        const int xmc = d2i(dadd(ddiv(dmul(dadd(b0[0], b1[0]), 0.5), s), (double)nxm));
+        const int ymc = d2i(dadd(ddiv(dmul(dsub(-b0[1], b1[1]), 0.5), s), (double)nym));
+        const int zmc = d2i(dadd(ddiv(dmul(dsub(-b0[2], b1[2]), 0.5), step), (double)nzm));
+        if (xmc >= 0 && ymc >= 0 && zmc >= 0 && xmc <= P.N - 1 && ymc <= P.N - 1 && zmc <= P.Z - 1) {
+            const double r = dmul(__dsqrt_rn(dadd(dmul(dadd(b0[0], b1[0]), dadd(b0[0], b1[0])),
+                                                  dmul(dsub(-b0[1], b1[1]), dsub(-b0[1], b1[1])))), 0.5);
+            if (!(r >= dmul(dmul((double)P.N, 0.5), s))) {
+                R.first_idx = (ymc * P.N + xmc) * P.Z + zmc;
+                R.first_len = (float)rr;
+            }
+        }
+    }
 
     // iterations whose segments can pass the cylinder mask and the z bounds
     const double Rv = P.N * 0.5;
@@ -228,12 +258,12 @@ __device__ void ray_setup(const ProjParams& P, const ViewGeom& vg, int j, int jj
         return;
     }
     if (!(th > tl)) return;
-    int klo = (int)fmax(0.0, floor(tl) - 1.0);
+    // iteration k >= 1 covers t in [k-1, k]; one step of margin each side
+    int klo = (int)fmax(1.0, floor(tl) - 1.0);
     int khi = (int)fmin((double)ks, floor(th) + 2.0);
     if (khi < klo) return;
     R.klo = klo;
     R.khi = khi;
-    R.active = 1;
 }
 
 // Map a cell index to the reference's (int)-truncated voxel index: the value
@@ -263,8 +293,9 @@ __device__ __forceinline__ float cross_t(double c0, double inv1, int m)
     return (float)(((double)m - c0) * inv1);
 }
 
-// The FP32 march of one ray (reprojectionOnGPU.cu:200-429 and its y-dominant
-// mirror :441-666).  `visit(ix, iy, iz, len)` is called for every segment
+// The FP32 march of iterations k in [Klo, Khi] (k >= 1) of one ray
+// (reprojectionOnGPU.cu:200-429 and its y-dominant mirror :441-666).
+// `visit(idx, len)` is called with the packed voxel index of every segment
 // that passes the voxel-bounds test and the cylinder mask.
 template <class Visit>
 __device__ __forceinline__ void march(const ProjParams& P, const RayPlan& R, int Klo, int Khi,
@@ -284,7 +315,7 @@ __device__ __forceinline__ void march(const ProjParams& P, const RayPlan& R, int
     const double invO1 = diro ? 1.0 / R.O1 : 0.0;
     const double invZ1 = dirz ? 1.0 / R.Z1 : 0.0;
 
-    const int ks = max(Klo, 1);
+    const int ks = Klo;
     const double t0s = (double)(ks - 1);
     Axis ao = make_axis(R.O0, R.O1, t0s);
     Axis az = make_axis(R.Z0, R.Z1, t0s);
@@ -321,14 +352,9 @@ __device__ __forceinline__ void march(const ProjParams& P, const RayPlan& R, int
         const int iz = trunc_index(nzm - 1 - cz, P.Z);
         if ((ix | iy | iz) < 0) return;
         if (!(fmaf(vd, vd, vo * vo) < R2)) return;
-        visit(ix, iy, iz, fabsf(tb - ta) * R.Lt);
+        visit((iy * P.N + ix) * P.Z + iz, fabsf(tb - ta) * R.Lt);
     };
 
-    if (Klo == 0 && R.kstar >= 0) {
-        // iteration 0: one unsplit segment from the entry point to the first
-        // step point (:405-427 with ik == 0)
-        segment(R.tI, 0.0f, 0.0f, Id0);
-    }
     const int kcap = Khi;
     for (int k = ks; k <= kcap; k++) {
         const float tk = (float)k;
@@ -381,9 +407,9 @@ struct AccumU16 {
     float L[M];
     float Lp[M];
     unsigned nseg;
-    __device__ __forceinline__ void operator()(int ix, int iy, int iz, float len)
+    __device__ __forceinline__ void operator()(int idx, float len)
     {
-        const uint4 v = __ldg(vol + ((size_t)(iy * N + ix) * Z + iz));
+        const uint4 v = __ldg(vol + idx);
         Lp[0] = fmaf((float)(v.x & 0xFFFFu), len, Lp[0]);
         Lp[1] = fmaf((float)(v.x >> 16), len, Lp[1]);
         Lp[2] = fmaf((float)(v.y & 0xFFFFu), len, Lp[2]);
@@ -405,9 +431,9 @@ struct AccumF32 {
     float L[M];
     float Lp[M];
     unsigned nseg;
-    __device__ __forceinline__ void operator()(int ix, int iy, int iz, float len)
+    __device__ __forceinline__ void operator()(int idx, float len)
     {
-        const float4* p = vol + 2 * ((size_t)(iy * N + ix) * Z + iz);
+        const float4* p = vol + 2 * (size_t)idx;
         const float4 a = __ldg(p), b = __ldg(p + 1);
         Lp[0] = fmaf(a.x, len, Lp[0]);
         Lp[1] = fmaf(a.y, len, Lp[1]);
@@ -427,9 +453,9 @@ struct Scatter {
     float4* __restrict__ grad;
     int N, Z;
     float g[8];
-    __device__ __forceinline__ void operator()(int ix, int iy, int iz, float len)
+    __device__ __forceinline__ void operator()(int idx, float len)
     {
-        float4* p = grad + 2 * ((size_t)(iy * N + ix) * Z + iz);
+        float4* p = grad + 2 * (size_t)idx;
         atomicAdd(p, make_float4(g[0] * len, g[1] * len, g[2] * len, g[3] * len));
         atomicAdd(p + 1, make_float4(g[4] * len, g[5] * len, g[6] * len, g[7] * len));
     }
@@ -443,6 +469,7 @@ __device__ __forceinline__ void march_accumulate(const ProjParams& P, const RayP
 {
 #pragma unroll
     for (int i = 0; i < M; i++) { acc.L[i] = 0.0f; acc.Lp[i] = 0.0f; }
+    if (R.first_idx >= 0) acc(R.first_idx, R.first_len);
     for (int k0 = Klo; k0 <= Khi; k0 += 32) {
         const int k1 = min(Khi, k0 + 31);
         march(P, R, k0, k1, acc);
@@ -519,14 +546,14 @@ __global__ void __launch_bounds__(256) forward_kernel(ForwardArgs a)
     unsigned nseg = 0;
     if (F32VOL) {
         AccumF32<M> acc{a.vol_f32, P.N, P.Z, {}, {}, 0u};
-        if (Klo <= Khi && R.active) march_accumulate<AccumF32<M>, M>(P, R, Klo, Khi, acc);
+        if (R.active) march_accumulate<AccumF32<M>, M>(P, R, Klo, Khi, acc);
         else for (int i = 0; i < M; i++) acc.L[i] = 0.0f;
 #pragma unroll
         for (int i = 0; i < M; i++) L[i] = acc.L[i];
         nseg = acc.nseg;
     } else {
         AccumU16<M> acc{a.vol_u16, P.N, P.Z, {}, {}, 0u};
-        if (Klo <= Khi && R.active) march_accumulate<AccumU16<M>, M>(P, R, Klo, Khi, acc);
+        if (R.active) march_accumulate<AccumU16<M>, M>(P, R, Klo, Khi, acc);
         else for (int i = 0; i < M; i++) acc.L[i] = 0.0f;
 #pragma unroll
         for (int i = 0; i < M; i++) L[i] = acc.L[i];
@@ -568,7 +595,7 @@ __global__ void __launch_bounds__(256) adjoint_kernel(AdjointArgs a)
     int Klo, Khi;
     // rays with a zero residual do not scatter
     warp_range(R, valid && r != 0.0f, Klo, Khi);
-    if (Klo > Khi) return;
+    if (!__any_sync(0xffffffffu, valid && r != 0.0f && R.active)) return;
 
     // pass 1: recompute the per-element path integrals of this ray
     AccumF32<M> acc{a.vol_f32, P.N, P.Z, {}, {}, 0u};
@@ -600,7 +627,10 @@ __global__ void __launch_bounds__(256) adjoint_kernel(AdjointArgs a)
 #pragma unroll
     for (int i = 0; i < 8; i++) sc.g[i] = g[i] * scale;
     // pass 2: scatter along the same segments (lanes with r == 0 add zeros)
-    if (R.active && r != 0.0f) march(P, R, Klo, Khi, sc);
+    if (R.active && r != 0.0f) {
+        if (R.first_idx >= 0) sc(R.first_idx, R.first_len);
+        if (Klo <= Khi) march(P, R, Klo, Khi, sc);
+    }
 }
 
 // ------------------------------------------------------- layout kernels --
