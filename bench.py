@@ -1,0 +1,368 @@
+#!/usr/bin/env python
+"""Benchmark of the MBFPA hot path (plus FDK) on synthetic data.
+
+Metric: MBFPA ray-voxel throughput in Gseg/s -- one "segment"
+is one in-volume, in-cylinder, non-degenerate segment of the reference's
+Siddon-style march that reads one voxel's six element values -- with FDK
+backprojection GUPS, the forward+adjoint / forward ratio and the CPU baseline
+reported beside it.
+
+Workload (one GPU): "Plain MBFPA + FDK at scale": 25 cm water cylinder,
+512x512x200 uint16 x 6 elements (0.5 x 0.5 x 2 mm), 360 views at 1 deg with the
+half-fan detector offset (xshift 1.6 in the projector flexmap = 160 px),
+400x400 float32 projections, a 100 kV filtered-Kramers spectrum in 1 keV bins
+(90 bins); FDK to 270x270x200 (1 mm) with cosine + half-fan weights + ramp.
+All inputs are seeded synthetic data in the reference's formats.
+
+A step = one forward projection of the whole stack (every ray, every bin).
+`value` is measured with the volume resident in HBM; `e2e` repeats the step
+through the C ABI with pinned host buffers (volume upload + re-layout +
+projection + download inside the timed region).
+
+Usage:  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+For N > 1 run under torch.distributed.run: every rank projects its own copy
+of the workload (weak scaling, no data-path collective).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+DATA = os.path.join(ROOT, "virtualcbct_b200", "data")
+MINIDB = os.path.join(DATA, "xraydb_mini")
+
+METRIC = "MBFPA ray-voxel Gseg/s & FDK GUPS; batched vs plain; grad-step/fwd ratio @stated err"
+
+# DRAM traffic of one forward launch of this workload, from
+# profiles/mbfpa_forward_c2.md (ncu dram__bytes_read.sum + dram__bytes_write.sum,
+# scaled from the captured case as documented there).  None until captured.
+FORWARD_DRAM_BYTES = None
+
+
+def workload():
+    from virtualcbct_b200 import ProjGeometry, FdkGeometry, attenuation_table, phantoms
+    N, Z, s, step = 512, 200, 0.05, 0.2
+    V, W, H = 360, 400, 400
+    g = ProjGeometry(N=N, Z=Z, s=s, step=step, W=W, H=H, V=V)
+    angles_deg = phantoms.view_angles(V, -180.0001)
+    xs_proj = np.full(V, 1.6)          # projector flexmap (x100 px, misc.cpp:31)
+    xs_fdk = np.full(V, 16.0)          # FDK flexmap (x10 px, filterSinogram.cpp:86)
+    vol = phantoms.water_cylinder(N, Z, s, 12.5)
+    mu, pdf = attenuation_table(os.path.join(DATA, "spectrum_kramers100_90.csv"), MINIDB, 6)
+    fg = FdkGeometry(W=W, H=H, V=V, N=270, Z=200, zstart=-20, step=0.2, scale=0.1,
+                     redundancy=1)
+    return dict(g=g, angles_deg=angles_deg, xs_proj=xs_proj, xs_fdk=xs_fdk, vol=vol, mu=mu,
+                pdf=pdf, fg=fg, xfactor=1000.0,
+                name="25 cm water cylinder 512x512x200x6 u16 (0.5x0.5x2 mm), 360 views/1 deg, "
+                     "half-fan 160 px, 400x400 f32, 90-bin 100 kV; FDK 270x270x200")
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    def __init__(self, index: int):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={index}", f"--query-gpu={q}",
+                                       "--format=csv,noheader,nounits", "-lms", "100"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        rows = [r.split(",") for r in open(self.f.name).read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm = [float(r[1]) for r in rows if len(r) >= 9 and r[1].strip().isdigit()]
+        mx = [float(r[2]) for r in rows if len(r) >= 9 and r[2].strip().isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in rows:
+            if len(r) < 9:
+                continue
+            for n, v in zip(names, r[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def cpu_reference_sample(w, views, bins, nthreads):
+    """Time the reference's own CPU projector (oracle/_ref) on (views x bins)."""
+    import oracle as O
+    from virtualcbct_b200 import trig_tables
+    g = w["g"]
+    ang = np.deg2rad(w["angles_deg"])
+    tabs = trig_tables(g.W, g.H, ang, w["xs_proj"], np.zeros(g.V), g.pdet, g.dpn)
+    _, secs = O.ref_mbfpa_views(g, tabs, w["vol"], w["mu"], w["pdf"], w["xfactor"], views, bins,
+                                nthreads=nthreads)
+    return secs
+
+
+def segments_per_view_cpu(w, views):
+    """Segment count of the sampled views from the CPU oracle (the unit's
+    definition); used by the reference arm, which must not touch the GPU."""
+    import oracle as O
+    from virtualcbct_b200 import trig_tables
+    g = w["g"]
+    ang = np.deg2rad(w["angles_deg"])
+    tabs = trig_tables(g.W, g.H, ang, w["xs_proj"], np.zeros(g.V), g.pdet, g.dpn)
+    r = O.mbfpa_forward(g, tabs, w["vol"], w["mu"][:, :1], w["pdf"][:1], w["xfactor"],
+                        views=views, exact=False, want=("nm",))
+    return {int(v): int(r["nm"][v].sum()) for v in views}
+
+
+def run_reference(args, rank, world):
+    """Reference arm: the reference's CPU projector (reprojection.cpp compiled
+    from its sources, driven per view and bin over all host threads) on a
+    bounded sample of the workload each step; Gseg/s over the full job."""
+    if rank != 0:
+        return
+    import oracle as O
+    w = workload()
+    g = w["g"]
+    if not O.have_reference():
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "oracle/_ref (reference CPU code compiled from its sources) is not built"}))
+        return
+    ncores = os.cpu_count() or 1
+    NE = int(w["pdf"].shape[0])
+    nviews = max(1, min(g.V, ncores))
+    rng = np.random.default_rng(0)
+    seg_cache = {}
+    times, segs = [], []
+    for it in range(args.warmup + args.steps):
+        views = np.sort(rng.choice(g.V, size=nviews, replace=False)).astype(np.int32)
+        bins = np.array([rng.integers(NE)], np.int32)
+        need = [v for v in views if v not in seg_cache]
+        if need:
+            seg_cache.update(segments_per_view_cpu(w, np.array(need, np.int32)))
+        t = cpu_reference_sample(w, views, bins, ncores)
+        if it >= args.warmup:
+            times.append(t)
+            segs.append(sum(seg_cache[int(v)] for v in views) * len(bins))
+    # one sampled (view, bin) call re-marches the view's rays for one bin;
+    # the full job is V x NE such calls over the whole stack's segments.
+    per_seg = np.sum(times) / np.sum(segs)           # s per segment per bin
+    total_segs = np.mean([seg_cache[v] for v in seg_cache]) * g.V
+    full_time = per_seg * total_segs * NE
+    value = total_segs / full_time / 1e9
+    ms = full_time * 1e3
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "Gseg/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": w["name"], "sample": f"{nviews} views x 1 bin per step",
+                   "parallelism": f"cpu{ncores}"},
+        "cpu_baseline": {"value": value, "unit": "Gseg/s", "cores": ncores, "kind": "reference",
+                         "sample": f"{nviews} views x 1 of {NE} bins per step, extrapolated to "
+                                   f"{g.V} views x {NE} bins"},
+        "e2e": {"value": value, "unit": "Gseg/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import virtualcbct_b200 as vc
+    from virtualcbct_b200 import Fdk, Projector, trig_tables
+
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    w = workload()
+    g = w["g"]
+    ang = np.deg2rad(w["angles_deg"])
+    tabs = trig_tables(g.W, g.H, ang, w["xs_proj"], np.zeros(g.V), g.pdet, g.dpn)
+    P = Projector(g, *tabs)
+    P.set_spectrum(w["mu"], w["pdf"], w["xfactor"])
+    vol_h = torch.from_numpy(w["vol"].view(np.int16)).pin_memory()
+    vol_d = vol_h.to(dev)
+    P.load_volume(vol_d)
+    out = torch.empty((g.V, g.H, g.W), dtype=torch.float32, device=dev)
+    nseg = P.count_segments()
+    stream = torch.cuda.current_stream()
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    def max_over_ranks(x):
+        if world > 1:
+            t = torch.tensor([x], dtype=torch.float64, device=dev)
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            return float(t.item())
+        return x
+
+    # ---- device-resident step
+    for _ in range(max(3, args.warmup)):
+        P.forward(out)
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local_rank)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        P.forward(out)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    barrier()
+    ms = max_over_ranks(e0.elapsed_time(e1) / args.steps)
+    value = nseg * world / (ms * 1e-3) / 1e9
+
+    # ---- end-to-end through the C ABI with pinned host buffers
+    out_h = torch.empty((g.V, g.H, g.W), dtype=torch.float32).pin_memory()
+    out_np = out_h.numpy()
+    vol_np = vol_h.numpy().view(np.uint16)
+    lib = vc.lib()
+    import ctypes as C
+    h = P._h
+    sp = C.c_void_p(stream.cuda_stream)
+
+    def e2e_step():
+        vc._native.check(lib.vcbct_projector_load_volume(h, C.c_void_p(vol_np.ctypes.data), 0, sp))
+        vc._native.check(lib.vcbct_projector_forward(h, C.c_void_p(out_np.ctypes.data), 0, sp))
+
+    for _ in range(2):
+        e2e_step()
+    torch.cuda.synchronize()
+    barrier()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for _ in range(args.steps):
+        e2e_step()
+    t1.record(stream)
+    torch.cuda.synchronize()
+    ms_e2e = max_over_ranks(t0.elapsed_time(t1) / args.steps)
+    e2e = nseg * world / (ms_e2e * 1e-3) / 1e9
+    P.load_volume(vol_d)
+
+    # ---- FDK on the projections just made (device resident)
+    fg = w["fg"]
+    F = Fdk(fg, ang, w["xs_fdk"], np.zeros(fg.V))
+    P.forward(out)
+    method = vc.FILTER_DIRECT_F32
+    filt = F.filter(out, method=method)
+    vf, vi = F.backproject(filt)
+    for _ in range(2):
+        F.filter(out, method=method)
+        F.backproject(filt)
+    torch.cuda.synchronize()
+    a0, a1, a2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    a0.record(stream)
+    for _ in range(args.steps):
+        F.filter(out, filt, method=method)
+    a1.record(stream)
+    for _ in range(args.steps):
+        F.backproject(filt)
+    a2.record(stream)
+    torch.cuda.synchronize()
+    ms_filter = a0.elapsed_time(a1) / args.steps
+    ms_bp = a1.elapsed_time(a2) / args.steps
+    gups = fg.N * fg.N * fg.Z * fg.V / (ms_bp * 1e-3) / 1e9
+
+    peak, peak_kind = measured_peaks()
+    alg_bytes = 12.0 * nseg
+    achieved = alg_bytes / (ms * 1e-3) / 1e9
+    res = {
+        "metric": METRIC, "value": value, "unit": "Gseg/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": w["name"], "segments_per_step": nseg, "parallelism": f"replica{world}",
+                   "l2": "inputs larger than L2 (packed volume 839 MB)"},
+        "e2e": {"value": e2e, "unit": "Gseg/s", "ms_per_step": ms_e2e,
+                "h2d_bytes_per_step": int(vol_np.nbytes), "d2h_bytes_per_step": int(out_np.nbytes)},
+        "gpu_launches": args.steps * 1,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": peak_kind,
+                     "traffic": FORWARD_DRAM_BYTES,
+                     "note": "achieved = 12 B (6 x uint16) per segment / forward launch time"},
+        "fdk": {"filter_ms": ms_filter, "filter_method": "direct_f32", "bp_ms": ms_bp,
+                "bp_gups": gups, "short_volume_range": [int(vi.min().item()), int(vi.max().item())]},
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            ncores = os.cpu_count() or 1
+            nviews = max(1, min(g.V, ncores))
+            views = np.arange(0, g.V, max(1, g.V // nviews))[:nviews].astype(np.int32)
+            bins = np.array([w["pdf"].shape[0] // 2], np.int32)
+            secs = cpu_reference_sample(w, views, bins, ncores)
+            per_view = nseg / g.V
+            full = secs * (g.V / len(views)) * w["pdf"].shape[0]
+            res["cpu_baseline"] = {"value": nseg / full / 1e9, "unit": "Gseg/s", "cores": ncores,
+                                   "kind": "reference",
+                                   "sample": f"reprojection() on {len(views)} views x 1 of "
+                                             f"{w['pdf'].shape[0]} bins ({secs:.1f} s), "
+                                             f"extrapolated to {g.V} views x all bins",
+                                   "segments_per_view": per_view}
+        except Exception as e:  # the baseline is informative, never fatal
+            res["cpu_baseline"] = {"value": None, "unit": "Gseg/s", "cores": os.cpu_count(),
+                                   "kind": "reference", "sample": f"unavailable: {e}"}
+    if rank == 0:
+        print(json.dumps(res))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        torch.cuda.set_device(local_rank)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    try:
+        run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch
+            torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()
