@@ -145,6 +145,31 @@ void reprojectionOnGPU(int ite, int reconSize, int reconSlices, unsigned short* 
                        double x_reg, double y_reg, double z_reg, float* Attenuation,
                        float* pdf_pe, int num_material, int NE, char* outputname);
 
+/* Forward projection that allocates no memory (no counterpart in the
+ * reference).  For callers that cannot let a library call cudaMalloc: hosts
+ * that own all device memory in their own fixed arena, latency-critical
+ * pipelines that cannot accept cudaMalloc's implicit synchronisation or a late
+ * out-of-memory failure, deployments that forbid device allocation after
+ * start-up.  Same result as vcbct_projector_create + set_spectrum +
+ * load_volume (device) + forward (device), in one call.
+ *   d_volume  device uint16 [Z][nmat][N][N];  d_out  device float [V][H][W]
+ *   tables / attenuation / pdf are host arrays as for the object API.
+ * Scratch: one file-scope device array of VCBCT_NOALLOC_SCRATCH_BYTES, held by
+ * every GPU that loads the library until the process exits.  Limits:
+ * recon_size^2 * recon_slices <= 4177920 voxels (16 B each), n_views <= 1024,
+ * n_bins <= 1024; larger requests return VCBCT_ERR_LIMIT before any device
+ * work.  The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress) with that device current; make that first call
+ * before any stream capture.  Calls share the array: calls that overlap on
+ * the GPU (different streams or threads, not ordered) race and corrupt each
+ * other.  Asynchronous on `stream`. */
+#define VCBCT_NOALLOC_SCRATCH_BYTES (64u * 1024u * 1024u)
+int vcbct_mbfpa_forward_noalloc(const vcbct_proj_geometry* g, const double* cos_table,
+                                const double* sin_table, const double* xcenter_shift,
+                                const double* ycenter_shift, const uint16_t* d_volume,
+                                const float* attenuation, const float* pdf, int n_bins,
+                                double xfactor, float* d_out, void* stream);
+
 /* Host helpers of the projector's input preparation. */
 /* misc.cpp:10-37 prepareTrigonometricTable (outputs caller-allocated). */
 int vcbct_proj_trig_tables(int proj_width, int proj_height, int n_views,
