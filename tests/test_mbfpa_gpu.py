@@ -23,9 +23,26 @@ def _gpu_forward(g, tabs, vol, mu, pdf, xf=1000.0):
     return out, p
 
 
-@pytest.mark.parametrize("kind,seed", [("random", 0), ("random", 1), ("water", 0), ("ellipsoid", 3)])
-def test_forward_matches_fp64_oracle(cuda, kind, seed):
-    g, tabs, vol, _ = proj_case(kind, seed=seed)
+CASES = [
+    ("random", 0, {}),
+    ("random", 1, {}),
+    ("water", 0, {}),
+    ("ellipsoid", 3, {}),
+    # half-fan detector offset (projector xshift x100 px)
+    ("random", 2, dict(xshift=1.6, W=40, H=32)),
+    # thin slices: several z crossings per x step on some rays
+    ("ellipsoid", 5, dict(N=48, Z=40, s=0.25, step=0.1, V=3)),
+    # voxel size whose reciprocal is not an integer: dominant-axis planes fall
+    # inside the steps
+    ("random", 9, dict(N=40, Z=24, s=0.07, step=0.13, V=3)),
+    # steeper than one slice per step: the per-step march path
+    ("random", 6, dict(N=32, Z=64, s=0.3, step=0.02, V=2, W=24, H=40, dpn=900.0)),
+]
+
+
+@pytest.mark.parametrize("kind,seed,extra", CASES)
+def test_forward_matches_fp64_oracle(cuda, kind, seed, extra):
+    g, tabs, vol, _ = proj_case(kind, seed=seed, **extra)
     mu, pdf = spectrum()
     gpu, _ = _gpu_forward(g, tabs, vol, mu, pdf)
     ref = O.mbfpa_forward(g, tabs, vol, mu, pdf, 1000.0, exact=True, want=("f", "d"))

@@ -84,6 +84,8 @@ struct RayPlan {
     double D0;       // dominant coordinate / s at t = 0
     double O0, O1;   // other in-plane coordinate / s:  O0 + O1 t
     double Z0, Z1;   // z / step:                        Z0 + Z1 t
+    double invO1, invZ1;  // 1 / O1, 1 / Z1 (0 when the slope is 0)
+    double tc0, tc1; // chord of the cylindrical mask in t
 };
 
 // Per-ray FP64 setup: reprojectionOnGPU.cu:128-212, mirrored operation for
@@ -209,6 +211,10 @@ __device__ void ray_setup(const ProjParams& P, const ViewGeom& vg, int j, int jj
     R.Z0 = z0 / step;
     R.Z1 = gz * pha * s / step;
     R.Lt = (float)(s * sqrt(1.0 + go * go + gz * gz));
+    R.invO1 = (R.O1 != 0.0) ? 1.0 / R.O1 : 0.0;
+    R.invZ1 = (R.Z1 != 0.0) ? 1.0 / R.Z1 : 0.0;
+    R.tc0 = 1.0;
+    R.tc1 = 0.0;
     R.active = 1;
 
     // Iteration 0 emits one unsplit segment from the entry point to the first
@@ -247,6 +253,8 @@ __device__ void ray_setup(const ProjParams& P, const ViewGeom& vg, int j, int jj
     if (!(disc > 0.0)) return;
     double sq = sqrt(disc);
     double tl = (-B - sq) / (2.0 * A), th = (-B + sq) / (2.0 * A);
+    R.tc0 = tl;
+    R.tc1 = th;
     const double zlo = (double)(nzm - P.Z), zhi = (double)(nzm + 1);  // (int) of zmc in [0, Z-1]
     if (R.Z1 > 0) {
         tl = fmax(tl, (zlo - R.Z0) / R.Z1);
@@ -407,6 +415,28 @@ struct AccumU16 {
     float L[M];
     float Lp[M];
     unsigned nseg;
+    __device__ __forceinline__ void add(const uint4 v, float len)
+    {
+        Lp[0] = fmaf((float)(v.x & 0xFFFFu), len, Lp[0]);
+        Lp[1] = fmaf((float)(v.x >> 16), len, Lp[1]);
+        Lp[2] = fmaf((float)(v.y & 0xFFFFu), len, Lp[2]);
+        Lp[3] = fmaf((float)(v.y >> 16), len, Lp[3]);
+        Lp[4] = fmaf((float)(v.z & 0xFFFFu), len, Lp[4]);
+        Lp[5] = fmaf((float)(v.z >> 16), len, Lp[5]);
+        if (M > 6) {
+            Lp[6 % M] = fmaf((float)(v.w & 0xFFFFu), len, Lp[6 % M]);
+            Lp[7 % M] = fmaf((float)(v.w >> 16), len, Lp[7 % M]);
+        }
+    }
+    __device__ __forceinline__ void pair(bool va, int ia, float la, bool vb, int ib, float lb)
+    {
+        const uint4 zero = make_uint4(0, 0, 0, 0);
+        const uint4 A = va ? __ldg(vol + ia) : zero;
+        const uint4 B = vb ? __ldg(vol + ib) : zero;
+        add(A, la);
+        add(B, lb);
+        nseg += (unsigned)va + (unsigned)vb;
+    }
     __device__ __forceinline__ void operator()(int idx, float len)
     {
         const uint4 v = __ldg(vol + idx);
@@ -431,6 +461,11 @@ struct AccumF32 {
     float L[M];
     float Lp[M];
     unsigned nseg;
+    __device__ __forceinline__ void pair(bool va, int ia, float la, bool vb, int ib, float lb)
+    {
+        if (va) (*this)(ia, la);
+        if (vb) (*this)(ib, lb);
+    }
     __device__ __forceinline__ void operator()(int idx, float len)
     {
         const float4* p = vol + 2 * (size_t)idx;
@@ -453,6 +488,11 @@ struct Scatter {
     float4* __restrict__ grad;
     int N, Z;
     float g[8];
+    __device__ __forceinline__ void pair(bool va, int ia, float la, bool vb, int ib, float lb)
+    {
+        if (va) (*this)(ia, la);
+        if (vb) (*this)(ib, lb);
+    }
     __device__ __forceinline__ void operator()(int idx, float len)
     {
         float4* p = grad + 2 * (size_t)idx;
@@ -460,6 +500,246 @@ struct Scatter {
         atomicAdd(p + 1, make_float4(g[4] * len, g[5] * len, g[6] * len, g[7] * len));
     }
 };
+
+// ------------------------------------------------- interval march (fast) --
+// The xy part of a ray's segments is the same for the 32 rays of a warp (one
+// detector column): the dominant-axis steps cut by the crossings of the other
+// in-plane axis.  Every 32 steps the lanes compute those xy intervals in
+// parallel (lane l takes step k0 + l: its o-plane crossing, each piece's xy
+// cell and cylinder test, all in FP64), a warp scan packs them into shared
+// memory, and then every lane walks the list with only its own z work: a
+// cached slice index, and an exact slow path at the rare z-plane crossings.
+// The segments are those of the per-step march whenever at most one z plane
+// is crossed per step (|Z1| < 1); warps with steeper rays use the per-step
+// march, which reproduces the reference's last-plane-only split.
+struct IvRec {
+    float ta, tb;  // parameter range of the xy interval
+    int base;      // (iy*N + ix)*Z of its midpoint, or -1 (outside mask / bounds)
+    int exact;     // 1: every sub-segment has the same xy cell and mask result
+};
+
+constexpr int kIvPerWarp = 64;
+
+// xy cell of the point at parameter t (FP64), as the reference's midpoint
+// rule: -1 when outside the cylindrical mask or the volume.
+__device__ __forceinline__ int xy_base_at(const ProjParams& P, const RayPlan& R, double t)
+{
+    const int nxm = (int)(P.N * 0.5), nym = (int)(P.N * 0.5);
+    const double Rv = P.N * 0.5;
+    const double Dm = R.D0 + R.pha * t, Om = R.O0 + R.O1 * t;
+    if (!(Dm * Dm + Om * Om < Rv * Rv)) return -1;
+    const int cd = (int)floor(Dm), co = (int)floor(Om);
+    const int cx = R.d ? co : cd, cy = R.d ? cd : co;
+    const int ix = trunc_index(nxm + cx, P.N), iy = trunc_index(nym - 1 - cy, P.N);
+    if (ix < 0 || iy < 0) return -1;
+    return (iy * P.N + ix) * P.Z;
+}
+
+__device__ __forceinline__ bool make_rec(const ProjParams& P, const RayPlan& R, double ta,
+                                         double tb, IvRec& rec)
+{
+    // keep every interval that meets the mask chord: a z split can move a
+    // sub-segment's midpoint inside even when the interval's is outside
+    if (!(tb > R.tc0 - 1e-9 && ta < R.tc1 + 1e-9)) return false;
+    rec.ta = (float)ta;
+    rec.tb = (float)tb;
+    if (!(rec.tb > rec.ta)) return false;  // zero-length (a crossing exactly at a step)
+    rec.base = xy_base_at(P, R, 0.5 * (ta + tb));
+    // a dominant-axis plane strictly inside (only when 1/s is not an integer)
+    // or the mask boundary inside makes sub-segments' cells differ
+    const double da = R.D0 + R.pha * ta, db = R.D0 + R.pha * tb;
+    const double lo = fmin(da, db), hi = fmax(da, db);
+    double m = floor(hi);
+    if (m == hi) m -= 1.0;
+    const bool dplane = m > lo;
+    const bool edge = (R.tc0 > ta && R.tc0 < tb) || (R.tc1 > ta && R.tc1 < tb);
+    rec.exact = (dplane || edge) ? 0 : 1;
+    return true;
+}
+
+// Intervals of steps [k0, min(k0 + 31, Khi)] into buf; returns their number.
+__device__ __forceinline__ int produce_intervals(const ProjParams& P, const RayPlan& R, int k0,
+                                                 int Khi, IvRec* buf)
+{
+    const int lane = threadIdx.x;
+    const int k = k0 + lane;
+    IvRec r0, r1;
+    bool v0 = false, v1 = false;
+    if (k <= Khi) {
+        const double tk = (double)k, tkm = tk - 1.0;
+        double tsplit = tk;
+        bool ev = false;
+        if (R.O1 != 0.0) {
+            // a plane m of the other axis is crossed in (k-1, k]: floor changes
+            // (all integers, the zero plane included: reprojectionOnGPU.cu:226)
+            const double fk = floor(R.O0 + R.O1 * tk), fkm = floor(R.O0 + R.O1 * tkm);
+            if (fk != fkm) {
+                const double m = (R.O1 > 0.0) ? fk : fkm;
+                const double t = (m - R.O0) * R.invO1;
+                if (t > tkm && t < tk) {
+                    ev = true;
+                    tsplit = t;
+                }
+            }
+        }
+        v0 = make_rec(P, R, tkm, tsplit, r0);
+        if (ev) v1 = make_rec(P, R, tsplit, tk, r1);
+    }
+    const int n = (int)v0 + (int)v1;
+    int incl = n;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+    }
+    const int total = __shfl_sync(0xffffffffu, incl, 31);
+    const int off = incl - n;
+    if (v0) buf[off] = r0;
+    if (v1) buf[off + (int)v0] = r1;
+    __syncwarp();
+    return total;
+}
+
+// Per-lane z state of the interval march.
+struct ZState {
+    int cz;        // floor(z / step) of the current position's cell
+    int iz;        // its slice index (trunc rule), or -1
+    int mz;        // next z plane that splits (never 0: :237-238)
+    int dirz;
+    float tz_next; // parameter of that crossing
+    float tz0;     // parameter of the (non-splitting) z = 0 crossing ahead, or inf
+};
+
+__device__ __forceinline__ float zcross(const RayPlan& R, int m)
+{
+    return (float)(((double)m - R.Z0) * R.invZ1);
+}
+
+__device__ __forceinline__ void zstate_init(const ProjParams& P, const RayPlan& R, double t0, ZState& z)
+{
+    const int nzm = (int)(P.Z * 0.5);
+    const double v = R.Z0 + R.Z1 * t0;
+    const double fl = floor(v);
+    z.cz = (int)fl;
+    z.dirz = (R.Z1 > 0.0) ? 1 : ((R.Z1 < 0.0) ? -1 : 0);
+    z.tz_next = kInf;
+    z.tz0 = kInf;
+    if (z.dirz) {
+        z.mz = (z.dirz > 0) ? z.cz + 1 : ((v == fl) ? z.cz - 1 : z.cz);
+        if (z.mz == 0) z.mz += z.dirz;
+        z.tz_next = zcross(R, z.mz);
+        if ((z.dirz > 0 && v < 0.0) || (z.dirz < 0 && v > 0.0)) z.tz0 = zcross(R, 0);
+    }
+    z.iz = trunc_index(nzm - 1 - z.cz, P.Z);
+}
+
+// One interval, exact: split it at the z planes inside it (and apply the
+// midpoint rule across the z = 0 plane, which does not split).
+template <class Visit>
+__device__ __forceinline__ void consume_slow(const ProjParams& P, const RayPlan& R, const IvRec& rc,
+                                             ZState& z, Visit& visit)
+{
+    const int nzm = (int)(P.Z * 0.5);
+    float cur = rc.ta;
+    const float tb = rc.tb;
+    // crossings in intervals that were not produced (outside the mask chord)
+    // only move the state
+    for (int guard = 0; z.tz_next <= cur && guard < 64; guard++) {
+        z.cz = (z.dirz > 0) ? z.mz : z.mz - 1;
+        z.mz += z.dirz;
+        if (z.mz == 0) z.mz += z.dirz;
+        z.tz_next = zcross(R, z.mz);
+    }
+    if (z.tz0 <= cur) {
+        z.cz = (z.dirz > 0) ? 0 : -1;
+        z.tz0 = kInf;
+    }
+    for (int guard = 0; guard < 8; guard++) {
+        const bool split = z.tz_next <= tb;
+        const float end = split ? z.tz_next : tb;
+        int cseg = z.cz;
+        if (z.tz0 <= end) {
+            const int after = (z.dirz > 0) ? 0 : -1;
+            if (0.5f * (cur + end) >= z.tz0) cseg = after;
+            z.cz = after;
+            z.tz0 = kInf;
+        }
+        if (end > cur) {
+            const bool whole = (cur == rc.ta) && (end == tb);
+            const int base = whole ? rc.base : xy_base_at(P, R, 0.5 * ((double)cur + (double)end));
+            const int iz = trunc_index(nzm - 1 - cseg, P.Z);
+            if (base >= 0 && iz >= 0) visit(base + iz, (end - cur) * R.Lt);
+        }
+        if (!split) break;
+        z.cz = (z.dirz > 0) ? z.mz : z.mz - 1;
+        cur = end;
+        z.mz += z.dirz;
+        if (z.mz == 0) z.mz += z.dirz;
+        z.tz_next = zcross(R, z.mz);
+    }
+    z.iz = trunc_index(nzm - 1 - z.cz, P.Z);
+}
+
+template <class Visit>
+__device__ __forceinline__ void consume_one(const ProjParams& P, const RayPlan& R, const IvRec& rc,
+                                            ZState& z, Visit& visit)
+{
+    if (z.tz_next <= rc.tb || z.tz0 <= rc.tb) {
+        consume_slow(P, R, rc, z, visit);
+    } else if (rc.base >= 0 && z.iz >= 0) {
+        visit(rc.base + z.iz, (rc.tb - rc.ta) * R.Lt);
+    }
+}
+
+// Iterations [Klo, Khi] of one ray by intervals; `flush` folds partial sums.
+// Per interval the common case is one vector load in the lane's current z
+// cell; a z crossing inside an exact interval splits it inline (second load
+// in the new cell).  Everything else -- the non-splitting z = 0 plane, a
+// crossing in an interval whose sub-segments may change xy cell or mask
+// result, and crossings passed in intervals that were not produced -- goes
+// through consume_slow.  Both branches are taken warp-uniformly.
+template <class Visit, class Flush>
+__device__ __forceinline__ void march_intervals(const ProjParams& P, const RayPlan& R, bool act,
+                                                int Klo, int Khi, IvRec* buf, Visit& visit,
+                                                Flush flush)
+{
+    const int nzm = (int)(P.Z * 0.5);
+    ZState z;
+    zstate_init(P, R, (double)(Klo - 1), z);
+    if (!act) {  // inactive lanes follow the warp without contributing
+        z.iz = -1;
+        z.tz_next = kInf;
+        z.tz0 = kInf;
+    }
+    const float Lt = R.Lt;
+    for (int k0 = Klo; k0 <= Khi; k0 += 32) {
+        const int total = produce_intervals(P, R, k0, Khi, buf);
+        for (int i = 0; i < total; i++) {
+            const IvRec rc = buf[i];
+            const float lim = rc.exact ? rc.ta : rc.tb;
+            const bool rare = (z.tz0 <= rc.tb) || (z.tz_next <= lim);
+            if (__any_sync(0xffffffffu, rare)) {
+                consume_one(P, R, rc, z, visit);
+                continue;
+            }
+            const bool ev = z.tz_next <= rc.tb;
+            const float tz = ev ? z.tz_next : rc.tb;
+            if (rc.base >= 0 && z.iz >= 0) visit(rc.base + z.iz, (tz - rc.ta) * Lt);
+            if (__any_sync(0xffffffffu, ev)) {
+                if (ev) {
+                    z.cz = (z.dirz > 0) ? z.mz : z.mz - 1;
+                    z.iz = trunc_index(nzm - 1 - z.cz, P.Z);
+                    z.mz += z.dirz;
+                    if (z.mz == 0) z.mz += z.dirz;
+                    z.tz_next = zcross(R, z.mz);
+                    if (rc.base >= 0 && z.iz >= 0 && rc.tb > tz) visit(rc.base + z.iz, (rc.tb - tz) * Lt);
+                }
+            }
+        }
+        __syncwarp();
+        flush();
+    }
+}
 
 // Two-level summation: the visitor accumulates into Lp; every 32 iterations
 // the partials are folded into L (bounds the FP32 error growth).
@@ -519,12 +799,43 @@ __device__ __forceinline__ void warp_range(const RayPlan& R, bool valid, int& Kl
 }
 
 // grid: (ceil(W / cols_per_block), ceil(H / 32), V); block: (32, cols_per_block).
+// Per-element path integrals of one ray (first segment + iterations
+// [Klo, Khi]).  The interval march is used unless a lane of the warp has
+// |Z1| >= 1 (more than one z plane per step), where the per-step march keeps
+// the reference's last-plane-only split.  R.active is warp-uniform.
+template <class Acc, int M>
+__device__ __forceinline__ void ray_integrals(const ProjParams& P, const RayPlan& R, bool act,
+                                              int Klo, int Khi, IvRec* wbuf, Acc& acc)
+{
+#pragma unroll
+    for (int i = 0; i < M; i++) { acc.L[i] = 0.0f; acc.Lp[i] = 0.0f; }
+    if (!R.active) return;
+    const bool steep = __any_sync(0xffffffffu, fabs(R.Z1) >= 1.0);
+    if (steep) {
+        march_accumulate<Acc, M>(P, R, Klo, Khi, acc);
+        if (!act) for (int i = 0; i < M; i++) acc.L[i] = 0.0f;
+        return;
+    }
+    if (act && R.first_idx >= 0) acc(R.first_idx, R.first_len);
+    auto fold = [&]() {
+#pragma unroll
+        for (int i = 0; i < M; i++) { acc.L[i] += acc.Lp[i]; acc.Lp[i] = 0.0f; }
+    };
+    if (Klo <= Khi) march_intervals(P, R, act, Klo, Khi, wbuf, acc, fold);
+    fold();
+}
+
+// grid: (ceil(W / cols_per_block), V, ceil(H / 32)); block: (32, cols_per_block).
+// Blocks are dispatched view-fastest within a band of 32 detector rows, so
+// the blocks resident at a time share one z band of the volume (L2 reuse
+// across views).
 template <int M, bool F32VOL, bool COUNT>
 __global__ void __launch_bounds__(256) forward_kernel(ForwardArgs a)
 {
     extern __shared__ float4 smem[];
     float4* s_mu = smem;
     float* s_pdf = reinterpret_cast<float*>(smem + 2 * a.spec.NE);
+    IvRec* s_iv = reinterpret_cast<IvRec*>(smem + 2 * a.spec.NE + (a.spec.NE + 3) / 4);
     load_spectrum(a.spec, s_mu, s_pdf);
     __syncthreads();
 
@@ -532,9 +843,10 @@ __global__ void __launch_bounds__(256) forward_kernel(ForwardArgs a)
     const int lane = threadIdx.x;
     const int jj = blockIdx.x * blockDim.y + threadIdx.y;  // detector column
     if (jj >= P.W) return;                                 // whole warp exits together
-    const int j = blockIdx.y * 32 + lane;                  // detector row
-    const int v = blockIdx.z;
+    const int v = blockIdx.y;
+    const int j = blockIdx.z * 32 + lane;                  // detector row
     const bool valid = j < P.H;
+    IvRec* wbuf = s_iv + threadIdx.y * kIvPerWarp;
 
     const ViewGeom vg = a.views[v];
     RayPlan R;
@@ -546,15 +858,13 @@ __global__ void __launch_bounds__(256) forward_kernel(ForwardArgs a)
     unsigned nseg = 0;
     if (F32VOL) {
         AccumF32<M> acc{a.vol_f32, P.N, P.Z, {}, {}, 0u};
-        if (R.active) march_accumulate<AccumF32<M>, M>(P, R, Klo, Khi, acc);
-        else for (int i = 0; i < M; i++) acc.L[i] = 0.0f;
+        ray_integrals<AccumF32<M>, M>(P, R, valid, Klo, Khi, wbuf, acc);
 #pragma unroll
         for (int i = 0; i < M; i++) L[i] = acc.L[i];
         nseg = acc.nseg;
     } else {
         AccumU16<M> acc{a.vol_u16, P.N, P.Z, {}, {}, 0u};
-        if (R.active) march_accumulate<AccumU16<M>, M>(P, R, Klo, Khi, acc);
-        else for (int i = 0; i < M; i++) acc.L[i] = 0.0f;
+        ray_integrals<AccumU16<M>, M>(P, R, valid, Klo, Khi, wbuf, acc);
 #pragma unroll
         for (int i = 0; i < M; i++) L[i] = acc.L[i];
         nseg = acc.nseg;
@@ -577,6 +887,7 @@ __global__ void __launch_bounds__(256) adjoint_kernel(AdjointArgs a)
     extern __shared__ float4 smem[];
     float4* s_mu = smem;
     float* s_pdf = reinterpret_cast<float*>(smem + 2 * a.spec.NE);
+    IvRec* s_iv = reinterpret_cast<IvRec*>(smem + 2 * a.spec.NE + (a.spec.NE + 3) / 4);
     load_spectrum(a.spec, s_mu, s_pdf);
     __syncthreads();
 
@@ -584,23 +895,24 @@ __global__ void __launch_bounds__(256) adjoint_kernel(AdjointArgs a)
     const int lane = threadIdx.x;
     const int jj = blockIdx.x * blockDim.y + threadIdx.y;
     if (jj >= P.W) return;
-    const int j = blockIdx.y * 32 + lane;
-    const int v = blockIdx.z;
+    const int v = blockIdx.y;
+    const int j = blockIdx.z * 32 + lane;
     const bool valid = j < P.H;
+    IvRec* wbuf = s_iv + threadIdx.y * kIvPerWarp;
     const ViewGeom vg = a.views[v];
     RayPlan R;
     ray_setup(P, vg, j, jj, R);
     float r = 0.0f;
     if (valid) r = a.grad_out[((size_t)v * P.H + (P.H - 1 - j)) * P.W + jj];
+    const bool act = valid && r != 0.0f;
     int Klo, Khi;
     // rays with a zero residual do not scatter
-    warp_range(R, valid && r != 0.0f, Klo, Khi);
-    if (!__any_sync(0xffffffffu, valid && r != 0.0f && R.active)) return;
+    warp_range(R, act, Klo, Khi);
+    if (!__any_sync(0xffffffffu, act && R.active)) return;
 
     // pass 1: recompute the per-element path integrals of this ray
     AccumF32<M> acc{a.vol_f32, P.N, P.Z, {}, {}, 0u};
-    if (R.active) march_accumulate<AccumF32<M>, M>(P, R, Klo, Khi, acc);
-    else for (int i = 0; i < M; i++) acc.L[i] = 0.0f;
+    ray_integrals<AccumF32<M>, M>(P, R, act, Klo, Khi, wbuf, acc);
 
     // d I / d L_k = -leng * sum_E pdf_E mu'_k(E) exp(-sum_k mu'_k(E) L_k)
     float g[8] = {0, 0, 0, 0, 0, 0, 0, 0};
@@ -626,11 +938,18 @@ __global__ void __launch_bounds__(256) adjoint_kernel(AdjointArgs a)
     Scatter sc{a.grad_packed, P.N, P.Z, {}};
 #pragma unroll
     for (int i = 0; i < 8; i++) sc.g[i] = g[i] * scale;
-    // pass 2: scatter along the same segments (lanes with r == 0 add zeros)
-    if (R.active && r != 0.0f) {
-        if (R.first_idx >= 0) sc(R.first_idx, R.first_len);
-        if (Klo <= Khi) march(P, R, Klo, Khi, sc);
+    // pass 2: scatter along the same segments
+    if (!R.active) return;
+    const bool steep = __any_sync(0xffffffffu, fabs(R.Z1) >= 1.0);
+    if (steep) {
+        if (act) {
+            if (R.first_idx >= 0) sc(R.first_idx, R.first_len);
+            if (Klo <= Khi) march(P, R, Klo, Khi, sc);
+        }
+        return;
     }
+    if (act && R.first_idx >= 0) sc(R.first_idx, R.first_len);
+    if (Klo <= Khi) march_intervals(P, R, act, Klo, Khi, wbuf, sc, []() {});
 }
 
 // ------------------------------------------------------- layout kernels --
@@ -744,8 +1063,9 @@ static cudaError_t launch_fwd_t(const ForwardArgs& a, cudaStream_t st)
 {
     const int cpb = a.cols_per_block;
     dim3 block(32, cpb);
-    dim3 grid((a.p.W + cpb - 1) / cpb, (a.p.H + 31) / 32, a.p.V);
-    size_t shm = (size_t)a.spec.NE * (2 * sizeof(float4) + sizeof(float));
+    dim3 grid((a.p.W + cpb - 1) / cpb, a.p.V, (a.p.H + 31) / 32);
+    size_t shm = ((size_t)2 * a.spec.NE + (a.spec.NE + 3) / 4) * sizeof(float4) +
+                 (size_t)cpb * kIvPerWarp * sizeof(IvRec);
     auto k = forward_kernel<M, F32VOL, COUNT>;
     if (shm > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
@@ -772,8 +1092,9 @@ static cudaError_t launch_adj_t(const AdjointArgs& a, cudaStream_t st)
 {
     const int cpb = a.cols_per_block;
     dim3 block(32, cpb);
-    dim3 grid((a.p.W + cpb - 1) / cpb, (a.p.H + 31) / 32, a.p.V);
-    size_t shm = (size_t)a.spec.NE * (2 * sizeof(float4) + sizeof(float));
+    dim3 grid((a.p.W + cpb - 1) / cpb, a.p.V, (a.p.H + 31) / 32);
+    size_t shm = ((size_t)2 * a.spec.NE + (a.spec.NE + 3) / 4) * sizeof(float4) +
+                 (size_t)cpb * kIvPerWarp * sizeof(IvRec);
     auto k = adjoint_kernel<M>;
     if (shm > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
