@@ -71,3 +71,19 @@ def test_fdk_chain_short_volume_within_one_lsb(cuda):
     ref, _ = O.ref_backproject(g.N, g.Z, g.zstart, g.step, g.scale, filt, g.xfactor, ang, xs, g.piso)
     d = np.abs(vi.astype(np.int32) - ref.astype(np.int16).astype(np.int32))
     assert d.max() <= 1, f"{(d > 1).sum()} voxels differ by more than 1 LSB"
+
+
+@pytest.mark.parametrize("V,H,W,xshift", [(6, 40, 48, 0.0), (4, 8, 400, 0.0), (3, 100, 400, 16.0),
+                                          (2, 70, 256, 2.0)])
+def test_bf16x3_tensor_core_filter_matches_fp64(cuda, V, H, W, xshift):
+    """The tcgen05 BF16 3-term split GEMM against the FP64 filter; the same
+    tolerance as the direct FP32 path (1e-5 of the output scale)."""
+    from virtualcbct_b200 import FILTER_BF16X3
+    g, proj, ang, xs = _case(V=V, H=H, W=W, seed=W + V, xshift=xshift)
+    f = Fdk(g, ang, xs, np.zeros(g.V))
+    gpu = f.filter(proj, method=FILTER_BF16X3)
+    d64 = O.filter_sinogram(proj, xs, np.zeros(g.V), O.fdk_consts(g.piso), mode=1)
+    assert np.isfinite(gpu).all()
+    assert np.abs(gpu - d64).max() <= 1e-5 * np.abs(d64).max()
+    direct = f.filter(proj, method=FILTER_DIRECT_F32)
+    assert np.abs(gpu - direct).max() <= 1e-5 * np.abs(d64).max()
