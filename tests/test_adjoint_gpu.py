@@ -1,0 +1,87 @@
+"""Adjoint of the polychromatic projection with respect to the six float
+element volumes: against the FP64 gradient of the oracle and against central
+finite differences of the FP64 forward (h = 1e-3 on 64 random voxels)."""
+import numpy as np
+import pytest
+
+import oracle as O
+from tests.cases import proj_case, spectrum
+from virtualcbct_b200 import Projector
+
+pytestmark = pytest.mark.gpu
+
+
+def _float_case(seed=0, **kw):
+    g, tabs, vol, _ = proj_case("ellipsoid", seed=seed, **kw)
+    rng = np.random.default_rng(seed)
+    volf = vol.astype(np.float32) * rng.uniform(0.9, 1.1, size=vol.shape).astype(np.float32)
+    return g, tabs, volf
+
+
+def test_float_volume_forward_matches_oracle(cuda):
+    import torch
+    g, tabs, volf = _float_case(1)
+    mu, pdf = spectrum()
+    p = Projector(g, *tabs)
+    p.set_spectrum(mu, pdf, 1000.0)
+    p.load_volume_f32(torch.from_numpy(volf).to(cuda))
+    out = p.forward().cpu().numpy()
+    ref = O.mbfpa_forward(g, tabs, None, mu, pdf, 1000.0, volf=volf, exact=False, want=("d",))["d"]
+    assert np.max(np.abs(out - ref) / ref) <= 1e-5
+
+
+@pytest.mark.parametrize("seed", [0, 4])
+def test_adjoint_matches_fp64_gradient(cuda, seed):
+    import torch
+    from virtualcbct_b200.autograd import project
+    g, tabs, volf = _float_case(seed)
+    mu, pdf = spectrum()
+    rng = np.random.default_rng(100 + seed)
+    resid = rng.normal(size=(g.V, g.H, g.W)).astype(np.float32)
+    p = Projector(g, *tabs)
+    p.set_spectrum(mu, pdf, 1000.0)
+    v = torch.from_numpy(volf).to(cuda).requires_grad_(True)
+    out = project(v, p)
+    (out * torch.from_numpy(resid).to(cuda)).sum().backward()
+    gpu = v.grad.cpu().numpy().astype(np.float64)
+    ref = O.mbfpa_adjoint(g, tabs, volf, mu, pdf, 1000.0, resid.astype(np.float64))
+    scale = np.abs(ref).max()
+    assert scale > 0
+    assert np.abs(gpu - ref).max() <= 2e-4 * scale
+    rel = np.linalg.norm(gpu - ref) / np.linalg.norm(ref)
+    assert rel <= 1e-5
+
+
+def test_adjoint_matches_central_finite_differences(cuda):
+    """loss = 0.5 * sum (I - target)^2, target from a phantom with +10% Ca/P."""
+    import torch
+    from virtualcbct_b200.autograd import decomposition_step
+    g, tabs, volf = _float_case(7, N=40, Z=12, V=3, W=32, H=28)
+    mu, pdf = spectrum()
+    tgt_vol = volf.copy()
+    tgt_vol[:, 4] *= 1.1
+    tgt_vol[:, 5] *= 1.1
+    target = O.mbfpa_forward(g, tabs, None, mu, pdf, 1000.0, volf=tgt_vol, exact=False, want=("d",))["d"]
+    p = Projector(g, *tabs)
+    p.set_spectrum(mu, pdf, 1000.0)
+    loss, grad = decomposition_step(torch.from_numpy(volf).to(cuda), torch.from_numpy(target.astype(np.float32)).to(cuda), p)
+    grad = grad.cpu().numpy()
+
+    def loss64(v):
+        d = O.mbfpa_forward(g, tabs, None, mu, pdf, 1000.0, volf=v, exact=False, want=("d",))["d"]
+        return 0.5 * np.sum((d - target) ** 2)
+
+    rng = np.random.default_rng(1234)
+    # 64 random voxels with a non-negligible gradient (inside the traversed region)
+    cand = np.argwhere(np.abs(grad) > 1e-3 * np.abs(grad).max())
+    pick = cand[rng.choice(len(cand), size=64, replace=False)]
+    # h = 2^-10 (~1e-3): v +- h is exact in float32 for |v| < 2^14
+    h = 2.0 ** -10
+    assert np.abs(volf).max() < 2 ** 14
+    errs = []
+    for idx in map(tuple, pick):
+        vp = volf.astype(np.float64).copy(); vm = vp.copy()
+        vp[idx] += h; vm[idx] -= h
+        fd = (loss64(vp.astype(np.float32)) - loss64(vm.astype(np.float32))) / (2 * h)
+        errs.append(abs(fd - grad[idx]) / max(abs(grad[idx]), 1e-30))
+    assert np.median(errs) <= 1e-3 and np.max(errs) <= 2e-2
