@@ -120,6 +120,27 @@ int vcbct_projector_count_segments(vcbct_projector* p, unsigned long long* total
 int vcbct_projector_adjoint(vcbct_projector* p, const float* d_grad_out, float* d_grad,
                             void* stream);
 
+/* Batched projection (no reference counterpart; the reference projects one
+ * phantom per process run).  Items are projector objects holding a uint16
+ * volume and a spectrum, each with its own device output [V][H][W]; the items
+ * may differ in volume size, view count and detector.  vcbct_batch_forward
+ * projects all of them in one persistent launch that balances the uneven work
+ * through a global tile counter; with use_graph != 0 the launch sequence is
+ * captured into a CUDA graph on the first call and replayed on later calls
+ * (the items must not change in between; adding an item rebuilds it). */
+typedef struct vcbct_batch vcbct_batch;
+int vcbct_batch_create(vcbct_batch** out);
+int vcbct_batch_add(vcbct_batch* b, vcbct_projector* p, float* d_out);
+int vcbct_batch_forward(vcbct_batch* b, int use_graph, void* stream);
+int vcbct_batch_destroy(vcbct_batch* b);
+
+/* Autotuner: time the launch-shape candidates (columns of the detector per
+ * thread block) on the object's own data and keep the fastest, per geometry
+ * signature; with the environment variable VCBCT_TUNE_CACHE naming a file the
+ * choices persist across processes.  d_out receives a projection. */
+int vcbct_projector_autotune(vcbct_projector* p, float* d_out, void* stream, int* chosen);
+int vcbct_batch_autotune(vcbct_batch* b, void* stream, int* chosen);
+
 /* Reference-named entry points (Release_CBCT_Projection_CM/reprojectionOnGPU.h).
  * Same argument lists and meaning, including the ignored ones (ite,
  * reprojection_float, npf_double, projVolume, anglesRad, xalpha,

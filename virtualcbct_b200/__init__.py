@@ -7,9 +7,9 @@ from . import _native
 from ._native import FILTER_BF16X3, FILTER_DIRECT_F32, VcbctError
 from .fdk import Fdk
 from .geometry import FdkGeometry, ProjGeometry, attenuation_table, trig_tables
-from .projector import Projector
+from .projector import Batch, Projector
 
-__all__ = ["Projector", "Fdk", "ProjGeometry", "FdkGeometry", "trig_tables", "attenuation_table",
+__all__ = ["Projector", "Batch", "Fdk", "ProjGeometry", "FdkGeometry", "trig_tables", "attenuation_table",
            "VcbctError", "FILTER_DIRECT_F32", "FILTER_BF16X3", "lib"]
 
 

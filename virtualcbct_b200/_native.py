@@ -67,6 +67,12 @@ SIGNATURES = {
     "vcbct_projector_path_integrals": (C.c_int, [_vp, _vp, _vp]),
     "vcbct_projector_count_segments": (C.c_int, [_vp, C.POINTER(C.c_ulonglong), _vp]),
     "vcbct_projector_adjoint": (C.c_int, [_vp, _vp, _vp, _vp]),
+    "vcbct_batch_create": (C.c_int, [C.POINTER(_vp)]),
+    "vcbct_batch_add": (C.c_int, [_vp, _vp, _vp]),
+    "vcbct_batch_forward": (C.c_int, [_vp, C.c_int, _vp]),
+    "vcbct_batch_destroy": (C.c_int, [_vp]),
+    "vcbct_projector_autotune": (C.c_int, [_vp, _vp, _vp, _ip]),
+    "vcbct_batch_autotune": (C.c_int, [_vp, _vp, _ip]),
     "vcbct_mbfpa_forward_noalloc": (C.c_int, [C.POINTER(ProjGeometryC), _dp, _dp, _dp, _dp, _vp, _fp,
                                               _fp, C.c_int, C.c_double, _vp, _vp]),
     "vcbct_proj_trig_tables": (C.c_int, [C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, C.c_double,

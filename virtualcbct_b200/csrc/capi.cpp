@@ -3,8 +3,12 @@
 // preparation.
 #include <cuda_runtime.h>
 
+#include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <fstream>
+#include <map>
+#include <sstream>
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
@@ -296,6 +300,267 @@ extern "C" int vcbct_projector_adjoint(vcbct_projector* p, const float* d_grad_o
     a.cols_per_block = p->cols_per_block;
     VCBCT_CUDA_TRY(launch_adjoint(a, st));
     VCBCT_CUDA_TRY(launch_unpack_grad(p->grad_pk.as<float4>(), g.recon_size, g.recon_slices, g.num_material, d_grad, st));
+    return VCBCT_OK;
+}
+
+// ------------------------------------------------------------------ batching --
+//
+// A batch is a list of (projector, device output) items projected by one
+// persistent launch (batch_forward_kernel) whose launch sequence -- counter
+// reset + kernel -- is captured once into a CUDA graph and replayed.
+
+struct vcbct_batch {
+    std::vector<vcbct_projector*> proj;
+    std::vector<float*> outs;
+    DevBuf items;       // BatchItem[]
+    DevBuf counter;
+    long long total = 0;
+    int NEmax = 0, nmat_max = 0;
+    int cols_per_block = 4, blocks = 0;
+    bool dirty = true;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaStream_t graph_stream = nullptr;
+};
+
+static void batch_drop_graph(vcbct_batch* b)
+{
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    b->exec = nullptr;
+    b->graph = nullptr;
+}
+
+extern "C" int vcbct_batch_create(vcbct_batch** out)
+{
+    if (!out) return fail(VCBCT_ERR_ARG, "out is NULL");
+    *out = new vcbct_batch();
+    return VCBCT_OK;
+}
+
+extern "C" int vcbct_batch_destroy(vcbct_batch* b)
+{
+    if (!b) return VCBCT_OK;
+    batch_drop_graph(b);
+    b->items.release();
+    b->counter.release();
+    delete b;
+    return VCBCT_OK;
+}
+
+extern "C" int vcbct_batch_add(vcbct_batch* b, vcbct_projector* p, float* d_out)
+{
+    if (!b || !p || !d_out) return fail(VCBCT_ERR_ARG, "NULL argument");
+    if (!p->have_u16) return fail(VCBCT_ERR_STATE, "batched projection needs a uint16 volume");
+    if (p->NE <= 0) return fail(VCBCT_ERR_STATE, "no spectrum set");
+    b->proj.push_back(p);
+    b->outs.push_back(d_out);
+    b->dirty = true;
+    return VCBCT_OK;
+}
+
+static int batch_build(vcbct_batch* b)
+{
+    if (b->proj.empty()) return fail(VCBCT_ERR_STATE, "empty batch");
+    std::vector<BatchItem> it(b->proj.size());
+    long long u = 0;
+    b->NEmax = 0;
+    b->nmat_max = 0;
+    const int cpb = b->cols_per_block;
+    for (size_t i = 0; i < b->proj.size(); i++) {
+        vcbct_projector* p = b->proj[i];
+        ForwardArgs a;
+        int rc = make_fwd_args(p, a);
+        if (rc) return rc;
+        a.out = b->outs[i];
+        a.cols_per_block = cpb;
+        it[i].fa = a;
+        it[i].unit_begin = u;
+        it[i].ncolb = (p->g.proj_width + cpb - 1) / cpb;
+        it[i].pad = 0;
+        u += (long long)it[i].ncolb * p->g.n_views * ((p->g.proj_height + 31) / 32);
+        b->NEmax = std::max(b->NEmax, p->NE);
+        b->nmat_max = std::max(b->nmat_max, p->g.num_material);
+    }
+    b->total = u;
+    VCBCT_CUDA_TRY(b->items.ensure(sizeof(BatchItem) * it.size()));
+    VCBCT_CUDA_TRY(cudaMemcpy(b->items.p, it.data(), sizeof(BatchItem) * it.size(), cudaMemcpyHostToDevice));
+    VCBCT_CUDA_TRY(b->counter.ensure(64));
+    int dev = 0, sms = 0;
+    VCBCT_CUDA_TRY(cudaGetDevice(&dev));
+    VCBCT_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const int per_sm = batch_blocks_per_sm(b->nmat_max, cpb, b->NEmax);
+    b->blocks = std::max(1, per_sm) * sms;
+    batch_drop_graph(b);
+    b->dirty = false;
+    return VCBCT_OK;
+}
+
+static int batch_launch(vcbct_batch* b, cudaStream_t st)
+{
+    VCBCT_CUDA_TRY(launch_batch_forward(b->items.as<BatchItem>(), (int)b->proj.size(), b->total, b->NEmax,
+                                        b->nmat_max, b->cols_per_block, b->blocks,
+                                        b->counter.as<unsigned long long>(), st));
+    return VCBCT_OK;
+}
+
+extern "C" int vcbct_batch_forward(vcbct_batch* b, int use_graph, void* stream)
+{
+    if (!b) return fail(VCBCT_ERR_ARG, "NULL batch");
+    cudaStream_t st = (cudaStream_t)stream;
+    if (b->dirty) {
+        int rc = batch_build(b);
+        if (rc) return rc;
+    }
+    if (!use_graph) return batch_launch(b, st);
+    if (!b->exec || b->graph_stream != st) {
+        batch_drop_graph(b);
+        cudaStream_t cap = st;
+        bool own = false;
+        if (cap == nullptr) {  // the legacy stream cannot be captured
+            VCBCT_CUDA_TRY(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+            own = true;
+        }
+        VCBCT_CUDA_TRY(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
+        int rc = batch_launch(b, cap);
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamEndCapture(cap, &g);
+        if (own) cudaStreamDestroy(cap);
+        if (rc) return rc;
+        if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+        b->graph = g;
+        VCBCT_CUDA_TRY(cudaGraphInstantiate(&b->exec, b->graph, 0));
+        b->graph_stream = st;
+    }
+    VCBCT_CUDA_TRY(cudaGraphLaunch(b->exec, st));
+    return VCBCT_OK;
+}
+
+// ----------------------------------------------------------------- autotuner --
+//
+// Launch shapes are picked by timing the candidates on the caller's data:
+// columns per block (warps per block) for the plain and the batched forward
+// projection.  Results are kept per geometry signature in memory and, when
+// VCBCT_TUNE_CACHE names a file, in that file ("signature value" lines).
+
+namespace {
+std::mutex g_tune_mu;
+std::map<std::string, int> g_tune;
+bool g_tune_loaded = false;
+
+void tune_load()
+{
+    if (g_tune_loaded) return;
+    g_tune_loaded = true;
+    const char* f = std::getenv("VCBCT_TUNE_CACHE");
+    if (!f) return;
+    std::ifstream in(f);
+    std::string key;
+    int v;
+    while (in >> key >> v) g_tune[key] = v;
+}
+
+void tune_store(const std::string& key, int v)
+{
+    g_tune[key] = v;
+    const char* f = std::getenv("VCBCT_TUNE_CACHE");
+    if (!f) return;
+    std::ofstream out(f, std::ios::app);
+    out << key << " " << v << "\n";
+}
+
+std::string device_tag()
+{
+    int dev = 0;
+    cudaDeviceProp prop;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaGetDeviceProperties(&prop, dev) != cudaSuccess) return "dev?";
+    std::string n = prop.name;
+    for (auto& c : n)
+        if (c == ' ') c = '_';
+    return n;
+}
+
+template <class F>
+float time_ms(F f, cudaStream_t st, int reps)
+{
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    f();
+    cudaEventRecord(a, st);
+    for (int i = 0; i < reps; i++) f();
+    cudaEventRecord(b, st);
+    cudaEventSynchronize(b);
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    return ms / reps;
+}
+}  // namespace
+
+extern "C" int vcbct_projector_autotune(vcbct_projector* p, float* d_out, void* stream, int* chosen)
+{
+    if (!p || !d_out) return fail(VCBCT_ERR_ARG, "NULL argument");
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    tune_load();
+    const auto& g = p->g;
+    std::ostringstream key;
+    key << "fwd:" << device_tag() << ":" << g.recon_size << "x" << g.recon_slices << ":" << g.proj_width << "x"
+        << g.proj_height << "x" << g.n_views << ":" << g.num_material << ":" << p->NE;
+    auto it = g_tune.find(key.str());
+    if (it == g_tune.end()) {
+        cudaStream_t st = (cudaStream_t)stream;
+        float best = 1e30f;
+        int bestc = p->cols_per_block;
+        for (int c : {2, 4, 8}) {
+            p->cols_per_block = c;
+            float ms = time_ms([&]() { vcbct_projector_forward(p, d_out, 1, stream); }, st, 2);
+            if (ms < best) {
+                best = ms;
+                bestc = c;
+            }
+        }
+        tune_store(key.str(), bestc);
+        p->cols_per_block = bestc;
+    } else {
+        p->cols_per_block = it->second;
+    }
+    if (chosen) *chosen = p->cols_per_block;
+    return VCBCT_OK;
+}
+
+extern "C" int vcbct_batch_autotune(vcbct_batch* b, void* stream, int* chosen)
+{
+    if (!b || b->proj.empty()) return fail(VCBCT_ERR_ARG, "empty batch");
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    tune_load();
+    std::ostringstream key;
+    key << "batch:" << device_tag() << ":" << b->proj.size();
+    for (auto* p : b->proj)
+        key << ":" << p->g.recon_size << "x" << p->g.recon_slices << "x" << p->g.n_views << "x" << p->g.proj_width
+            << "x" << p->g.proj_height;
+    auto it = g_tune.find(key.str());
+    int bestc = b->cols_per_block;
+    if (it == g_tune.end()) {
+        cudaStream_t st = (cudaStream_t)stream;
+        float best = 1e30f;
+        for (int c : {2, 4, 8}) {
+            b->cols_per_block = c;
+            b->dirty = true;
+            float ms = time_ms([&]() { vcbct_batch_forward(b, 0, stream); }, st, 1);
+            if (ms < best) {
+                best = ms;
+                bestc = c;
+            }
+        }
+        tune_store(key.str(), bestc);
+    } else {
+        bestc = it->second;
+    }
+    b->cols_per_block = bestc;
+    b->dirty = true;
+    if (chosen) *chosen = bestc;
     return VCBCT_OK;
 }
 

@@ -67,6 +67,18 @@ struct ForwardArgs {
 };
 cudaError_t launch_forward(const ForwardArgs& a, cudaStream_t st);
 
+// One phantom of a batched forward projection (u16 volume, no counter).
+struct BatchItem {
+    ForwardArgs fa;
+    long long unit_begin;  // index of its first work tile
+    int ncolb;             // column blocks per view and row band
+    int pad;
+};
+cudaError_t launch_batch_forward(const BatchItem* d_items, int nitems, long long total_units, int NEmax,
+                                 int nmat_max, int cols_per_block, int blocks, unsigned long long* counter,
+                                 cudaStream_t st);
+int batch_blocks_per_sm(int nmat_max, int cols_per_block, int NEmax);
+
 struct AdjointArgs {
     ProjParams p;
     const ViewGeom* views;

@@ -825,26 +825,18 @@ __device__ __forceinline__ void ray_integrals(const ProjParams& P, const RayPlan
     fold();
 }
 
-// grid: (ceil(W / cols_per_block), V, ceil(H / 32)); block: (32, cols_per_block).
-// Blocks are dispatched view-fastest within a band of 32 detector rows, so
-// the blocks resident at a time share one z band of the volume (L2 reuse
-// across views).
+// One work tile of the forward projection: detector columns
+// [colb*cpb, colb*cpb + cpb) (one per warp), rows [rowt*32, rowt*32 + 32) (one
+// per lane) of view v.  The spectrum table must already be in shared memory.
 template <int M, bool F32VOL, bool COUNT>
-__global__ void __launch_bounds__(256) forward_kernel(ForwardArgs a)
+__device__ __forceinline__ void forward_tile(const ForwardArgs& a, const float4* s_mu, const float* s_pdf,
+                                             IvRec* s_iv, int v, int rowt, int colb)
 {
-    extern __shared__ float4 smem[];
-    float4* s_mu = smem;
-    float* s_pdf = reinterpret_cast<float*>(smem + 2 * a.spec.NE);
-    IvRec* s_iv = reinterpret_cast<IvRec*>(smem + 2 * a.spec.NE + (a.spec.NE + 3) / 4);
-    load_spectrum(a.spec, s_mu, s_pdf);
-    __syncthreads();
-
     const ProjParams& P = a.p;
     const int lane = threadIdx.x;
-    const int jj = blockIdx.x * blockDim.y + threadIdx.y;  // detector column
-    if (jj >= P.W) return;                                 // whole warp exits together
-    const int v = blockIdx.y;
-    const int j = blockIdx.z * 32 + lane;                  // detector row
+    const int jj = colb * blockDim.y + threadIdx.y;  // detector column
+    if (jj >= P.W) return;                           // whole warp exits together
+    const int j = rowt * 32 + lane;                  // detector row
     const bool valid = j < P.H;
     IvRec* wbuf = s_iv + threadIdx.y * kIvPerWarp;
 
@@ -879,6 +871,69 @@ __global__ void __launch_bounds__(256) forward_kernel(ForwardArgs a)
         for (int i = 0; i < P.nmat; i++) a.L_out[o * P.nmat + i] = L[i];
     }
     if (a.out) a.out[o] = spectral_sum<M>(s_mu, s_pdf, a.spec.NE, L) * R.leng;
+}
+
+__device__ __forceinline__ IvRec* iv_buffer(float4* smem, int NEmax)
+{
+    return reinterpret_cast<IvRec*>(smem + 2 * NEmax + (NEmax + 3) / 4);
+}
+
+// grid: (ceil(W / cols_per_block), V, ceil(H / 32)); block: (32, cols_per_block).
+// Blocks are dispatched view-fastest within a band of 32 detector rows, so
+// the blocks resident at a time share one z band of the volume (L2 reuse
+// across views).
+template <int M, bool F32VOL, bool COUNT>
+__global__ void __launch_bounds__(256) forward_kernel(ForwardArgs a)
+{
+    extern __shared__ float4 smem[];
+    float4* s_mu = smem;
+    float* s_pdf = reinterpret_cast<float*>(smem + 2 * a.spec.NE);
+    load_spectrum(a.spec, s_mu, s_pdf);
+    __syncthreads();
+    forward_tile<M, F32VOL, COUNT>(a, s_mu, s_pdf, iv_buffer(smem, a.spec.NE), blockIdx.y, blockIdx.z, blockIdx.x);
+}
+
+// Persistent batched forward projection: every block repeatedly takes the
+// next work tile from a global counter.  Tiles are numbered item by item,
+// and within an item by row band, then view, then column block (the order of
+// forward_kernel's grid), so the items' uneven view and slice counts
+// load-balance across the whole GPU in one launch.
+template <int M>
+__global__ void __launch_bounds__(256) batch_forward_kernel(const BatchItem* __restrict__ items, int nitems,
+                                                            long long total, int NEmax,
+                                                            unsigned long long* counter)
+{
+    extern __shared__ float4 smem[];
+    __shared__ long long s_unit;
+    float4* s_mu = smem;
+    float* s_pdf = reinterpret_cast<float*>(smem + 2 * NEmax);
+    IvRec* s_iv = iv_buffer(smem, NEmax);
+    int cur = -1;
+    for (;;) {
+        if (threadIdx.x == 0 && threadIdx.y == 0) s_unit = (long long)atomicAdd(counter, 1ull);
+        __syncthreads();
+        const long long u = s_unit;
+        if (u >= total) break;
+        int lo = 0, hi = nitems - 1;  // last item with begin <= u
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) / 2;
+            if (items[mid].unit_begin <= u) lo = mid;
+            else hi = mid - 1;
+        }
+        const BatchItem& it = items[lo];
+        if (lo != cur) {
+            load_spectrum(it.fa.spec, s_mu, s_pdf);
+            cur = lo;
+        }
+        __syncthreads();
+        const long long w = u - it.unit_begin;
+        const int colb = (int)(w % it.ncolb);
+        const long long rest = w / it.ncolb;
+        const int v = (int)(rest % it.fa.p.V);
+        const int rowt = (int)(rest / it.fa.p.V);
+        forward_tile<M, false, false>(it.fa, s_mu, s_pdf, s_iv, v, rowt, colb);
+        __syncthreads();
+    }
 }
 
 template <int M>
@@ -1073,6 +1128,34 @@ static cudaError_t launch_fwd_t(const ForwardArgs& a, cudaStream_t st)
     }
     k<<<grid, block, shm, st>>>(a);
     return cudaGetLastError();
+}
+
+cudaError_t launch_batch_forward(const BatchItem* d_items, int nitems, long long total_units, int NEmax,
+                                 int nmat_max, int cols_per_block, int blocks, unsigned long long* counter,
+                                 cudaStream_t st)
+{
+    dim3 block(32, cols_per_block);
+    size_t shm = ((size_t)2 * NEmax + (NEmax + 3) / 4) * sizeof(float4) +
+                 (size_t)cols_per_block * kIvPerWarp * sizeof(IvRec);
+    // (the shared-memory attribute is set by batch_blocks_per_sm, before any
+    // stream capture)
+    cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st);
+    if (e != cudaSuccess) return e;
+    if (nmat_max <= 6) batch_forward_kernel<6><<<blocks, block, shm, st>>>(d_items, nitems, total_units, NEmax, counter);
+    else batch_forward_kernel<8><<<blocks, block, shm, st>>>(d_items, nitems, total_units, NEmax, counter);
+    return cudaGetLastError();
+}
+
+int batch_blocks_per_sm(int nmat_max, int cols_per_block, int NEmax)
+{
+    size_t shm = ((size_t)2 * NEmax + (NEmax + 3) / 4) * sizeof(float4) +
+                 (size_t)cols_per_block * kIvPerWarp * sizeof(IvRec);
+    int n = 0;
+    auto k = (nmat_max <= 6) ? batch_forward_kernel<6> : batch_forward_kernel<8>;
+    if (shm > 48 * 1024 && cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm) != cudaSuccess)
+        return 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, 32 * cols_per_block, shm);
+    return n;
 }
 
 cudaError_t launch_forward(const ForwardArgs& a, cudaStream_t st)

@@ -132,6 +132,16 @@ class Projector:
         N.check(N.lib().vcbct_projector_count_segments(self._h, C.byref(tot), _stream_ptr(stream)))
         return int(tot.value)
 
+    def autotune(self, stream=None) -> int:
+        """Pick the fastest launch shape for this geometry (see vcbct.h)."""
+        import torch
+        g = self.geom
+        tmp = torch.empty((g.V, g.H, g.W), dtype=torch.float32, device="cuda")
+        c = C.c_int(0)
+        N.check(N.lib().vcbct_projector_autotune(self._h, C.c_void_p(tmp.data_ptr()), _stream_ptr(stream),
+                                                 C.byref(c)))
+        return c.value
+
     def adjoint(self, grad_out, grad=None, stream=None):
         """Accumulate d loss / d volume (float [Z][nmat][N][N], device) for a
         device d loss / d projection ``grad_out`` [V][H][W]."""
@@ -143,3 +153,45 @@ class Projector:
         N.check(N.lib().vcbct_projector_adjoint(self._h, C.c_void_p(go.data_ptr()),
                                                 C.c_void_p(grad.data_ptr()), _stream_ptr(stream)))
         return grad
+
+
+class Batch:
+    """Several projectors (uneven phantoms, view sets and detectors) projected
+    by one persistent launch, optionally replayed from a captured CUDA graph."""
+
+    def __init__(self):
+        h = C.c_void_p()
+        N.check(N.lib().vcbct_batch_create(C.byref(h)))
+        self._h = h
+        self._items = []
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            N.lib().vcbct_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add(self, projector: Projector, out=None):
+        """Add a projector (uint16 volume and spectrum loaded); returns its
+        device output tensor [V][H][W]."""
+        import torch
+        g = projector.geom
+        if out is None:
+            out = torch.empty((g.V, g.H, g.W), dtype=torch.float32, device="cuda")
+        N.check(N.lib().vcbct_batch_add(self._h, projector._h, C.c_void_p(out.data_ptr())))
+        self._items.append((projector, out))
+        return out
+
+    def forward(self, use_graph: bool = True, stream=None):
+        N.check(N.lib().vcbct_batch_forward(self._h, int(bool(use_graph)), _stream_ptr(stream)))
+        return [o for _, o in self._items]
+
+    def autotune(self, stream=None) -> int:
+        c = C.c_int(0)
+        N.check(N.lib().vcbct_batch_autotune(self._h, _stream_ptr(stream), C.byref(c)))
+        return c.value
