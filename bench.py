@@ -191,6 +191,102 @@ def run_reference(args, rank, world):
     }))
 
 
+def decomposition_section(stream):
+    """Config 4: one least-squares decomposition step (forward + adjoint
+    through torch.autograd) vs a plain forward: six FP32 element volumes
+    256x256x64 (1x1x2 mm), 90 views, 200x200 detector (2 mm), 91-bin 100 kV
+    spectrum; target from the same phantom with bone Ca/P +10%."""
+    import torch
+    from virtualcbct_b200 import Projector, ProjGeometry, attenuation_table, phantoms, trig_tables
+    from virtualcbct_b200.autograd import decomposition_step
+    g = ProjGeometry(N=256, Z=64, s=0.1, step=0.2, W=200, H=200, V=90)
+    ang = np.deg2rad(phantoms.view_angles(g.V))
+    tabs = trig_tables(g.W, g.H, ang, np.zeros(g.V), np.zeros(g.V), g.pdet, g.dpn)
+    mu, pdf = attenuation_table(os.path.join(DATA, "spectrum_kramers100_91.csv"), MINIDB, 6)
+    vol = phantoms.ellipsoid_phantom_torch(g.N, g.Z, g.s, g.step, seed=21, as_float=True)
+    tgt_vol = vol.clone()
+    tgt_vol[:, 4] *= 1.1
+    tgt_vol[:, 5] *= 1.1
+    p = Projector(g, *tabs)
+    p.set_spectrum(mu, pdf, 1000.0)
+    p.load_volume_f32(tgt_vol)
+    target = p.forward().clone()
+    p.load_volume_f32(vol)
+    out = torch.empty_like(target)
+    for _ in range(3):
+        p.forward(out)
+        decomposition_step(vol, target, p)
+    torch.cuda.synchronize()
+    reps = 5
+    e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    e[0].record(stream)
+    for _ in range(reps):
+        p.load_volume_f32(vol)
+        p.forward(out)
+    e[1].record(stream)
+    for _ in range(reps):
+        loss, grad = decomposition_step(vol, target, p)
+    e[2].record(stream)
+    torch.cuda.synchronize()
+    fwd = e[0].elapsed_time(e[1]) / reps
+    step = e[1].elapsed_time(e[2]) / reps
+    return {"workload": "6 x FP32 256x256x64 (1x1x2 mm), 90 views, 200x200 (2 mm), 91 bins",
+            "forward_ms": fwd, "step_ms": step, "step_over_forward": step / fwd,
+            "loss": float(loss.item())}
+
+
+def batched_section(stream, args):
+    """Config 3: 16 ellipsoid phantoms with uneven slice (64-256) and view
+    (90-720) counts, 512x512 slices (0.625 mm), 400x400 detector: one
+    persistent launch replayed from a CUDA graph vs one plain launch per
+    phantom, both on device-resident volumes."""
+    import torch
+    from virtualcbct_b200 import Batch, Projector, ProjGeometry, attenuation_table, phantoms, trig_tables
+    rng = np.random.default_rng(2024)
+    mu, pdf = attenuation_table(os.path.join(DATA, "spectrum_kramers100_90.csv"), MINIDB, 6)
+    projs, outs = [], []
+    batch = Batch()
+    zs, vs = [], []
+    for i in range(16):
+        Z = int(rng.integers(64, 257))
+        V = int(rng.integers(90, 721))
+        g = ProjGeometry(N=512, Z=Z, s=0.0625, step=0.2, W=400, H=400, V=V)
+        ang = np.deg2rad(phantoms.view_angles(V))
+        tabs = trig_tables(g.W, g.H, ang, np.zeros(V), np.zeros(V), g.pdet, g.dpn)
+        p = Projector(g, *tabs)
+        p.set_spectrum(mu, pdf, 1000.0)
+        vol = phantoms.ellipsoid_phantom_torch(g.N, Z, g.s, g.step, seed=100 + i)
+        p.load_volume(vol)
+        del vol
+        projs.append(p)
+        outs.append(batch.add(p))
+        zs.append(Z)
+        vs.append(V)
+    torch.cuda.synchronize()
+    nseg = sum(p.count_segments() for p in projs)
+    tuned = batch.autotune()
+    batch.forward(use_graph=True)
+    for p, o in zip(projs, outs):
+        p.forward(o)
+    torch.cuda.synchronize()
+    reps = 2
+    e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    e[0].record(stream)
+    for _ in range(reps):
+        for p, o in zip(projs, outs):
+            p.forward(o)
+    e[1].record(stream)
+    for _ in range(reps):
+        batch.forward(use_graph=True)
+    e[2].record(stream)
+    torch.cuda.synchronize()
+    plain = e[0].elapsed_time(e[1]) / reps
+    bat = e[1].elapsed_time(e[2]) / reps
+    return {"workload": "16 ellipsoid phantoms 512x512xZ (Z 64-256), V 90-720, 400x400",
+            "slices": zs, "views": vs, "segments": nseg, "autotuned_cols_per_block": tuned, "plain_ms": plain, "batched_graph_ms": bat,
+            "batched_over_plain_speedup": plain / bat, "batched_gseg_s": nseg / (bat * 1e-3) / 1e9}
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import virtualcbct_b200 as vc
@@ -273,25 +369,41 @@ def run_ours(args, rank, world, local_rank):
     fg = w["fg"]
     F = Fdk(fg, ang, w["xs_fdk"], np.zeros(fg.V))
     P.forward(out)
-    method = vc.FILTER_DIRECT_F32
-    filt = F.filter(out, method=method)
+    filt_d = F.filter(out, method=vc.FILTER_DIRECT_F32)
+    filt = F.filter(out, method=vc.FILTER_BF16X3)
+    filt_err = float((filt - filt_d).abs().max() / filt_d.abs().max())
     vf, vi = F.backproject(filt)
     for _ in range(2):
-        F.filter(out, method=method)
+        F.filter(out, filt_d, method=vc.FILTER_DIRECT_F32)
+        F.filter(out, filt, method=vc.FILTER_BF16X3)
         F.backproject(filt)
     torch.cuda.synchronize()
-    a0, a1, a2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    a0, a1, a2, a3 = (torch.cuda.Event(enable_timing=True) for _ in range(4))
     a0.record(stream)
     for _ in range(args.steps):
-        F.filter(out, filt, method=method)
+        F.filter(out, filt_d, method=vc.FILTER_DIRECT_F32)
     a1.record(stream)
     for _ in range(args.steps):
-        F.backproject(filt)
+        F.filter(out, filt, method=vc.FILTER_BF16X3)
     a2.record(stream)
+    for _ in range(args.steps):
+        F.backproject(filt)
+    a3.record(stream)
     torch.cuda.synchronize()
-    ms_filter = a0.elapsed_time(a1) / args.steps
-    ms_bp = a1.elapsed_time(a2) / args.steps
+    ms_filter_direct = a0.elapsed_time(a1) / args.steps
+    ms_filter = a1.elapsed_time(a2) / args.steps
+    ms_bp = a2.elapsed_time(a3) / args.steps
     gups = fg.N * fg.N * fg.Z * fg.V / (ms_bp * 1e-3) / 1e9
+    # BF16x3 work: 6 split products of a (V*H) x Kp x Np GEMM
+    Kp = (fg.W + 63) // 64 * 64
+    Np = (fg.W + 15) // 16 * 16
+    gemm_tflops = 2.0 * 6 * fg.V * fg.H * Kp * Np / (ms_filter * 1e-3) / 1e12
+    del F, filt_d
+
+    extra = {}
+    if not args.no_extras:
+        extra["decomposition"] = decomposition_section(stream)
+        extra["batched"] = batched_section(stream, args)
 
     peak, peak_kind = measured_peaks()
     alg_bytes = 12.0 * nseg
@@ -309,10 +421,13 @@ def run_ours(args, rank, world, local_rank):
                      "frac": achieved / peak, "peak_kind": peak_kind,
                      "traffic": FORWARD_DRAM_BYTES,
                      "note": "achieved = 12 B (6 x uint16) per segment / forward launch time"},
-        "fdk": {"filter_ms": ms_filter, "filter_method": "direct_f32", "bp_ms": ms_bp,
-                "bp_gups": gups, "short_volume_range": [int(vi.min().item()), int(vi.max().item())]},
+        "fdk": {"filter_ms": ms_filter, "filter_method": "bf16x3_tcgen05", "filter_tflops": gemm_tflops,
+                "filter_ms_direct_f32": ms_filter_direct, "bf16x3_vs_direct_max_rel": filt_err,
+                "bp_ms": ms_bp, "bp_gups": gups,
+                "short_volume_range": [int(vi.min().item()), int(vi.max().item())]},
         "clocks": clk,
     }
+    res.update(extra)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             ncores = os.cpu_count() or 1
@@ -342,6 +457,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the decomposition-step and batched sections")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     world = int(os.environ.get("WORLD_SIZE", "1"))

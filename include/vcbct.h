@@ -205,6 +205,56 @@ int vcbct_proj_trig_tables(int proj_width, int proj_height, int n_views,
 int vcbct_attenuation_table(const char* spectrum_csv, const char* xraydb_dir, int num_material,
                             int nthin, float* mu, float* pdf, int* n_bins);
 
+/* ------------------------------------------------ projector input deck */
+
+/* The projector's info file (txt), read as loadData does
+ * (Release_CBCT_Projection_CM/projectionData.cpp:63-102; fields of
+ * projectionData.h:2-63): six header lines, then per field two skipped lines
+ * and one value line parsed with the reference's scanf formats.  Relative
+ * paths inside are relative to the current directory, as in the reference.
+ * The derived members are computed exactly as projectionData.cpp:173-218 and
+ * main.cpp:101-103 do; the volume itself is read by
+ * vcbct_proj_deck_load_volume. */
+typedef struct {
+    char spectrum[256];      /* SpectrumString: spectrum CSV path */
+    int total_proj;          /* totalProjNumber: views (flexmap entries) */
+    int proj_width;          /* projImgWidth */
+    int proj_height;         /* projImgHeight */
+    char angle_file[256];    /* angleDataFilename: flexmap path */
+    char mat_prefix[256];    /* matImgFileDirname: slices "<prefix>_%03d.raw" */
+    int z_ic;                /* zICposition as written (isocentre slice) */
+    char output_name[256];   /* outputname: projections go to "<name>.raw" */
+    double x_scale, y_scale, z_scale;  /* voxel pitch [cm] */
+    int recon_size;          /* reconSize: N */
+    int recon_slices;        /* reconSlices: slices on disk */
+    int mat_num;             /* element planes per slice */
+    char mat_type[16];       /* human / watercylinder / ...: no effect on mu */
+    double xfactor;          /* density factor */
+    double x_reg, y_reg, z_reg_file;   /* registration shift as written */
+    /* physParams.h:47-51 ("CM" block) */
+    double det_pitch_cm, det_pitch_iso_cm, sad_cm, det_pixel_num, det_iso_cm;
+    /* derived */
+    int slice_first;         /* linemin: first slice read */
+    int used_slices;         /* usedZNumber: slices in the volume */
+    int z_ic_local;          /* zICposition - linemin */
+    double z_reg;            /* (used_slices/2 - z_ic_local) * z_scale (main.cpp:103) */
+} vcbct_proj_deck;
+
+int vcbct_proj_deck_read(const char* txt_path, vcbct_proj_deck* deck);
+/* Reads the used_slices slice files into volume uint16
+ * [used_slices][mat_num][N][N].  A missing or short slice file leaves that
+ * slice holding the previous slice's values (zeros for the first), as the
+ * reference's reused read buffer does (projectionData.cpp:187-215); their
+ * number goes to *n_incomplete (may be NULL) and a warning to stderr. */
+int vcbct_proj_deck_load_volume(const vcbct_proj_deck* deck, uint16_t* volume,
+                                int* n_incomplete);
+/* Flexmap "angle[deg] xshift yshift class" lines (projectionData.cpp:
+ * 164-171): angles_rad = angle * pi / 180.  Entries beyond `capacity` return
+ * VCBCT_ERR_LIMIT (the reference writes past its arrays); a malformed line
+ * returns VCBCT_ERR_IO.  Unfilled entries are left as they are. */
+int vcbct_flexmap_read(const char* path, int capacity, double* angles_rad, double* xshift,
+                       double* yshift, int* n_entries);
+
 /* -------------------------------------------------------------------- FDK */
 
 /* Geometry of filterSinogram / reconstructImage.  The reference fixes
@@ -256,6 +306,55 @@ int vcbct_fdk_filter(vcbct_fdk* f, const float* proj, float* filtered, int on_de
  * (short) cast of R/main.cpp:179-185; may be NULL).  Overwrites. */
 int vcbct_fdk_backproject(vcbct_fdk* f, const float* filtered, float* vol_f32, short* vol_i16,
                           int on_device, void* stream);
+
+/* The FDK info file, read as loadData + loadProjectionData do
+ * (R/projectionDataMVkV.cpp:51-321; fields of projectionDataMVkV.h:2-42):
+ *  - the "first file number" field is read in hex for "kV", in decimal for
+ *    "MV"; any other energy class returns VCBCT_ERR_ARG (the reference then
+ *    skips the field and leaves the isocentre pitch unset); kV and MV use
+ *    the same pitch at the isocentre (R/physParams.h:24-25);
+ *  - flexmap entries whose class matches target_class ("*" = all) are kept;
+ *    the list is reversed when the 1st angle minus the 30th is negative
+ *    (:156-211); with fewer than 30 entries the reference reads an
+ *    uninitialised value, and here the list is kept in file order;
+ *  - recon_slices is corrected when recon_offset + recon_step *
+ *    (recon_slices - 1) reaches proj_height (:283-302);
+ *  - panel_class is S / M / L from the mean xshift (:276-281).
+ * The per-view arrays hold total_proj entries (the views in the projection
+ * file); entries beyond n_target stay zero.  More than VCBCT_FDK_MAX_VIEWS
+ * flexmap lines, or more matching lines than total_proj, return
+ * VCBCT_ERR_LIMIT (the reference overruns its arrays). */
+#define VCBCT_FDK_MAX_VIEWS 1080   /* MAX_Proj_Num, R/physParams.h:47 */
+typedef struct {
+    char energy_class[16];   /* kVMVClassString */
+    int total_proj;          /* totalProjNumber as written = usedProjNumber */
+    int proj_width;
+    int proj_height;
+    int proj_header_bytes;   /* projImgFileOffset (unused by the float path) */
+    char proj_prefix[256];   /* projImgFileDirname: the file is "<prefix>.<ext>" */
+    int proj_num_digits;     /* projImgFileNumDigits (unused) */
+    int proj_first_number;   /* projImgFile1stNumber (unused; 0 if unparsed) */
+    char proj_ext[8];        /* projImgFileExt */
+    char angle_file[256];
+    int recon_size;
+    char target_class[16];   /* reconTgtClassString */
+    int recon_offset;        /* zstart [cm] (an int) */
+    double recon_step;
+    int recon_slices;        /* after the slice-count correction */
+    double recon_scale;
+    int xfactor;
+    char recon_file[256];    /* reconDataFilename: short volume output */
+    double det_pitch_iso_cm;
+    int n_lines;             /* flexmap entries */
+    int n_target;            /* entries matching target_class */
+    int reversed;            /* 1 when the list was reversed */
+    char panel_class[8];     /* SMLClassString */
+    double angles_rad[VCBCT_FDK_MAX_VIEWS];
+    double xshift[VCBCT_FDK_MAX_VIEWS];
+    double yshift[VCBCT_FDK_MAX_VIEWS];
+} vcbct_fdk_deck;
+
+int vcbct_fdk_deck_read(const char* txt_path, vcbct_fdk_deck* deck);
 
 /* Reference-named FDK entry points (R/filterSinogram.h:2-6,
  * R/reconstructImage.h:2-5).  Arrays are VOLUME-ONE style pointer tables over

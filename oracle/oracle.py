@@ -327,3 +327,58 @@ def ref_mask(N):
     m = np.zeros((N, N), np.int8)
     L.ref_mask(C.c_int(N), m.ctypes.data_as(C.c_char_p))
     return m
+
+
+def ref_proj_load(txt):
+    """Reference loadData + loadProjectionData of the projector
+    (P/projectionData.cpp:63-237), run in the current directory; returns a
+    dict of the fields, the flexmap arrays and the assembled volume."""
+    L = ref_proj()
+    L.ref_proj_load.restype = C.c_int
+    L.ref_free.restype = None
+    ints = np.zeros(8, np.int32)
+    dbls = np.zeros(12, np.float64)
+    spec, outn, mtype = (C.create_string_buffer(256), C.create_string_buffer(256),
+                         C.create_string_buffer(16))
+    vol, ang, xs, ys = C.POINTER(C.c_uint16)(), _dp(), _dp(), _dp()
+    r = L.ref_proj_load(txt.encode(), _ptr(ints, _ip), _ptr(dbls, _dp), spec, outn, mtype,
+                        C.byref(vol), C.byref(ang), C.byref(xs), C.byref(ys))
+    if r == 0:
+        raise RuntimeError("reference loadData failed")
+    V, N, nmat, used = int(ints[0]), int(ints[4]), int(ints[6]), int(ints[7])
+    out = dict(total_proj=V, proj_width=int(ints[1]), proj_height=int(ints[2]),
+               z_ic_local=int(ints[3]), recon_size=N, recon_slices=int(ints[5]), mat_num=nmat,
+               used_slices=used, x_scale=dbls[0], y_scale=dbls[1], z_scale=dbls[2],
+               xfactor=dbls[3], x_reg=dbls[4], y_reg=dbls[5], z_reg_file=dbls[6],
+               det_pitch_cm=dbls[7], det_pitch_iso_cm=dbls[8], sad_cm=dbls[9],
+               det_pixel_num=dbls[10], det_iso_cm=dbls[11], spectrum=spec.value.decode(),
+               output_name=outn.value.decode(), mat_type=mtype.value.decode())
+    out["angles_rad"] = np.ctypeslib.as_array(ang, (V,)).copy()
+    out["xshift"] = np.ctypeslib.as_array(xs, (V,)).copy()
+    out["yshift"] = np.ctypeslib.as_array(ys, (V,)).copy()
+    out["volume"] = np.ctypeslib.as_array(vol, (used * nmat * N * N,)).copy().reshape(used, nmat, N, N)
+    for p in (vol, ang, xs, ys):
+        L.ref_free(C.cast(p, C.c_void_p))
+    return out
+
+
+def ref_fdk_load(txt):
+    """Reference loadData + loadProjectionData of the FDK program
+    (R/projectionDataMVkV.cpp:51-321), run in the current directory."""
+    L = ref_fdk()
+    L.ref_fdk_load.restype = C.c_int
+    ints = np.zeros(8, np.int32)
+    dbls = np.zeros(3, np.float64)
+    pdir, ext, outn, sml = (C.create_string_buffer(256), C.create_string_buffer(8),
+                            C.create_string_buffer(256), C.create_string_buffer(8))
+    ang, xs, ys = (np.zeros(1080), np.zeros(1080), np.zeros(1080))
+    r = L.ref_fdk_load(txt.encode(), _ptr(ints, _ip), _ptr(dbls, _dp), pdir, ext, outn, sml,
+                       _ptr(ang, _dp), _ptr(xs, _dp), _ptr(ys, _dp))
+    used = int(ints[1])
+    return dict(ret=int(r), n_target=int(ints[0]), total_proj=used, proj_width=int(ints[2]),
+                proj_height=int(ints[3]), recon_size=int(ints[4]), recon_offset=int(ints[5]),
+                recon_slices=int(ints[6]), xfactor=int(ints[7]), recon_step=dbls[0],
+                recon_scale=dbls[1], det_pitch_iso_cm=dbls[2], proj_prefix=pdir.value.decode(),
+                proj_ext=ext.value.decode(), recon_file=outn.value.decode(),
+                panel_class=sml.value.decode(), angles_rad=ang[:used].copy(),
+                xshift=xs[:used].copy(), yshift=ys[:used].copy())

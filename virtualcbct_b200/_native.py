@@ -49,6 +49,37 @@ class FdkGeometryC(C.Structure):
                 ("gamma", C.c_double), ("alpha", C.c_double), ("redundancy", C.c_int)]
 
 
+FDK_MAX_VIEWS = 1080
+
+
+class ProjDeckC(C.Structure):
+    """vcbct_proj_deck (the projector's info file)."""
+    _fields_ = [("spectrum", C.c_char * 256), ("total_proj", C.c_int), ("proj_width", C.c_int),
+                ("proj_height", C.c_int), ("angle_file", C.c_char * 256), ("mat_prefix", C.c_char * 256),
+                ("z_ic", C.c_int), ("output_name", C.c_char * 256), ("x_scale", C.c_double),
+                ("y_scale", C.c_double), ("z_scale", C.c_double), ("recon_size", C.c_int),
+                ("recon_slices", C.c_int), ("mat_num", C.c_int), ("mat_type", C.c_char * 16),
+                ("xfactor", C.c_double), ("x_reg", C.c_double), ("y_reg", C.c_double),
+                ("z_reg_file", C.c_double), ("det_pitch_cm", C.c_double), ("det_pitch_iso_cm", C.c_double),
+                ("sad_cm", C.c_double), ("det_pixel_num", C.c_double), ("det_iso_cm", C.c_double),
+                ("slice_first", C.c_int), ("used_slices", C.c_int), ("z_ic_local", C.c_int),
+                ("z_reg", C.c_double)]
+
+
+class FdkDeckC(C.Structure):
+    """vcbct_fdk_deck (the FDK info file and its flexmap)."""
+    _fields_ = [("energy_class", C.c_char * 16), ("total_proj", C.c_int), ("proj_width", C.c_int),
+                ("proj_height", C.c_int), ("proj_header_bytes", C.c_int), ("proj_prefix", C.c_char * 256),
+                ("proj_num_digits", C.c_int), ("proj_first_number", C.c_int), ("proj_ext", C.c_char * 8),
+                ("angle_file", C.c_char * 256), ("recon_size", C.c_int), ("target_class", C.c_char * 16),
+                ("recon_offset", C.c_int), ("recon_step", C.c_double), ("recon_slices", C.c_int),
+                ("recon_scale", C.c_double), ("xfactor", C.c_int), ("recon_file", C.c_char * 256),
+                ("det_pitch_iso_cm", C.c_double), ("n_lines", C.c_int), ("n_target", C.c_int),
+                ("reversed", C.c_int), ("panel_class", C.c_char * 8),
+                ("angles_rad", C.c_double * FDK_MAX_VIEWS), ("xshift", C.c_double * FDK_MAX_VIEWS),
+                ("yshift", C.c_double * FDK_MAX_VIEWS)]
+
+
 _vp = C.c_void_p
 _dp = C.POINTER(C.c_double)
 _fp = C.POINTER(C.c_float)
@@ -78,6 +109,10 @@ SIGNATURES = {
     "vcbct_proj_trig_tables": (C.c_int, [C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, C.c_double,
                                          C.c_double, _dp, _dp, _dp, _dp]),
     "vcbct_attenuation_table": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int, C.c_int, _fp, _fp, _ip]),
+    "vcbct_proj_deck_read": (C.c_int, [C.c_char_p, C.POINTER(ProjDeckC)]),
+    "vcbct_proj_deck_load_volume": (C.c_int, [C.POINTER(ProjDeckC), _vp, _ip]),
+    "vcbct_flexmap_read": (C.c_int, [C.c_char_p, C.c_int, _dp, _dp, _dp, _ip]),
+    "vcbct_fdk_deck_read": (C.c_int, [C.c_char_p, C.POINTER(FdkDeckC)]),
     "vcbct_fdk_default_geometry": (None, [C.POINTER(FdkGeometryC)]),
     "vcbct_fdk_create": (C.c_int, [C.POINTER(FdkGeometryC), _dp, _dp, _dp, C.POINTER(_vp)]),
     "vcbct_fdk_destroy": (C.c_int, [_vp]),

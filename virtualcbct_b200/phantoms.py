@@ -137,3 +137,51 @@ def kramers_spectrum(kvp: float = 100.0, e_lo: float = 10.0, e_hi: float | None 
 def spectrum_csv_text(lo_mev, hi_mev, frac) -> str:
     rows = ["Energy,1000,Fraction"] + [f"{a:.6g},{b:.6g},{c:.6e}" for a, b, c in zip(lo_mev, hi_mev, frac)]
     return "\n".join(rows) + "\n"
+
+
+def ellipsoid_phantom_torch(N: int, Z: int, s: float, step: float, seed: int = 0, jitter: float = 0.05,
+                            as_float: bool = False, device="cuda"):
+    """Same phantom family as ``ellipsoid_phantom``, generated on the GPU with
+    a seeded torch generator (for large batched workloads); the element
+    encoding and jitter rule are the same, the random stream is not."""
+    import torch
+    gen = torch.Generator(device=device)
+    gen.manual_seed(seed)
+    x = (torch.arange(N, device=device, dtype=torch.float32) - (N - 1) / 2.0) * s
+    X = x[None, None, :].expand(Z, N, N)
+    Y = (-x)[None, :, None].expand(Z, N, N)
+    zc = (torch.arange(Z, device=device, dtype=torch.float32) - (Z - 1) / 2.0) * step
+    taper = torch.sqrt(torch.clamp(1.0 - (zc / (0.5 * Z * step + 20.0)) ** 2, min=0.0))[:, None, None]
+    cls = torch.full((Z, N, N), -1, dtype=torch.int8, device=device)
+    body = (X / (15.0 * taper)) ** 2 + (Y / (11.0 * taper)) ** 2 <= 1.0
+    inner = (X / (14.0 * taper)) ** 2 + (Y / (10.0 * taper)) ** 2 <= 1.0
+    cls[body] = 1
+    cls[inner] = 0
+    for sx in (-6.0, 6.0):
+        cls[(((X - sx) / 4.5) ** 2 + ((Y - 1.0) / 6.5) ** 2 <= 1.0) & inner] = 2
+    rr = (X / 12.5) ** 2 + (Y / 8.8) ** 2
+    iz = torch.arange(Z, device=device, dtype=torch.float32)[:, None, None]
+    ribs = (rr > 0.93) & (rr < 1.0) & (torch.cos(torch.atan2(Y, X) * 9.0 + iz * 0.3) > 0.2)
+    cls[(X / 1.6) ** 2 + ((Y + 7.0) / 1.6) ** 2 <= 1.0] = 3
+    cls[ribs & inner] = 3
+    names = ["soft", "fat", "lung", "bone"]
+    base = torch.zeros((5, 6), device=device, dtype=torch.float32)
+    rho = torch.zeros(5, device=device, dtype=torch.float32)
+    for ci, name in enumerate(names):
+        base[ci] = torch.tensor(TISSUE[name], dtype=torch.float32)
+        rho[ci] = DENSITY[name]
+    c = cls.long().clamp(min=0)
+    fr = base[c]  # [Z,N,N,6]
+    fr = fr * (1.0 + (torch.rand(fr.shape, generator=gen, device=device, dtype=torch.float32) * 2 - 1) * jitter)
+    fr[..., 3] = 1.0 - (fr.sum(-1) - fr[..., 3])
+    neg = fr[..., 3] < 0
+    fr[neg] = fr[neg] / fr[neg].sum(-1, keepdim=True)
+    fr[..., 3] = torch.where(neg, torch.zeros_like(fr[..., 3]), fr[..., 3])
+    vals = fr * rho[c][..., None] * 1000.0
+    air = cls < 0
+    vals[air] = 0.0
+    vals[..., 2] = torch.where(air, torch.full_like(vals[..., 2], 1.2), vals[..., 2])
+    vol = vals.permute(0, 3, 1, 2).contiguous()  # [Z][6][N][N]
+    if as_float:
+        return vol.float()
+    return torch.clamp(torch.round(vol), 0, 65535).to(torch.int32).to(torch.int16)  # uint16 bits
