@@ -1,5 +1,6 @@
-"""Batched projection: uneven phantoms in one persistent launch (and its
-CUDA-graph replay) give exactly the per-phantom results."""
+"""Batched projection: uneven phantoms in one persistent launch or as
+per-item launches on graph branches (and their CUDA-graph replay) give
+exactly the per-phantom results."""
 import numpy as np
 import pytest
 
@@ -28,15 +29,17 @@ def test_batched_equals_plain_launches(cuda):
     plain = [p.forward().cpu().numpy() for p in ps]
     b = Batch()
     outs = [b.add(p) for p in ps]
-    for use_graph in (False, True, True):
-        for o in outs:
-            o.fill_(float("nan"))
-        b.forward(use_graph=use_graph)
-        torch.cuda.synchronize()
-        for o, ref in zip(outs, plain):
-            assert np.array_equal(o.cpu().numpy(), ref)
+    for per_item, cpb in ((False, 4), (True, 4), (False, 2), (True, 8)):
+        b.configure(per_item, cpb)
+        for use_graph in (False, True, True):
+            for o in outs:
+                o.fill_(float("nan"))
+            b.forward(use_graph=use_graph)
+            torch.cuda.synchronize()
+            for o, ref in zip(outs, plain):
+                assert np.array_equal(o.cpu().numpy(), ref), (per_item, cpb, use_graph)
     c = b.autotune()
-    assert c in (2, 4, 8)
+    assert c % 100 in (2, 4, 8) and c // 100 in (0, 1)
     b.forward(use_graph=True)
     torch.cuda.synchronize()
     for o, ref in zip(outs, plain):

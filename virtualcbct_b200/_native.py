@@ -102,6 +102,7 @@ SIGNATURES = {
     "vcbct_batch_add": (C.c_int, [_vp, _vp, _vp]),
     "vcbct_batch_forward": (C.c_int, [_vp, C.c_int, _vp]),
     "vcbct_batch_destroy": (C.c_int, [_vp]),
+    "vcbct_batch_configure": (C.c_int, [_vp, C.c_int, C.c_int]),
     "vcbct_projector_autotune": (C.c_int, [_vp, _vp, _vp, _ip]),
     "vcbct_batch_autotune": (C.c_int, [_vp, _vp, _ip]),
     "vcbct_mbfpa_forward_noalloc": (C.c_int, [C.POINTER(ProjGeometryC), _dp, _dp, _dp, _dp, _vp, _fp,

@@ -12,7 +12,7 @@ from __future__ import annotations
 
 import torch
 
-from .projector import Projector
+from .projector import Projector, _volume_key
 
 
 class _MbfpaProject(torch.autograd.Function):
@@ -31,8 +31,10 @@ class _MbfpaProject(torch.autograd.Function):
     def backward(ctx, grad_out: torch.Tensor):
         (vol,) = ctx.saved_tensors
         p: Projector = ctx.projector
-        # the adjoint reads the float volume the forward used
-        p.load_volume_f32(vol)
+        # the adjoint reads the float volume the forward used: reload it only
+        # if the projector has been given another volume since
+        if p.loaded != _volume_key("f32", vol):
+            p.load_volume_f32(vol)
         grad = torch.zeros_like(vol)
         p.adjoint(grad_out.contiguous().float(), grad)
         return grad, None

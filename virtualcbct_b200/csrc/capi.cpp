@@ -305,9 +305,16 @@ extern "C" int vcbct_projector_adjoint(vcbct_projector* p, const float* d_grad_o
 
 // ------------------------------------------------------------------ batching --
 //
-// A batch is a list of (projector, device output) items projected by one
-// persistent launch (batch_forward_kernel) whose launch sequence -- counter
-// reset + kernel -- is captured once into a CUDA graph and replayed.
+// A batch is a list of (projector, device output) items.  Two launch
+// strategies, picked by vcbct_batch_autotune:
+//  - persistent: one launch of batch_forward_kernel over every item's tiles
+//    (counter reset + kernel);
+//  - per-item: each item's own forward_kernel launch, spread over two
+//    branches that fork from and join to the caller's stream, so one item's
+//    tail overlaps the next item's start.
+// Either launch sequence is captured once into a CUDA graph and replayed.
+
+constexpr int kBatchBranches = 2;
 
 struct vcbct_batch {
     std::vector<vcbct_projector*> proj;
@@ -317,10 +324,13 @@ struct vcbct_batch {
     long long total = 0;
     int NEmax = 0, nmat_max = 0;
     int cols_per_block = 4, blocks = 0;
+    int per_item = 0;   // 1: per-item launches instead of the persistent one
     bool dirty = true;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     cudaStream_t graph_stream = nullptr;
+    cudaStream_t branch[kBatchBranches] = {};
+    cudaEvent_t fork = nullptr, join[kBatchBranches] = {};
 };
 
 static void batch_drop_graph(vcbct_batch* b)
@@ -344,6 +354,11 @@ extern "C" int vcbct_batch_destroy(vcbct_batch* b)
     batch_drop_graph(b);
     b->items.release();
     b->counter.release();
+    for (int k = 0; k < kBatchBranches; k++) {
+        if (b->branch[k]) cudaStreamDestroy(b->branch[k]);
+        if (b->join[k]) cudaEventDestroy(b->join[k]);
+    }
+    if (b->fork) cudaEventDestroy(b->fork);
     delete b;
     return VCBCT_OK;
 }
@@ -355,6 +370,18 @@ extern "C" int vcbct_batch_add(vcbct_batch* b, vcbct_projector* p, float* d_out)
     if (p->NE <= 0) return fail(VCBCT_ERR_STATE, "no spectrum set");
     b->proj.push_back(p);
     b->outs.push_back(d_out);
+    b->dirty = true;
+    return VCBCT_OK;
+}
+
+extern "C" int vcbct_batch_configure(vcbct_batch* b, int per_item, int cols_per_block)
+{
+    if (!b) return fail(VCBCT_ERR_ARG, "NULL batch");
+    if ((per_item != 0 && per_item != 1) ||
+        !(cols_per_block == 1 || cols_per_block == 2 || cols_per_block == 4 || cols_per_block == 8))
+        return fail(VCBCT_ERR_ARG, "per_item must be 0 or 1 and cols_per_block 1, 2, 4 or 8");
+    b->per_item = per_item;
+    b->cols_per_block = cols_per_block;
     b->dirty = true;
     return VCBCT_OK;
 }
@@ -398,9 +425,33 @@ static int batch_build(vcbct_batch* b)
 
 static int batch_launch(vcbct_batch* b, cudaStream_t st)
 {
-    VCBCT_CUDA_TRY(launch_batch_forward(b->items.as<BatchItem>(), (int)b->proj.size(), b->total, b->NEmax,
-                                        b->nmat_max, b->cols_per_block, b->blocks,
-                                        b->counter.as<unsigned long long>(), st));
+    if (!b->per_item) {
+        VCBCT_CUDA_TRY(launch_batch_forward(b->items.as<BatchItem>(), (int)b->proj.size(), b->total, b->NEmax,
+                                            b->nmat_max, b->cols_per_block, b->blocks,
+                                            b->counter.as<unsigned long long>(), st));
+        return VCBCT_OK;
+    }
+    if (!b->fork) {
+        VCBCT_CUDA_TRY(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
+        for (int k = 0; k < kBatchBranches; k++) {
+            VCBCT_CUDA_TRY(cudaStreamCreateWithFlags(&b->branch[k], cudaStreamNonBlocking));
+            VCBCT_CUDA_TRY(cudaEventCreateWithFlags(&b->join[k], cudaEventDisableTiming));
+        }
+    }
+    VCBCT_CUDA_TRY(cudaEventRecord(b->fork, st));
+    for (int k = 0; k < kBatchBranches; k++) VCBCT_CUDA_TRY(cudaStreamWaitEvent(b->branch[k], b->fork, 0));
+    for (size_t i = 0; i < b->proj.size(); i++) {
+        ForwardArgs a;
+        int rc = make_fwd_args(b->proj[i], a);
+        if (rc) return rc;
+        a.out = b->outs[i];
+        a.cols_per_block = b->cols_per_block;
+        VCBCT_CUDA_TRY(launch_forward(a, b->branch[i % kBatchBranches]));
+    }
+    for (int k = 0; k < kBatchBranches; k++) {
+        VCBCT_CUDA_TRY(cudaEventRecord(b->join[k], b->branch[k]));
+        VCBCT_CUDA_TRY(cudaStreamWaitEvent(st, b->join[k], 0));
+    }
     return VCBCT_OK;
 }
 
@@ -541,24 +592,28 @@ extern "C" int vcbct_batch_autotune(vcbct_batch* b, void* stream, int* chosen)
         key << ":" << p->g.recon_size << "x" << p->g.recon_slices << "x" << p->g.n_views << "x" << p->g.proj_width
             << "x" << p->g.proj_height;
     auto it = g_tune.find(key.str());
-    int bestc = b->cols_per_block;
+    int bestc = b->cols_per_block + 100 * b->per_item;
     if (it == g_tune.end()) {
         cudaStream_t st = (cudaStream_t)stream;
         float best = 1e30f;
-        for (int c : {2, 4, 8}) {
-            b->cols_per_block = c;
-            b->dirty = true;
-            float ms = time_ms([&]() { vcbct_batch_forward(b, 0, stream); }, st, 1);
-            if (ms < best) {
-                best = ms;
-                bestc = c;
+        for (int mode : {0, 1}) {
+            for (int c : {2, 4, 8}) {
+                b->per_item = mode;
+                b->cols_per_block = c;
+                b->dirty = true;
+                float ms = time_ms([&]() { vcbct_batch_forward(b, 0, stream); }, st, 1);
+                if (ms < best) {
+                    best = ms;
+                    bestc = c + 100 * mode;
+                }
             }
         }
         tune_store(key.str(), bestc);
     } else {
         bestc = it->second;
     }
-    b->cols_per_block = bestc;
+    b->per_item = bestc >= 100 ? 1 : 0;
+    b->cols_per_block = bestc % 100;
     b->dirty = true;
     if (chosen) *chosen = bestc;
     return VCBCT_OK;

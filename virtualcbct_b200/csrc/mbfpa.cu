@@ -90,23 +90,24 @@ struct RayPlan {
 
 // Per-ray FP64 setup: reprojectionOnGPU.cu:128-212, mirrored operation for
 // operation.  Rays that hit the xy square fewer than twice are defined to miss
-// (the reference reads uninitialised entries there).
-__device__ void ray_setup(const ProjParams& P, const ViewGeom& vg, int j, int jj, RayPlan& R)
+// (the reference reads uninitialised entries there).  Written with scalars and
+// selects instead of small arrays indexed by the ray's axes, and inlined, so
+// the plan stays in registers (no per-ray stack traffic).
+__device__ __forceinline__ void ray_setup(const ProjParams& P, const ViewGeom& vg, int j, int jj, RayPlan& R)
 {
     const double s = P.s, step = P.step;
     const int nxm = (int)(P.N * 0.5), nym = (int)(P.N * 0.5), nzm = (int)(P.Z * 0.5);
-    double S[3], Pp[3];
-    S[0] = dadd(dmul(-P.sad, vg.sn), P.xr);
-    S[1] = dadd(dmul(P.sad, vg.cs), P.yr);
-    S[2] = P.zr;
+    const double S0 = dadd(dmul(-P.sad, vg.sn), P.xr);
+    const double S1 = dadd(dmul(P.sad, vg.cs), P.yr);
+    const double S2 = P.zr;
     const double bin = ddiv(P.dpn, (double)P.H);
-    Pp[2] = dadd(dmul(dmul(-dadd(vg.yc, (double)j), P.piso), bin), ddiv(dmul(P.zr, P.piso), P.pdet));
+    const double P2 = dadd(dmul(dmul(-dadd(vg.yc, (double)j), P.piso), bin), ddiv(dmul(P.zr, P.piso), P.pdet));
     const double pr = dmul(dmul(P.piso, dadd(vg.xc, (double)jj)), bin);
-    Pp[0] = dadd(dmul(pr, vg.cs), ddiv(dmul(P.xr, P.piso), P.pdet));
-    Pp[1] = dadd(dmul(pr, vg.sn), ddiv(dmul(P.yr, P.piso), P.pdet));
+    const double P0 = dadd(dmul(pr, vg.cs), ddiv(dmul(P.xr, P.piso), P.pdet));
+    const double P1 = dadd(dmul(pr, vg.sn), ddiv(dmul(P.yr, P.piso), P.pdet));
     {
         const double d2 = dmul(P.sad, P.sad);
-        double l = ddiv(d2, dadd(d2, dadd(dmul(pr, pr), dmul(Pp[2], Pp[2]))));
+        double l = ddiv(d2, dadd(d2, dadd(dmul(pr, pr), dmul(P2, P2))));
         R.leng = (float)dmul(l, __dsqrt_rn(l));
     }
     R.active = 0;
@@ -115,79 +116,63 @@ __device__ void ray_setup(const ProjParams& P, const ViewGeom& vg, int j, int jj
     R.first_idx = -1;
     R.first_len = 0.0f;
 
-    // entry / exit against the four side planes (:154-183)
+    // entry / exit against the four side planes (:154-183); only the first
+    // two hits are used, so only they are kept
     const double hx = dmul((double)nxm, s), hy = dmul((double)nym, s);
-    double xx[4], yy[4], zz[4];
+    double hx0 = 0.0, hy0 = 0.0, hz0 = 0.0, hx1 = 0.0, hy1 = 0.0, hz1 = 0.0;
     int m = 0;
-    yy[m] = hy;
-    if (fabs(line_at(yy[m], S[1], Pp[1], S[0], Pp[0])) < hx) {
-        xx[m] = line_at(yy[m], S[1], Pp[1], S[0], Pp[0]);
-        zz[m] = line_at(yy[m], S[1], Pp[1], S[2], Pp[2]);
+    auto hit = [&](double x, double y, double z) {
+        if (m == 0) { hx0 = x; hy0 = y; hz0 = z; }
+        else if (m == 1) { hx1 = x; hy1 = y; hz1 = z; }
         m++;
-    }
-    yy[m] = -hy;
-    if (fabs(line_at(yy[m], S[1], Pp[1], S[0], Pp[0])) < hx) {
-        xx[m] = line_at(yy[m], S[1], Pp[1], S[0], Pp[0]);
-        zz[m] = line_at(yy[m], S[1], Pp[1], S[2], Pp[2]);
-        m++;
-    }
-    if (m < 4) {
-        xx[m] = hx;
-        if (fabs(line_at(xx[m], S[0], Pp[0], S[1], Pp[1])) < hy) {
-            yy[m] = line_at(xx[m], S[0], Pp[0], S[1], Pp[1]);
-            zz[m] = line_at(xx[m], S[0], Pp[0], S[2], Pp[2]);
-            m++;
-        }
-    }
-    if (m < 4) {
-        xx[m] = -hx;
-        if (fabs(line_at(xx[m], S[0], Pp[0], S[1], Pp[1])) < hy) {
-            yy[m] = line_at(xx[m], S[0], Pp[0], S[1], Pp[1]);
-            zz[m] = line_at(xx[m], S[0], Pp[0], S[2], Pp[2]);
-            m++;
-        }
-    }
+    };
+    if (fabs(line_at(hy, S1, P1, S0, P0)) < hx) hit(line_at(hy, S1, P1, S0, P0), hy, line_at(hy, S1, P1, S2, P2));
+    if (fabs(line_at(-hy, S1, P1, S0, P0)) < hx) hit(line_at(-hy, S1, P1, S0, P0), -hy, line_at(-hy, S1, P1, S2, P2));
+    if (fabs(line_at(hx, S0, P0, S1, P1)) < hy) hit(hx, line_at(hx, S0, P0, S1, P1), line_at(hx, S0, P0, S2, P2));
+    if (fabs(line_at(-hx, S0, P0, S1, P1)) < hy) hit(-hx, line_at(-hx, S0, P0, S1, P1), line_at(-hx, S0, P0, S2, P2));
     if (m < 2) return;
 
-    double I[3], F[3];
+    // entry I = the hit nearer the source, exit F = the other
+    double I0, I1, I2, F0, F1, F2;
     {
-        double e0 = dadd(dadd(dmul(dsub(xx[0], S[0]), dsub(xx[0], S[0])),
-                              dmul(dsub(yy[0], S[1]), dsub(yy[0], S[1]))),
-                         dmul(dsub(zz[0], S[2]), dsub(zz[0], S[2])));
-        double e1 = dadd(dadd(dmul(dsub(xx[1], S[0]), dsub(xx[1], S[0])),
-                              dmul(dsub(yy[1], S[1]), dsub(yy[1], S[1]))),
-                         dmul(dsub(zz[1], S[2]), dsub(zz[1], S[2])));
-        const int f = (e0 < e1) ? 0 : 1;
-        I[0] = xx[f]; I[1] = yy[f]; I[2] = zz[f];
-        F[0] = xx[1 - f]; F[1] = yy[1 - f]; F[2] = zz[1 - f];
+        const double e0 = dadd(dadd(dmul(dsub(hx0, S0), dsub(hx0, S0)), dmul(dsub(hy0, S1), dsub(hy0, S1))),
+                               dmul(dsub(hz0, S2), dsub(hz0, S2)));
+        const double e1 = dadd(dadd(dmul(dsub(hx1, S0), dsub(hx1, S0)), dmul(dsub(hy1, S1), dsub(hy1, S1))),
+                               dmul(dsub(hz1, S2), dsub(hz1, S2)));
+        const bool f0 = e0 < e1;
+        I0 = f0 ? hx0 : hx1; I1 = f0 ? hy0 : hy1; I2 = f0 ? hz0 : hz1;
+        F0 = f0 ? hx1 : hx0; F1 = f0 ? hy1 : hy0; F2 = f0 ? hz1 : hz0;
     }
-    // dominant axis, GPU twin rule (:198)
-    const int d = (fabs(dsub(I[0], F[0])) > fabs(dsub(I[1], F[1]))) ? 0 : 1;
-    const int o = 1 - d;
-    const double dF = dsub(F[d], I[d]);
-    const double pha = ddiv(dF, fabs(dsub(I[d], F[d])));
+    // dominant axis, GPU twin rule (:198); _d / _o name the dominant and the
+    // other in-plane axis
+    const int d = (fabs(dsub(I0, F0)) > fabs(dsub(I1, F1))) ? 0 : 1;
+    const double Id = d ? I1 : I0, Fd = d ? F1 : F0;
+    const double Sd = d ? S1 : S0, So = d ? S0 : S1;
+    const double Pd = d ? P1 : P0, Po = d ? P0 : P1;
+    const double dF = dsub(Fd, Id);
+    const double pha = ddiv(dF, fabs(dsub(Id, Fd)));
     if (!(pha == 1.0 || pha == -1.0)) return;
     int ain;
-    if ((I[d] < 0 && dF < 0) || (I[d] > 0 && dF > 0))
-        ain = d2i(dadd((double)d2i(I[d]), ddiv(dF, fabs(dF))));
+    if ((Id < 0 && dF < 0) || (Id > 0 && dF > 0))
+        ain = d2i(dadd((double)d2i(Id), ddiv(dF, fabs(dF))));
     else
-        ain = d2i(I[d]);
+        ain = d2i(Id);
     if (ain == INT_MIN) return;
 
     const double h = hx;  // hx == hy (both from reconSize)
     auto inb = [&](double k) {
         double a = dadd((double)ain, dmul(dmul(pha, k), s));
-        double ov = line_at(a, S[d], Pp[d], S[o], Pp[o]);
+        double ov = line_at(a, Sd, Pd, So, Po);
         return a <= h && a >= -h && ov <= h && ov >= -h;
     };
     if (!inb(0.0)) return;
 
     // first iteration whose step point leaves the box; the loop of the
     // reference (:212) executes it and stops.
-    const double go = ddiv(dsub(Pp[o], S[o]), dsub(Pp[d], S[d]));
-    const double gz = ddiv(dsub(Pp[2], S[2]), dsub(Pp[d], S[d]));
-    const double o0 = line_at((double)ain, S[d], Pp[d], S[o], Pp[o]);
-    const double z0 = line_at((double)ain, S[d], Pp[d], S[2], Pp[2]);
+    const double go = ddiv(dsub(Po, So), dsub(Pd, Sd));
+    const double gz = ddiv(dsub(P2, S2), dsub(Pd, Sd));
+    const double o0 = line_at((double)ain, Sd, Pd, So, Po);
+    const double z0 = line_at((double)ain, Sd, Pd, S2, P2);
     double kd = floor((h - pha * ain) / s) + 1.0;
     double ko = 1e30;
     const double vo = go * pha * s;
@@ -223,20 +208,18 @@ __device__ void ray_setup(const ProjParams& P, const ViewGeom& vg, int j, int jj
     // its voxel, length and mask are evaluated in FP64 exactly as the
     // reference does.
     {
-        double b1[3];
-        b1[d] = (double)ain;
-        b1[o] = o0;
-        b1[2] = z0;
-        const double* b0 = I;
-        const double rr = __dsqrt_rn(dadd(dadd(dmul(dsub(b0[0], b1[0]), dsub(b0[0], b1[0])),
-                                               dmul(dsub(b0[1], b1[1]), dsub(b0[1], b1[1]))),
-                                          dmul(dsub(b0[2], b1[2]), dsub(b0[2], b1[2]))));
-        const int xmc = d2i(dadd(ddiv(dmul(dadd(b0[0], b1[0]), 0.5), s), (double)nxm));
-        const int ymc = d2i(dadd(ddiv(dmul(dsub(-b0[1], b1[1]), 0.5), s), (double)nym));
-        const int zmc = d2i(dadd(ddiv(dmul(dsub(-b0[2], b1[2]), 0.5), step), (double)nzm));
+        const double b10 = d ? o0 : (double)ain;
+        const double b11 = d ? (double)ain : o0;
+        const double b12 = z0;
+        const double rr = __dsqrt_rn(dadd(dadd(dmul(dsub(I0, b10), dsub(I0, b10)),
+                                               dmul(dsub(I1, b11), dsub(I1, b11))),
+                                          dmul(dsub(I2, b12), dsub(I2, b12))));
+        const int xmc = d2i(dadd(ddiv(dmul(dadd(I0, b10), 0.5), s), (double)nxm));
+        const int ymc = d2i(dadd(ddiv(dmul(dsub(-I1, b11), 0.5), s), (double)nym));
+        const int zmc = d2i(dadd(ddiv(dmul(dsub(-I2, b12), 0.5), step), (double)nzm));
         if (xmc >= 0 && ymc >= 0 && zmc >= 0 && xmc <= P.N - 1 && ymc <= P.N - 1 && zmc <= P.Z - 1) {
-            const double r = dmul(__dsqrt_rn(dadd(dmul(dadd(b0[0], b1[0]), dadd(b0[0], b1[0])),
-                                                  dmul(dsub(-b0[1], b1[1]), dsub(-b0[1], b1[1])))), 0.5);
+            const double r = dmul(__dsqrt_rn(dadd(dmul(dadd(I0, b10), dadd(I0, b10)),
+                                                  dmul(dsub(-I1, b11), dsub(-I1, b11)))), 0.5);
             if (!(r >= dmul(dmul((double)P.N, 0.5), s))) {
                 R.first_idx = (ymc * P.N + xmc) * P.Z + zmc;
                 R.first_len = (float)rr;
@@ -408,6 +391,19 @@ __device__ __forceinline__ void march(const ProjParams& P, const RayPlan& R, int
 }
 
 // -------------------------------------------------------------- visitors --
+// uint16 halves of a packed word as exact floats without the conversion
+// unit: the 16 bits are placed in the mantissa of 2^23 (0x4B000000 | u) and
+// 2^23 is subtracted, both exact.  A byte permute and an FADD run on the
+// integer and FMA pipes, which have 4-8x the throughput of I2F.
+__device__ __forceinline__ float u16lo(unsigned w)
+{
+    return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7410)) - 8388608.0f;
+}
+__device__ __forceinline__ float u16hi(unsigned w)
+{
+    return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7432)) - 8388608.0f;
+}
+
 template <int M>
 struct AccumU16 {
     const uint4* __restrict__ vol;
@@ -417,39 +413,20 @@ struct AccumU16 {
     unsigned nseg;
     __device__ __forceinline__ void add(const uint4 v, float len)
     {
-        Lp[0] = fmaf((float)(v.x & 0xFFFFu), len, Lp[0]);
-        Lp[1] = fmaf((float)(v.x >> 16), len, Lp[1]);
-        Lp[2] = fmaf((float)(v.y & 0xFFFFu), len, Lp[2]);
-        Lp[3] = fmaf((float)(v.y >> 16), len, Lp[3]);
-        Lp[4] = fmaf((float)(v.z & 0xFFFFu), len, Lp[4]);
-        Lp[5] = fmaf((float)(v.z >> 16), len, Lp[5]);
+        Lp[0] = fmaf(u16lo(v.x), len, Lp[0]);
+        Lp[1] = fmaf(u16hi(v.x), len, Lp[1]);
+        Lp[2] = fmaf(u16lo(v.y), len, Lp[2]);
+        Lp[3] = fmaf(u16hi(v.y), len, Lp[3]);
+        Lp[4] = fmaf(u16lo(v.z), len, Lp[4]);
+        Lp[5] = fmaf(u16hi(v.z), len, Lp[5]);
         if (M > 6) {
-            Lp[6 % M] = fmaf((float)(v.w & 0xFFFFu), len, Lp[6 % M]);
-            Lp[7 % M] = fmaf((float)(v.w >> 16), len, Lp[7 % M]);
+            Lp[6 % M] = fmaf(u16lo(v.w), len, Lp[6 % M]);
+            Lp[7 % M] = fmaf(u16hi(v.w), len, Lp[7 % M]);
         }
-    }
-    __device__ __forceinline__ void pair(bool va, int ia, float la, bool vb, int ib, float lb)
-    {
-        const uint4 zero = make_uint4(0, 0, 0, 0);
-        const uint4 A = va ? __ldg(vol + ia) : zero;
-        const uint4 B = vb ? __ldg(vol + ib) : zero;
-        add(A, la);
-        add(B, lb);
-        nseg += (unsigned)va + (unsigned)vb;
     }
     __device__ __forceinline__ void operator()(int idx, float len)
     {
-        const uint4 v = __ldg(vol + idx);
-        Lp[0] = fmaf((float)(v.x & 0xFFFFu), len, Lp[0]);
-        Lp[1] = fmaf((float)(v.x >> 16), len, Lp[1]);
-        Lp[2] = fmaf((float)(v.y & 0xFFFFu), len, Lp[2]);
-        Lp[3] = fmaf((float)(v.y >> 16), len, Lp[3]);
-        Lp[4] = fmaf((float)(v.z & 0xFFFFu), len, Lp[4]);
-        Lp[5] = fmaf((float)(v.z >> 16), len, Lp[5]);
-        if (M > 6) {
-            Lp[6 % M] = fmaf((float)(v.w & 0xFFFFu), len, Lp[6 % M]);
-            Lp[7 % M] = fmaf((float)(v.w >> 16), len, Lp[7 % M]);
-        }
+        add(__ldg(vol + idx), len);
         nseg++;
     }
 };
@@ -461,11 +438,6 @@ struct AccumF32 {
     float L[M];
     float Lp[M];
     unsigned nseg;
-    __device__ __forceinline__ void pair(bool va, int ia, float la, bool vb, int ib, float lb)
-    {
-        if (va) (*this)(ia, la);
-        if (vb) (*this)(ib, lb);
-    }
     __device__ __forceinline__ void operator()(int idx, float len)
     {
         const float4* p = vol + 2 * (size_t)idx;
@@ -484,20 +456,22 @@ struct AccumF32 {
     }
 };
 
+// Scatter of one segment's gradient into the packed float records: one
+// 16-byte vector reduction for elements 0-3 and one 8-byte (M = 6) or
+// 16-byte (M = 8) reduction for the rest.
+template <int M>
 struct Scatter {
     float4* __restrict__ grad;
     int N, Z;
     float g[8];
-    __device__ __forceinline__ void pair(bool va, int ia, float la, bool vb, int ib, float lb)
-    {
-        if (va) (*this)(ia, la);
-        if (vb) (*this)(ib, lb);
-    }
     __device__ __forceinline__ void operator()(int idx, float len)
     {
         float4* p = grad + 2 * (size_t)idx;
         atomicAdd(p, make_float4(g[0] * len, g[1] * len, g[2] * len, g[3] * len));
-        atomicAdd(p + 1, make_float4(g[4] * len, g[5] * len, g[6] * len, g[7] * len));
+        if (M > 6)
+            atomicAdd(p + 1, make_float4(g[4] * len, g[5] * len, g[6] * len, g[7] * len));
+        else
+            atomicAdd(reinterpret_cast<float2*>(p + 1), make_float2(g[4] * len, g[5] * len));
     }
 };
 
@@ -868,7 +842,9 @@ __device__ __forceinline__ void forward_tile(const ForwardArgs& a, const float4*
     if (!valid) return;
     const size_t o = ((size_t)v * P.H + (P.H - 1 - j)) * P.W + jj;
     if (a.L_out) {
-        for (int i = 0; i < P.nmat; i++) a.L_out[o * P.nmat + i] = L[i];
+#pragma unroll
+        for (int i = 0; i < M; i++)
+            if (i < P.nmat) a.L_out[o * P.nmat + i] = L[i];
     }
     if (a.out) a.out[o] = spectral_sum<M>(s_mu, s_pdf, a.spec.NE, L) * R.leng;
 }
@@ -898,13 +874,19 @@ __global__ void __launch_bounds__(256) forward_kernel(ForwardArgs a)
 // and within an item by row band, then view, then column block (the order of
 // forward_kernel's grid), so the items' uneven view and slice counts
 // load-balance across the whole GPU in one launch.
+// The current item's arguments are staged in shared memory, so the march
+// reads them like forward_kernel reads its parameters (no global loads or
+// registers held for them); the bounds cap registers as forward_kernel's.
 template <int M>
 __global__ void __launch_bounds__(256) batch_forward_kernel(const BatchItem* __restrict__ items, int nitems,
-                                                            long long total, int NEmax,
-                                                            unsigned long long* counter)
+                                                               long long total, int NEmax,
+                                                               unsigned long long* counter)
 {
     extern __shared__ float4 smem[];
     __shared__ long long s_unit;
+    __shared__ ForwardArgs s_fa;
+    __shared__ long long s_begin;
+    __shared__ int s_ncolb;
     float4* s_mu = smem;
     float* s_pdf = reinterpret_cast<float*>(smem + 2 * NEmax);
     IvRec* s_iv = iv_buffer(smem, NEmax);
@@ -920,18 +902,22 @@ __global__ void __launch_bounds__(256) batch_forward_kernel(const BatchItem* __r
             if (items[mid].unit_begin <= u) lo = mid;
             else hi = mid - 1;
         }
-        const BatchItem& it = items[lo];
-        if (lo != cur) {
-            load_spectrum(it.fa.spec, s_mu, s_pdf);
+        if (lo != cur) {  // block-uniform
+            if (threadIdx.x == 0 && threadIdx.y == 0) {
+                s_fa = items[lo].fa;
+                s_begin = items[lo].unit_begin;
+                s_ncolb = items[lo].ncolb;
+            }
+            load_spectrum(items[lo].fa.spec, s_mu, s_pdf);
             cur = lo;
         }
         __syncthreads();
-        const long long w = u - it.unit_begin;
-        const int colb = (int)(w % it.ncolb);
-        const long long rest = w / it.ncolb;
-        const int v = (int)(rest % it.fa.p.V);
-        const int rowt = (int)(rest / it.fa.p.V);
-        forward_tile<M, false, false>(it.fa, s_mu, s_pdf, s_iv, v, rowt, colb);
+        const long long w = u - s_begin;
+        const int colb = (int)(w % s_ncolb);
+        const long long rest = w / s_ncolb;
+        const int v = (int)(rest % s_fa.p.V);
+        const int rowt = (int)(rest / s_fa.p.V);
+        forward_tile<M, false, false>(s_fa, s_mu, s_pdf, s_iv, v, rowt, colb);
         __syncthreads();
     }
 }
@@ -990,7 +976,7 @@ __global__ void __launch_bounds__(256) adjoint_kernel(AdjointArgs a)
         g[6] = fmaf(w, m1.z, g[6]); g[7] = fmaf(w, m1.w, g[7]);
     }
     const float scale = -R.leng * r;
-    Scatter sc{a.grad_packed, P.N, P.Z, {}};
+    Scatter<M> sc{a.grad_packed, P.N, P.Z, {}};
 #pragma unroll
     for (int i = 0; i < 8; i++) sc.g[i] = g[i] * scale;
     // pass 2: scatter along the same segments

@@ -30,6 +30,11 @@ def _dp(a):
     return np.ascontiguousarray(a, np.float64).ctypes.data_as(C.POINTER(C.c_double))
 
 
+def _volume_key(kind, t):
+    """Identity of a loaded device volume: storage, version counter, shape."""
+    return (kind, t.data_ptr(), t._version, tuple(t.shape))
+
+
 class Projector:
     """Polychromatic material-based forward projector on one GPU."""
 
@@ -46,6 +51,7 @@ class Projector:
                                          C.byref(h)))
         self._h = h
         self.NE = 0
+        self.loaded = None  # key of the device volume last loaded, if any
 
     def close(self):
         if getattr(self, "_h", None) is not None and self._h.value:
@@ -86,9 +92,11 @@ class Projector:
             v = vol.contiguous()
             N.check(L.vcbct_projector_load_volume(self._h, C.c_void_p(v.data_ptr()), 1, _stream_ptr(stream)))
             self._vol_ref = v
+            self.loaded = _volume_key("u16", v)
         else:
             v = np.ascontiguousarray(vol, np.uint16)
             N.check(L.vcbct_projector_load_volume(self._h, C.c_void_p(v.ctypes.data), 0, None))
+            self.loaded = None
 
     def load_volume_f32(self, vol, stream=None):
         """float32 [Z][nmat][N][N] element volume (host numpy or CUDA torch)."""
@@ -98,9 +106,11 @@ class Projector:
             v = vol.contiguous()
             N.check(L.vcbct_projector_load_volume_f32(self._h, C.c_void_p(v.data_ptr()), 1, _stream_ptr(stream)))
             self._vol_ref = v
+            self.loaded = _volume_key("f32", v)
         else:
             v = np.ascontiguousarray(vol, np.float32)
             N.check(L.vcbct_projector_load_volume_f32(self._h, C.c_void_p(v.ctypes.data), 0, None))
+            self.loaded = None
 
     # ------------------------------------------------------------ outputs --
     def forward(self, out=None, stream=None):
@@ -191,7 +201,14 @@ class Batch:
         N.check(N.lib().vcbct_batch_forward(self._h, int(bool(use_graph)), _stream_ptr(stream)))
         return [o for _, o in self._items]
 
+    def configure(self, per_item: bool = False, cols_per_block: int = 4):
+        """Fix the launch strategy: one persistent launch (per_item=False) or
+        per-item launches on two graph branches; and the columns per block."""
+        N.check(N.lib().vcbct_batch_configure(self._h, int(bool(per_item)), int(cols_per_block)))
+
     def autotune(self, stream=None) -> int:
+        """Time both strategies x {2, 4, 8} columns per block and keep the
+        fastest; returns columns per block, +100 for per-item launches."""
         c = C.c_int(0)
         N.check(N.lib().vcbct_batch_autotune(self._h, _stream_ptr(stream), C.byref(c)))
         return c.value
