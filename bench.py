@@ -405,6 +405,19 @@ def run_ours(args, rank, world, local_rank):
         extra["decomposition"] = decomposition_section(stream)
         extra["batched"] = batched_section(stream, args)
 
+    # measured gather rooflines: the projector's and the backprojector's
+    # access patterns replayed without arithmetic on this device
+    probe_fwd = vc.probe_gather(0) / 1e9
+    probe_bp_smem = vc.probe_gather(1) / 1e9
+    probe_bp_l1 = vc.probe_gather(2) / 1e9
+    gather_roof = {
+        "mbfpa": {"pattern": "ray-front 16-B record gather (11-record runs, stride Z)",
+                  "peak_gseg_s": probe_fwd, "achieved_gseg_s": value, "frac": value / probe_fwd},
+        "bp": {"pattern": "bilinear detector-tile gather", "peak_gups_shared": probe_bp_smem,
+               "peak_gups_l1": probe_bp_l1, "achieved_gups": gups,
+               "frac": gups / max(probe_bp_smem, probe_bp_l1)},
+    }
+
     peak, peak_kind = measured_peaks()
     alg_bytes = 12.0 * nseg
     achieved = alg_bytes / (ms * 1e-3) / 1e9
@@ -426,6 +439,7 @@ def run_ours(args, rank, world, local_rank):
                 "bp_ms": ms_bp, "bp_gups": gups,
                 "short_volume_range": [int(vi.min().item()), int(vi.max().item())]},
         "clocks": clk,
+        "gather_roof": gather_roof,
     }
     res.update(extra)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -30,11 +30,11 @@ def test_float_volume_forward_matches_oracle(cuda):
     assert np.max(np.abs(out - ref) / ref) <= 1e-5
 
 
-@pytest.mark.parametrize("seed", [0, 4])
-def test_adjoint_matches_fp64_gradient(cuda, seed):
+@pytest.mark.parametrize("seed,zreg", [(0, 0.3), (4, 0.3), (2, 0.0)])
+def test_adjoint_matches_fp64_gradient(cuda, seed, zreg):
     import torch
     from virtualcbct_b200.autograd import project
-    g, tabs, volf = _float_case(seed)
+    g, tabs, volf = _float_case(seed, z_reg=zreg)
     mu, pdf = spectrum()
     rng = np.random.default_rng(100 + seed)
     resid = rng.normal(size=(g.V, g.H, g.W)).astype(np.float32)

@@ -37,6 +37,10 @@ CASES = [
     ("random", 9, dict(N=40, Z=24, s=0.07, step=0.13, V=3)),
     # steeper than one slice per step: the per-step march path
     ("random", 6, dict(N=32, Z=64, s=0.3, step=0.02, V=2, W=24, H=40, dpn=900.0)),
+    # z_reg = 0: the central detector row lies exactly in the z = 0 plane, a
+    # slice boundary (the reference's (int)(nzm - z/step) rule applies)
+    ("ellipsoid", 7, dict(z_reg=0.0, V=6)),
+    ("random", 8, dict(z_reg=0.0, N=32, Z=64, s=0.3, step=0.02, V=2, W=24, H=40, dpn=900.0)),
 ]
 
 

@@ -107,6 +107,7 @@ SIGNATURES = {
     "vcbct_batch_autotune": (C.c_int, [_vp, _vp, _ip]),
     "vcbct_mbfpa_forward_noalloc": (C.c_int, [C.POINTER(ProjGeometryC), _dp, _dp, _dp, _dp, _vp, _fp,
                                               _fp, C.c_int, C.c_double, _vp, _vp]),
+    "vcbct_probe_gather": (C.c_int, [C.c_int, _dp, _vp]),
     "vcbct_proj_trig_tables": (C.c_int, [C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, C.c_double,
                                          C.c_double, _dp, _dp, _dp, _dp]),
     "vcbct_attenuation_table": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int, C.c_int, _fp, _fp, _ip]),

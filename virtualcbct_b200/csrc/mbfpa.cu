@@ -265,6 +265,16 @@ __device__ __forceinline__ int trunc_index(int q, int size)
     return ((unsigned)(q + 1) <= (unsigned)size) ? max(q, 0) : -1;
 }
 
+// Slice index of a ray with Z1 == 0 (it stays in the plane z = Z0 * step;
+// with z_reg = 0 the central detector row does).  The reference's rule
+// (int)(nzm - z/step) differs from the cell rule when Z0 is an integer (the
+// midpoints then lie exactly on a slice boundary), so it is applied as is.
+__device__ __forceinline__ int flat_z_index(const ProjParams& P, double Z0)
+{
+    const double q = (double)(int)(P.Z * 0.5) - Z0;
+    return (q > -1.0 && q < (double)P.Z) ? (int)q : -1;
+}
+
 // Anchor of an axis at parameter t (FP64 value v = c0 + c1 t).
 __device__ __forceinline__ Axis make_axis(double c0, double c1, double t)
 {
@@ -324,6 +334,8 @@ __device__ __forceinline__ void march(const ProjParams& P, const RayPlan& R, int
         tz_next = cross_t(R.Z0, invZ1, mz);
     }
 
+    const int izflat = dirz ? -1 : flat_z_index(P, R.Z0);
+
     // One segment [ta, tb] within the step whose start is t = tbase, where the
     // dominant cell base is Idk.
     auto segment = [&](float ta, float tb, float tbase, int Idk) {
@@ -340,7 +352,7 @@ __device__ __forceinline__ void march(const ProjParams& P, const RayPlan& R, int
         const int cy = d ? cd : co;
         const int ix = trunc_index(nxm + cx, P.N);
         const int iy = trunc_index(nym - 1 - cy, P.N);
-        const int iz = trunc_index(nzm - 1 - cz, P.Z);
+        const int iz = dirz ? trunc_index(nzm - 1 - cz, P.Z) : izflat;
         if ((ix | iy | iz) < 0) return;
         if (!(fmaf(vd, vd, vo * vo) < R2)) return;
         visit((iy * P.N + ix) * P.Z + iz, fabsf(tb - ta) * R.Lt);
@@ -603,8 +615,10 @@ __device__ __forceinline__ void zstate_init(const ProjParams& P, const RayPlan& 
         if (z.mz == 0) z.mz += z.dirz;
         z.tz_next = zcross(R, z.mz);
         if ((z.dirz > 0 && v < 0.0) || (z.dirz < 0 && v > 0.0)) z.tz0 = zcross(R, 0);
+        z.iz = trunc_index(nzm - 1 - z.cz, P.Z);
+    } else {
+        z.iz = flat_z_index(P, R.Z0);
     }
-    z.iz = trunc_index(nzm - 1 - z.cz, P.Z);
 }
 
 // One interval, exact: split it at the z planes inside it (and apply the
