@@ -29,8 +29,9 @@ def _run(prog, deck, cwd):
     return r
 
 
-def test_proj_then_cbct2_from_decks(cuda, tmp_path):
+def test_proj_then_cbct2_from_decks(cuda, tmp_path, monkeypatch):
     tmp = str(tmp_path)
+    monkeypatch.chdir(tmp)  # deck paths are relative to the current directory
     N, slices, z_ic, V, W, H = 48, 40, 20, 36, 40, 32
     s, step = 0.2, 0.5
     vol_all = phantoms.ellipsoid_phantom(N, slices, s, step, seed=11)

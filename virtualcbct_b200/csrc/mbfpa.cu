@@ -403,67 +403,108 @@ __device__ __forceinline__ void march(const ProjParams& P, const RayPlan& R, int
 }
 
 // -------------------------------------------------------------- visitors --
-// uint16 halves of a packed word as exact floats without the conversion
-// unit: the 16 bits are placed in the mantissa of 2^23 (0x4B000000 | u) and
-// 2^23 is subtracted, both exact.  A byte permute and an FADD run on the
-// integer and FMA pipes, which have 4-8x the throughput of I2F.
-__device__ __forceinline__ float u16lo(unsigned w)
+// Partial sums are kept as pairs of floats and updated with Blackwell's
+// packed f32x2 add / fma (one instruction for two elements, each element
+// rounded exactly as the scalar fmaf / fadd would round it).
+typedef unsigned long long f32x2;
+
+__device__ __forceinline__ f32x2 f2pack(float a, float b)
 {
-    return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7410)) - 8388608.0f;
+    f32x2 r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+    return r;
 }
-__device__ __forceinline__ float u16hi(unsigned w)
+__device__ __forceinline__ void f2unpack(f32x2 r, float& a, float& b)
 {
-    return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7432)) - 8388608.0f;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(r));
+}
+__device__ __forceinline__ f32x2 fadd2(f32x2 a, f32x2 b)
+{
+    f32x2 r;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ f32x2 ffma2(f32x2 a, f32x2 b, f32x2 c)
+{
+    f32x2 r;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+    return r;
 }
 
+// Both uint16 halves of a packed word as exact floats {low, high} without
+// the conversion unit: each half is placed in the mantissa of 2^23
+// (0x4B000000 | u, a byte permute) and 2^23 is subtracted (exact).
+__device__ __forceinline__ f32x2 u16pair(unsigned w)
+{
+    const float lo = __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7410));
+    const float hi = __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7432));
+    return fadd2(f2pack(lo, hi), 0xCB000000CB000000ull);  // {-2^23, -2^23}
+}
+
+// Two-level sums: segments accumulate into the pairs P2 (element 2i in the
+// low half, 2i+1 in the high half); fold() adds them into L every 32
+// iterations, which bounds the FP32 error growth.
 template <int M>
-struct AccumU16 {
-    const uint4* __restrict__ vol;
-    int N, Z;
+struct PairSums {
+    static constexpr int NP = (M + 1) / 2;
     float L[M];
-    float Lp[M];
-    unsigned nseg;
-    __device__ __forceinline__ void add(const uint4 v, float len)
+    f32x2 P2[NP];
+    __device__ __forceinline__ void clear()
     {
-        Lp[0] = fmaf(u16lo(v.x), len, Lp[0]);
-        Lp[1] = fmaf(u16hi(v.x), len, Lp[1]);
-        Lp[2] = fmaf(u16lo(v.y), len, Lp[2]);
-        Lp[3] = fmaf(u16hi(v.y), len, Lp[3]);
-        Lp[4] = fmaf(u16lo(v.z), len, Lp[4]);
-        Lp[5] = fmaf(u16hi(v.z), len, Lp[5]);
-        if (M > 6) {
-            Lp[6 % M] = fmaf(u16lo(v.w), len, Lp[6 % M]);
-            Lp[7 % M] = fmaf(u16hi(v.w), len, Lp[7 % M]);
+#pragma unroll
+        for (int i = 0; i < M; i++) L[i] = 0.0f;
+#pragma unroll
+        for (int i = 0; i < NP; i++) P2[i] = 0ull;
+    }
+    __device__ __forceinline__ void fold()
+    {
+#pragma unroll
+        for (int i = 0; i < NP; i++) {
+            float a, b;
+            f2unpack(P2[i], a, b);
+            L[2 * i] += a;
+            if (2 * i + 1 < M) L[2 * i + 1] += b;
+            P2[i] = 0ull;
         }
     }
+    __device__ __forceinline__ void zero_L()
+    {
+#pragma unroll
+        for (int i = 0; i < M; i++) L[i] = 0.0f;
+    }
+};
+
+template <int M>
+struct AccumU16 : PairSums<M> {
+    const uint4* __restrict__ vol;
+    unsigned nseg;
+    __device__ __forceinline__ AccumU16(const uint4* v) : vol(v), nseg(0u) { this->clear(); }
     __device__ __forceinline__ void operator()(int idx, float len)
     {
-        add(__ldg(vol + idx), len);
+        const uint4 v = __ldg(vol + idx);
+        const f32x2 l2 = f2pack(len, len);
+        this->P2[0] = ffma2(u16pair(v.x), l2, this->P2[0]);
+        this->P2[1] = ffma2(u16pair(v.y), l2, this->P2[1]);
+        this->P2[2] = ffma2(u16pair(v.z), l2, this->P2[2]);
+        if (M > 6) this->P2[3 % PairSums<M>::NP] = ffma2(u16pair(v.w), l2, this->P2[3 % PairSums<M>::NP]);
         nseg++;
     }
 };
 
 template <int M>
-struct AccumF32 {
+struct AccumF32 : PairSums<M> {
     const float4* __restrict__ vol;
-    int N, Z;
-    float L[M];
-    float Lp[M];
     unsigned nseg;
+    __device__ __forceinline__ AccumF32(const float4* v) : vol(v), nseg(0u) { this->clear(); }
     __device__ __forceinline__ void operator()(int idx, float len)
     {
-        const float4* p = vol + 2 * (size_t)idx;
-        const float4 a = __ldg(p), b = __ldg(p + 1);
-        Lp[0] = fmaf(a.x, len, Lp[0]);
-        Lp[1] = fmaf(a.y, len, Lp[1]);
-        Lp[2] = fmaf(a.z, len, Lp[2]);
-        Lp[3] = fmaf(a.w, len, Lp[3]);
-        Lp[4] = fmaf(b.x, len, Lp[4]);
-        Lp[5] = fmaf(b.y, len, Lp[5]);
-        if (M > 6) {
-            Lp[6 % M] = fmaf(b.z, len, Lp[6 % M]);
-            Lp[7 % M] = fmaf(b.w, len, Lp[7 % M]);
-        }
+        const ulonglong2* p = reinterpret_cast<const ulonglong2*>(vol + 2 * (size_t)idx);
+        const ulonglong2 a = __ldg(p), b = __ldg(p + 1);
+        const f32x2 l2 = f2pack(len, len);
+        this->P2[0] = ffma2(a.x, l2, this->P2[0]);
+        this->P2[1] = ffma2(a.y, l2, this->P2[1]);
+        this->P2[2] = ffma2(b.x, l2, this->P2[2]);
+        if (M > 6) this->P2[3 % PairSums<M>::NP] = ffma2(b.y, l2, this->P2[3 % PairSums<M>::NP]);
         nseg++;
     }
 };
@@ -729,20 +770,18 @@ __device__ __forceinline__ void march_intervals(const ProjParams& P, const RayPl
     }
 }
 
-// Two-level summation: the visitor accumulates into Lp; every 32 iterations
+// Two-level summation: the visitor accumulates into its pair sums; every 32 iterations
 // the partials are folded into L (bounds the FP32 error growth).
 template <class Acc, int M>
 __device__ __forceinline__ void march_accumulate(const ProjParams& P, const RayPlan& R, int Klo,
                                                  int Khi, Acc& acc)
 {
-#pragma unroll
-    for (int i = 0; i < M; i++) { acc.L[i] = 0.0f; acc.Lp[i] = 0.0f; }
+    acc.clear();
     if (R.first_idx >= 0) acc(R.first_idx, R.first_len);
     for (int k0 = Klo; k0 <= Khi; k0 += 32) {
         const int k1 = min(Khi, k0 + 31);
         march(P, R, k0, k1, acc);
-#pragma unroll
-        for (int i = 0; i < M; i++) { acc.L[i] += acc.Lp[i]; acc.Lp[i] = 0.0f; }
+        acc.fold();
     }
 }
 
@@ -795,20 +834,16 @@ template <class Acc, int M>
 __device__ __forceinline__ void ray_integrals(const ProjParams& P, const RayPlan& R, bool act,
                                               int Klo, int Khi, IvRec* wbuf, Acc& acc)
 {
-#pragma unroll
-    for (int i = 0; i < M; i++) { acc.L[i] = 0.0f; acc.Lp[i] = 0.0f; }
+    acc.clear();
     if (!R.active) return;
     const bool steep = __any_sync(0xffffffffu, fabs(R.Z1) >= 1.0);
     if (steep) {
         march_accumulate<Acc, M>(P, R, Klo, Khi, acc);
-        if (!act) for (int i = 0; i < M; i++) acc.L[i] = 0.0f;
+        if (!act) acc.zero_L();
         return;
     }
     if (act && R.first_idx >= 0) acc(R.first_idx, R.first_len);
-    auto fold = [&]() {
-#pragma unroll
-        for (int i = 0; i < M; i++) { acc.L[i] += acc.Lp[i]; acc.Lp[i] = 0.0f; }
-    };
+    auto fold = [&]() { acc.fold(); };
     if (Klo <= Khi) march_intervals(P, R, act, Klo, Khi, wbuf, acc, fold);
     fold();
 }
@@ -837,13 +872,13 @@ __device__ __forceinline__ void forward_tile(const ForwardArgs& a, const float4*
     float L[M];
     unsigned nseg = 0;
     if (F32VOL) {
-        AccumF32<M> acc{a.vol_f32, P.N, P.Z, {}, {}, 0u};
+        AccumF32<M> acc(a.vol_f32);
         ray_integrals<AccumF32<M>, M>(P, R, valid, Klo, Khi, wbuf, acc);
 #pragma unroll
         for (int i = 0; i < M; i++) L[i] = acc.L[i];
         nseg = acc.nseg;
     } else {
-        AccumU16<M> acc{a.vol_u16, P.N, P.Z, {}, {}, 0u};
+        AccumU16<M> acc(a.vol_u16);
         ray_integrals<AccumU16<M>, M>(P, R, valid, Klo, Khi, wbuf, acc);
 #pragma unroll
         for (int i = 0; i < M; i++) L[i] = acc.L[i];
@@ -872,8 +907,18 @@ __device__ __forceinline__ IvRec* iv_buffer(float4* smem, int NEmax)
 // Blocks are dispatched view-fastest within a band of 32 detector rows, so
 // the blocks resident at a time share one z band of the volume (L2 reuse
 // across views).
+// Register cap of the forward kernel: minimum resident 256-thread blocks per
+// SM (0 leaves the choice to the compiler).
+#ifndef VCBCT_FWD_MIN_BLOCKS
+#define VCBCT_FWD_MIN_BLOCKS 0
+#endif
+#if VCBCT_FWD_MIN_BLOCKS > 0
+#define VCBCT_FWD_BOUNDS __launch_bounds__(256, VCBCT_FWD_MIN_BLOCKS)
+#else
+#define VCBCT_FWD_BOUNDS __launch_bounds__(256)
+#endif
 template <int M, bool F32VOL, bool COUNT>
-__global__ void __launch_bounds__(256) forward_kernel(ForwardArgs a)
+__global__ void VCBCT_FWD_BOUNDS forward_kernel(ForwardArgs a)
 {
     extern __shared__ float4 smem[];
     float4* s_mu = smem;
@@ -937,7 +982,7 @@ __global__ void __launch_bounds__(256) batch_forward_kernel(const BatchItem* __r
 }
 
 template <int M>
-__global__ void __launch_bounds__(256) adjoint_kernel(AdjointArgs a)
+__global__ void __launch_bounds__(256, 2) adjoint_kernel(AdjointArgs a)
 {
     extern __shared__ float4 smem[];
     float4* s_mu = smem;
@@ -966,7 +1011,7 @@ __global__ void __launch_bounds__(256) adjoint_kernel(AdjointArgs a)
     if (!__any_sync(0xffffffffu, act && R.active)) return;
 
     // pass 1: recompute the per-element path integrals of this ray
-    AccumF32<M> acc{a.vol_f32, P.N, P.Z, {}, {}, 0u};
+    AccumF32<M> acc(a.vol_f32);
     ray_integrals<AccumF32<M>, M>(P, R, act, Klo, Khi, wbuf, acc);
 
     // d I / d L_k = -leng * sum_E pdf_E mu'_k(E) exp(-sum_k mu'_k(E) L_k)
