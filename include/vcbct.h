@@ -119,6 +119,15 @@ int vcbct_projector_count_segments(vcbct_projector* p, unsigned long long* total
  * recomputed, not stored. */
 int vcbct_projector_adjoint(vcbct_projector* p, const float* d_grad_out, float* d_grad,
                             void* stream);
+/* The same pair with the per-ray element path integrals L[V][H][W][nmat]
+ * (device, float) kept between them: vcbct_projector_forward_state writes
+ * the projection d_out [V][H][W] and L in one launch, and
+ * vcbct_projector_adjoint_state reads L instead of re-marching each ray to
+ * recompute it; the per-ray spectral derivatives are still recomputed from L.
+ * Results are bitwise those of vcbct_projector_forward / _adjoint. */
+int vcbct_projector_forward_state(vcbct_projector* p, float* d_out, float* d_L, void* stream);
+int vcbct_projector_adjoint_state(vcbct_projector* p, const float* d_L, const float* d_grad_out,
+                                  float* d_grad, void* stream);
 
 /* Batched projection (no reference counterpart; the reference projects one
  * phantom per process run).  Items are projector objects holding a uint16

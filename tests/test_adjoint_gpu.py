@@ -30,10 +30,12 @@ def test_float_volume_forward_matches_oracle(cuda):
     assert np.max(np.abs(out - ref) / ref) <= 1e-5
 
 
-@pytest.mark.parametrize("seed,zreg", [(0, 0.3), (4, 0.3), (2, 0.0)])
-def test_adjoint_matches_fp64_gradient(cuda, seed, zreg):
+@pytest.mark.parametrize("seed,zreg,keep", [(0, 0.3, True), (4, 0.3, False), (2, 0.0, True), (2, 0.0, False)])
+def test_adjoint_matches_fp64_gradient(cuda, seed, zreg, keep):
+    """Both backward forms: path integrals kept from the forward launch, or
+    recomputed by a first march (keep_limit = 0)."""
     import torch
-    from virtualcbct_b200.autograd import project
+    from virtualcbct_b200.autograd import KEEP_LIMIT, project
     g, tabs, volf = _float_case(seed, z_reg=zreg)
     mu, pdf = spectrum()
     rng = np.random.default_rng(100 + seed)
@@ -41,7 +43,7 @@ def test_adjoint_matches_fp64_gradient(cuda, seed, zreg):
     p = Projector(g, *tabs)
     p.set_spectrum(mu, pdf, 1000.0)
     v = torch.from_numpy(volf).to(cuda).requires_grad_(True)
-    out = project(v, p)
+    out = project(v, p, KEEP_LIMIT if keep else 0)
     (out * torch.from_numpy(resid).to(cuda)).sum().backward()
     gpu = v.grad.cpu().numpy().astype(np.float64)
     ref = O.mbfpa_adjoint(g, tabs, volf, mu, pdf, 1000.0, resid.astype(np.float64))
@@ -85,3 +87,21 @@ def test_adjoint_matches_central_finite_differences(cuda):
         fd = (loss64(vp.astype(np.float32)) - loss64(vm.astype(np.float32))) / (2 * h)
         errs.append(abs(fd - grad[idx]) / max(abs(grad[idx]), 1e-30))
     assert np.median(errs) <= 1e-3 and np.max(errs) <= 2e-2
+
+
+def test_forward_state_is_forward_plus_path_integrals(cuda):
+    import torch
+    g, tabs, volf = _float_case(3)
+    mu, pdf = spectrum()
+    p = Projector(g, *tabs)
+    p.set_spectrum(mu, pdf, 1000.0)
+    p.load_volume_f32(torch.from_numpy(volf).to(cuda))
+    out, L = p.forward_state()
+    assert torch.equal(out, p.forward())
+    assert torch.equal(L, p.path_integrals())
+    rng = np.random.default_rng(7)
+    go = torch.from_numpy(rng.normal(size=(g.V, g.H, g.W)).astype(np.float32)).to(cuda)
+    a = p.adjoint(go).double()
+    b = p.adjoint_state(L, go).double()
+    # the same contributions; only the order of the atomic additions differs
+    assert (a - b).abs().max().item() <= 1e-5 * a.abs().max().item()

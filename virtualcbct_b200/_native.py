@@ -98,6 +98,8 @@ SIGNATURES = {
     "vcbct_projector_path_integrals": (C.c_int, [_vp, _vp, _vp]),
     "vcbct_projector_count_segments": (C.c_int, [_vp, C.POINTER(C.c_ulonglong), _vp]),
     "vcbct_projector_adjoint": (C.c_int, [_vp, _vp, _vp, _vp]),
+    "vcbct_projector_forward_state": (C.c_int, [_vp, _vp, _vp, _vp]),
+    "vcbct_projector_adjoint_state": (C.c_int, [_vp, _vp, _vp, _vp, _vp]),
     "vcbct_batch_create": (C.c_int, [C.POINTER(_vp)]),
     "vcbct_batch_add": (C.c_int, [_vp, _vp, _vp]),
     "vcbct_batch_forward": (C.c_int, [_vp, C.c_int, _vp]),

@@ -278,8 +278,36 @@ extern "C" int vcbct_projector_count_segments(vcbct_projector* p, unsigned long 
     return VCBCT_OK;
 }
 
+static int projector_adjoint(vcbct_projector* p, const float* d_L, const float* d_grad_out, float* d_grad,
+                             void* stream);
+
 extern "C" int vcbct_projector_adjoint(vcbct_projector* p, const float* d_grad_out, float* d_grad,
                                        void* stream)
+{
+    return projector_adjoint(p, nullptr, d_grad_out, d_grad, stream);
+}
+
+extern "C" int vcbct_projector_forward_state(vcbct_projector* p, float* d_out, float* d_L, void* stream)
+{
+    if (!p || !d_out || !d_L) return fail(VCBCT_ERR_ARG, "NULL argument");
+    ForwardArgs a;
+    int rc = make_fwd_args(p, a);
+    if (rc) return rc;
+    a.out = d_out;
+    a.L_out = d_L;
+    VCBCT_CUDA_TRY(launch_forward(a, (cudaStream_t)stream));
+    return VCBCT_OK;
+}
+
+extern "C" int vcbct_projector_adjoint_state(vcbct_projector* p, const float* d_L, const float* d_grad_out,
+                                             float* d_grad, void* stream)
+{
+    if (!d_L) return fail(VCBCT_ERR_ARG, "NULL argument");
+    return projector_adjoint(p, d_L, d_grad_out, d_grad, stream);
+}
+
+static int projector_adjoint(vcbct_projector* p, const float* d_L, const float* d_grad_out, float* d_grad,
+                             void* stream)
 {
     if (!p || !d_grad_out || !d_grad) return fail(VCBCT_ERR_ARG, "NULL argument");
     if (!p->have_f32) return fail(VCBCT_ERR_STATE, "the adjoint needs a float volume (load_volume_f32)");
@@ -295,6 +323,7 @@ extern "C" int vcbct_projector_adjoint(vcbct_projector* p, const float* d_grad_o
     a.spec = SpectrumDev{p->spec_mu.as<float4>(), p->spec_pdf.as<float>(), p->NE};
     a.vol_f32 = p->vol_f32.as<float4>();
     a.grad_out = d_grad_out;
+    a.L_in = d_L;
     a.grad_packed = p->grad_pk.as<float4>();
     a.err_flag = reinterpret_cast<int*>(p->counter.as<char>() + 8);
     a.cols_per_block = p->cols_per_block;

@@ -85,6 +85,8 @@ struct AdjointArgs {
     SpectrumDev spec;
     const float4* vol_f32;   // packed float volume
     const float* grad_out;   // [V][H][W] d loss / d intensity
+    const float* L_in;       // [V][H][W][nmat] path integrals of the forward, or
+                             // nullptr: recompute them (first march)
     float4* grad_packed;     // packed [..][8] float accumulator
     int* err_flag;
     int cols_per_block;

@@ -133,7 +133,7 @@ __device__ __forceinline__ void ray_setup(const ProjParams& P, const ViewGeom& v
     if (m < 2) return;
 
     // entry I = the hit nearer the source, exit F = the other
-    double I0, I1, I2, F0, F1, F2;
+    double I0, I1, I2, F0, F1;
     {
         const double e0 = dadd(dadd(dmul(dsub(hx0, S0), dsub(hx0, S0)), dmul(dsub(hy0, S1), dsub(hy0, S1))),
                                dmul(dsub(hz0, S2), dsub(hz0, S2)));
@@ -141,7 +141,7 @@ __device__ __forceinline__ void ray_setup(const ProjParams& P, const ViewGeom& v
                                dmul(dsub(hz1, S2), dsub(hz1, S2)));
         const bool f0 = e0 < e1;
         I0 = f0 ? hx0 : hx1; I1 = f0 ? hy0 : hy1; I2 = f0 ? hz0 : hz1;
-        F0 = f0 ? hx1 : hx0; F1 = f0 ? hy1 : hy0; F2 = f0 ? hz1 : hz0;
+        F0 = f0 ? hx1 : hx0; F1 = f0 ? hy1 : hy0;
     }
     // dominant axis, GPU twin rule (:198); _d / _o name the dominant and the
     // other in-plane axis
@@ -547,9 +547,36 @@ struct IvRec {
 
 constexpr int kIvPerWarp = 64;
 
+// The xy part of the ray plan: identical for the 32 rays of a warp (one
+// detector column), so it is kept once per warp in shared memory after the
+// interval buffer instead of in every lane's registers.  The interval
+// producer and the slow path read it from there.
+struct XyPlan {
+    double D0, O0, O1, invO1, tc0, tc1;
+    int pha, d;
+};
+constexpr int kIvSlots = kIvPerWarp + (int)((sizeof(XyPlan) + sizeof(IvRec) - 1) / sizeof(IvRec));
+
+__device__ __forceinline__ const XyPlan& publish_plan(const RayPlan& R, IvRec* wbuf)
+{
+    XyPlan* xp = reinterpret_cast<XyPlan*>(wbuf + kIvPerWarp);
+    if (threadIdx.x == 0 && R.active) {
+        xp->D0 = R.D0;
+        xp->O0 = R.O0;
+        xp->O1 = R.O1;
+        xp->invO1 = R.invO1;
+        xp->tc0 = R.tc0;
+        xp->tc1 = R.tc1;
+        xp->pha = R.pha;
+        xp->d = R.d;
+    }
+    __syncwarp();
+    return *xp;
+}
+
 // xy cell of the point at parameter t (FP64), as the reference's midpoint
 // rule: -1 when outside the cylindrical mask or the volume.
-__device__ __forceinline__ int xy_base_at(const ProjParams& P, const RayPlan& R, double t)
+__device__ __forceinline__ int xy_base_at(const ProjParams& P, const XyPlan& R, double t)
 {
     const int nxm = (int)(P.N * 0.5), nym = (int)(P.N * 0.5);
     const double Rv = P.N * 0.5;
@@ -562,7 +589,7 @@ __device__ __forceinline__ int xy_base_at(const ProjParams& P, const RayPlan& R,
     return (iy * P.N + ix) * P.Z;
 }
 
-__device__ __forceinline__ bool make_rec(const ProjParams& P, const RayPlan& R, double ta,
+__device__ __forceinline__ bool make_rec(const ProjParams& P, const XyPlan& R, double ta,
                                          double tb, IvRec& rec)
 {
     // keep every interval that meets the mask chord: a z split can move a
@@ -585,7 +612,7 @@ __device__ __forceinline__ bool make_rec(const ProjParams& P, const RayPlan& R, 
 }
 
 // Intervals of steps [k0, min(k0 + 31, Khi)] into buf; returns their number.
-__device__ __forceinline__ int produce_intervals(const ProjParams& P, const RayPlan& R, int k0,
+__device__ __forceinline__ int produce_intervals(const ProjParams& P, const XyPlan& R, int k0,
                                                  int Khi, IvRec* buf)
 {
     const int lane = threadIdx.x;
@@ -665,7 +692,8 @@ __device__ __forceinline__ void zstate_init(const ProjParams& P, const RayPlan& 
 // One interval, exact: split it at the z planes inside it (and apply the
 // midpoint rule across the z = 0 plane, which does not split).
 template <class Visit>
-__device__ __forceinline__ void consume_slow(const ProjParams& P, const RayPlan& R, const IvRec& rc,
+__device__ __forceinline__ void consume_slow(const ProjParams& P, const RayPlan& R, const XyPlan& xp,
+                                             const IvRec& rc,
                                              ZState& z, Visit& visit)
 {
     const int nzm = (int)(P.Z * 0.5);
@@ -695,7 +723,7 @@ __device__ __forceinline__ void consume_slow(const ProjParams& P, const RayPlan&
         }
         if (end > cur) {
             const bool whole = (cur == rc.ta) && (end == tb);
-            const int base = whole ? rc.base : xy_base_at(P, R, 0.5 * ((double)cur + (double)end));
+            const int base = whole ? rc.base : xy_base_at(P, xp, 0.5 * ((double)cur + (double)end));
             const int iz = trunc_index(nzm - 1 - cseg, P.Z);
             if (base >= 0 && iz >= 0) visit(base + iz, (end - cur) * R.Lt);
         }
@@ -710,11 +738,12 @@ __device__ __forceinline__ void consume_slow(const ProjParams& P, const RayPlan&
 }
 
 template <class Visit>
-__device__ __forceinline__ void consume_one(const ProjParams& P, const RayPlan& R, const IvRec& rc,
+__device__ __forceinline__ void consume_one(const ProjParams& P, const RayPlan& R, const XyPlan& xp,
+                                            const IvRec& rc,
                                             ZState& z, Visit& visit)
 {
     if (z.tz_next <= rc.tb || z.tz0 <= rc.tb) {
-        consume_slow(P, R, rc, z, visit);
+        consume_slow(P, R, xp, rc, z, visit);
     } else if (rc.base >= 0 && z.iz >= 0) {
         visit(rc.base + z.iz, (rc.tb - rc.ta) * R.Lt);
     }
@@ -728,7 +757,7 @@ __device__ __forceinline__ void consume_one(const ProjParams& P, const RayPlan& 
 // result, and crossings passed in intervals that were not produced -- goes
 // through consume_slow.  Both branches are taken warp-uniformly.
 template <class Visit, class Flush>
-__device__ __forceinline__ void march_intervals(const ProjParams& P, const RayPlan& R, bool act,
+__device__ __forceinline__ void march_intervals(const ProjParams& P, const RayPlan& R, const XyPlan& xp, bool act,
                                                 int Klo, int Khi, IvRec* buf, Visit& visit,
                                                 Flush flush)
 {
@@ -742,13 +771,13 @@ __device__ __forceinline__ void march_intervals(const ProjParams& P, const RayPl
     }
     const float Lt = R.Lt;
     for (int k0 = Klo; k0 <= Khi; k0 += 32) {
-        const int total = produce_intervals(P, R, k0, Khi, buf);
+        const int total = produce_intervals(P, xp, k0, Khi, buf);
         for (int i = 0; i < total; i++) {
             const IvRec rc = buf[i];
             const float lim = rc.exact ? rc.ta : rc.tb;
             const bool rare = (z.tz0 <= rc.tb) || (z.tz_next <= lim);
             if (__any_sync(0xffffffffu, rare)) {
-                consume_one(P, R, rc, z, visit);
+                consume_one(P, R, xp, rc, z, visit);
                 continue;
             }
             const bool ev = z.tz_next <= rc.tb;
@@ -844,7 +873,8 @@ __device__ __forceinline__ void ray_integrals(const ProjParams& P, const RayPlan
     }
     if (act && R.first_idx >= 0) acc(R.first_idx, R.first_len);
     auto fold = [&]() { acc.fold(); };
-    if (Klo <= Khi) march_intervals(P, R, act, Klo, Khi, wbuf, acc, fold);
+    const XyPlan& xp = publish_plan(R, wbuf);
+    if (Klo <= Khi) march_intervals(P, R, xp, act, Klo, Khi, wbuf, acc, fold);
     fold();
 }
 
@@ -861,7 +891,7 @@ __device__ __forceinline__ void forward_tile(const ForwardArgs& a, const float4*
     if (jj >= P.W) return;                           // whole warp exits together
     const int j = rowt * 32 + lane;                  // detector row
     const bool valid = j < P.H;
-    IvRec* wbuf = s_iv + threadIdx.y * kIvPerWarp;
+    IvRec* wbuf = s_iv + threadIdx.y * kIvSlots;
 
     const ViewGeom vg = a.views[v];
     RayPlan R;
@@ -908,9 +938,13 @@ __device__ __forceinline__ IvRec* iv_buffer(float4* smem, int NEmax)
 // the blocks resident at a time share one z band of the volume (L2 reuse
 // across views).
 // Register cap of the forward kernel: minimum resident 256-thread blocks per
-// SM (0 leaves the choice to the compiler).
+// SM (0 leaves the choice to the compiler).  The march is bound by the
+// latency of its L2 gathers, so occupancy pays more than registers: 5 blocks
+// (48 registers, 40 warps per SM) measured 26 % faster on B200 than the
+// compiler's own choice (80 registers, 24 warps), although the rarely taken
+// paths then spill.
 #ifndef VCBCT_FWD_MIN_BLOCKS
-#define VCBCT_FWD_MIN_BLOCKS 0
+#define VCBCT_FWD_MIN_BLOCKS 5
 #endif
 #if VCBCT_FWD_MIN_BLOCKS > 0
 #define VCBCT_FWD_BOUNDS __launch_bounds__(256, VCBCT_FWD_MIN_BLOCKS)
@@ -981,8 +1015,13 @@ __global__ void __launch_bounds__(256) batch_forward_kernel(const BatchItem* __r
     }
 }
 
+// Register cap of the adjoint (minimum resident 256-thread blocks per SM):
+// 4 (64 registers) measured fastest on B200 among 2 to 5.
+#ifndef VCBCT_ADJ_MIN_BLOCKS
+#define VCBCT_ADJ_MIN_BLOCKS 4
+#endif
 template <int M>
-__global__ void __launch_bounds__(256, 2) adjoint_kernel(AdjointArgs a)
+__global__ void __launch_bounds__(256, VCBCT_ADJ_MIN_BLOCKS) adjoint_kernel(AdjointArgs a)
 {
     extern __shared__ float4 smem[];
     float4* s_mu = smem;
@@ -998,7 +1037,7 @@ __global__ void __launch_bounds__(256, 2) adjoint_kernel(AdjointArgs a)
     const int v = blockIdx.y;
     const int j = blockIdx.z * 32 + lane;
     const bool valid = j < P.H;
-    IvRec* wbuf = s_iv + threadIdx.y * kIvPerWarp;
+    IvRec* wbuf = s_iv + threadIdx.y * kIvSlots;
     const ViewGeom vg = a.views[v];
     RayPlan R;
     ray_setup(P, vg, j, jj, R);
@@ -1010,9 +1049,19 @@ __global__ void __launch_bounds__(256, 2) adjoint_kernel(AdjointArgs a)
     warp_range(R, act, Klo, Khi);
     if (!__any_sync(0xffffffffu, act && R.active)) return;
 
-    // pass 1: recompute the per-element path integrals of this ray
+    // pass 1: the per-element path integrals of this ray, recomputed by a
+    // first march or read from the forward projection that made them
     AccumF32<M> acc(a.vol_f32);
-    ray_integrals<AccumF32<M>, M>(P, R, act, Klo, Khi, wbuf, acc);
+    if (a.L_in) {
+        if (act) {
+            const float* Lr = a.L_in + (((size_t)v * P.H + (P.H - 1 - j)) * P.W + jj) * P.nmat;
+#pragma unroll
+            for (int i = 0; i < M; i++)
+                if (i < P.nmat) acc.L[i] = Lr[i];
+        }
+    } else {
+        ray_integrals<AccumF32<M>, M>(P, R, act, Klo, Khi, wbuf, acc);
+    }
 
     // d I / d L_k = -leng * sum_E pdf_E mu'_k(E) exp(-sum_k mu'_k(E) L_k)
     float g[8] = {0, 0, 0, 0, 0, 0, 0, 0};
@@ -1049,7 +1098,8 @@ __global__ void __launch_bounds__(256, 2) adjoint_kernel(AdjointArgs a)
         return;
     }
     if (act && R.first_idx >= 0) sc(R.first_idx, R.first_len);
-    if (Klo <= Khi) march_intervals(P, R, act, Klo, Khi, wbuf, sc, []() {});
+    const XyPlan& xp = publish_plan(R, wbuf);
+    if (Klo <= Khi) march_intervals(P, R, xp, act, Klo, Khi, wbuf, sc, []() {});
 }
 
 // ------------------------------------------------------- layout kernels --
@@ -1165,7 +1215,7 @@ static cudaError_t launch_fwd_t(const ForwardArgs& a, cudaStream_t st)
     dim3 block(32, cpb);
     dim3 grid((a.p.W + cpb - 1) / cpb, a.p.V, (a.p.H + 31) / 32);
     size_t shm = ((size_t)2 * a.spec.NE + (a.spec.NE + 3) / 4) * sizeof(float4) +
-                 (size_t)cpb * kIvPerWarp * sizeof(IvRec);
+                 (size_t)cpb * kIvSlots * sizeof(IvRec);
     auto k = forward_kernel<M, F32VOL, COUNT>;
     if (shm > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
@@ -1181,7 +1231,7 @@ cudaError_t launch_batch_forward(const BatchItem* d_items, int nitems, long long
 {
     dim3 block(32, cols_per_block);
     size_t shm = ((size_t)2 * NEmax + (NEmax + 3) / 4) * sizeof(float4) +
-                 (size_t)cols_per_block * kIvPerWarp * sizeof(IvRec);
+                 (size_t)cols_per_block * kIvSlots * sizeof(IvRec);
     // (the shared-memory attribute is set by batch_blocks_per_sm, before any
     // stream capture)
     cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st);
@@ -1194,7 +1244,7 @@ cudaError_t launch_batch_forward(const BatchItem* d_items, int nitems, long long
 int batch_blocks_per_sm(int nmat_max, int cols_per_block, int NEmax)
 {
     size_t shm = ((size_t)2 * NEmax + (NEmax + 3) / 4) * sizeof(float4) +
-                 (size_t)cols_per_block * kIvPerWarp * sizeof(IvRec);
+                 (size_t)cols_per_block * kIvSlots * sizeof(IvRec);
     int n = 0;
     auto k = (nmat_max <= 6) ? batch_forward_kernel<6> : batch_forward_kernel<8>;
     if (shm > 48 * 1024 && cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm) != cudaSuccess)
@@ -1222,7 +1272,7 @@ static cudaError_t launch_adj_t(const AdjointArgs& a, cudaStream_t st)
     dim3 block(32, cpb);
     dim3 grid((a.p.W + cpb - 1) / cpb, a.p.V, (a.p.H + 31) / 32);
     size_t shm = ((size_t)2 * a.spec.NE + (a.spec.NE + 3) / 4) * sizeof(float4) +
-                 (size_t)cpb * kIvPerWarp * sizeof(IvRec);
+                 (size_t)cpb * kIvSlots * sizeof(IvRec);
     auto k = adjoint_kernel<M>;
     if (shm > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);

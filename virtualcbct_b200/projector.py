@@ -152,6 +152,32 @@ class Projector:
                                                  C.byref(c)))
         return c.value
 
+    def forward_state(self, out=None, L=None, stream=None):
+        """Device projection [V][H][W] and per-ray path integrals
+        L [V][H][W][nmat] in one launch (for adjoint_state)."""
+        import torch
+        g = self.geom
+        if out is None:
+            out = torch.empty((g.V, g.H, g.W), dtype=torch.float32, device="cuda")
+        if L is None:
+            L = torch.empty((g.V, g.H, g.W, g.nmat), dtype=torch.float32, device="cuda")
+        N.check(N.lib().vcbct_projector_forward_state(self._h, C.c_void_p(out.data_ptr()),
+                                                      C.c_void_p(L.data_ptr()), _stream_ptr(stream)))
+        return out, L
+
+    def adjoint_state(self, L, grad_out, grad=None, stream=None):
+        """adjoint() with the path integrals L of forward_state instead of a
+        recomputing march."""
+        import torch
+        g = self.geom
+        if grad is None:
+            grad = torch.zeros((g.Z, g.nmat, g.N, g.N), dtype=torch.float32, device="cuda")
+        go = grad_out.contiguous()
+        N.check(N.lib().vcbct_projector_adjoint_state(self._h, C.c_void_p(L.data_ptr()),
+                                                      C.c_void_p(go.data_ptr()),
+                                                      C.c_void_p(grad.data_ptr()), _stream_ptr(stream)))
+        return grad
+
     def adjoint(self, grad_out, grad=None, stream=None):
         """Accumulate d loss / d volume (float [Z][nmat][N][N], device) for a
         device d loss / d projection ``grad_out`` [V][H][W]."""
