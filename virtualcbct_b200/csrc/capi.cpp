@@ -314,7 +314,7 @@ static int projector_adjoint(vcbct_projector* p, const float* d_L, const float* 
     if (p->NE <= 0) return fail(VCBCT_ERR_STATE, "no spectrum set");
     cudaStream_t st = (cudaStream_t)stream;
     const auto& g = p->g;
-    const size_t pk = packed_f32_bytes(g.recon_size, g.recon_slices);
+    const size_t pk = (size_t)g.num_material * g.recon_size * g.recon_size * g.recon_slices * sizeof(float);
     VCBCT_CUDA_TRY(p->grad_pk.ensure(pk));
     VCBCT_CUDA_TRY(cudaMemsetAsync(p->grad_pk.p, 0, pk, st));
     AdjointArgs a{};
@@ -324,11 +324,11 @@ static int projector_adjoint(vcbct_projector* p, const float* d_L, const float* 
     a.vol_f32 = p->vol_f32.as<float4>();
     a.grad_out = d_grad_out;
     a.L_in = d_L;
-    a.grad_packed = p->grad_pk.as<float4>();
+    a.grad_planes = p->grad_pk.as<float>();
     a.err_flag = reinterpret_cast<int*>(p->counter.as<char>() + 8);
     a.cols_per_block = p->cols_per_block;
     VCBCT_CUDA_TRY(launch_adjoint(a, st));
-    VCBCT_CUDA_TRY(launch_unpack_grad(p->grad_pk.as<float4>(), g.recon_size, g.recon_slices, g.num_material, d_grad, st));
+    VCBCT_CUDA_TRY(launch_unpack_grad(p->grad_pk.as<float>(), g.recon_size, g.recon_slices, g.num_material, d_grad, st));
     return VCBCT_OK;
 }
 

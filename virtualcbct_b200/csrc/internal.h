@@ -43,8 +43,7 @@ cudaError_t launch_pack_u16(const uint16_t* src, int N, int Z, int nmat, uint4* 
                             cudaStream_t st);
 cudaError_t launch_pack_f32(const float* src, int N, int Z, int nmat, float4* dst,
                             cudaStream_t st);
-cudaError_t launch_unpack_grad(const float4* packed, int N, int Z, int nmat, float* dst,
-                               cudaStream_t st);
+cudaError_t launch_unpack_grad(const float* planes, int N, int Z, int nmat, float* dst, cudaStream_t st);
 
 // Spectral table: per bin 8 floats mu_k(E)/xfactor (zero padded) + pdf.
 struct SpectrumDev {
@@ -87,7 +86,7 @@ struct AdjointArgs {
     const float* grad_out;   // [V][H][W] d loss / d intensity
     const float* L_in;       // [V][H][W][nmat] path integrals of the forward, or
                              // nullptr: recompute them (first march)
-    float4* grad_packed;     // packed [..][8] float accumulator
+    float* grad_planes;      // [nmat][N*N*Z] float accumulator, z fastest
     int* err_flag;
     int cols_per_block;
 };

@@ -479,6 +479,11 @@ struct AccumU16 : PairSums<M> {
     const uint4* __restrict__ vol;
     unsigned nseg;
     __device__ __forceinline__ AccumU16(const uint4* v) : vol(v), nseg(0u) { this->clear(); }
+    // called by all 32 lanes together; p: this lane has a segment
+    __device__ __forceinline__ void lanes(bool p, int idx, float len)
+    {
+        if (p) (*this)(idx, len);
+    }
     __device__ __forceinline__ void operator()(int idx, float len)
     {
         const uint4 v = __ldg(vol + idx);
@@ -496,6 +501,10 @@ struct AccumF32 : PairSums<M> {
     const float4* __restrict__ vol;
     unsigned nseg;
     __device__ __forceinline__ AccumF32(const float4* v) : vol(v), nseg(0u) { this->clear(); }
+    __device__ __forceinline__ void lanes(bool p, int idx, float len)
+    {
+        if (p) (*this)(idx, len);
+    }
     __device__ __forceinline__ void operator()(int idx, float len)
     {
         const ulonglong2* p = reinterpret_cast<const ulonglong2*>(vol + 2 * (size_t)idx);
@@ -512,19 +521,27 @@ struct AccumF32 : PairSums<M> {
 // Scatter of one segment's gradient into the packed float records: one
 // 16-byte vector reduction for elements 0-3 and one 8-byte (M = 6) or
 // 16-byte (M = 8) reduction for the rest.
+// Scatter of one segment's gradient into element planes: plane k holds
+// element k of every voxel at the packed record index (y*N + x)*Z + z, so
+// the 32 lanes of a warp -- adjacent detector rows, adjacent z cells of one
+// xy cell -- reduce into a few consecutive sectors of each plane (one
+// reduction per element and lane; the L2 applies them per sector).
 template <int M>
 struct Scatter {
-    float4* __restrict__ grad;
-    int N, Z;
+    float* __restrict__ grad;   // [nmat][N*N*Z]
+    size_t plane;               // N*N*Z
+    int nmat;
     float g[8];
     __device__ __forceinline__ void operator()(int idx, float len)
     {
-        float4* p = grad + 2 * (size_t)idx;
-        atomicAdd(p, make_float4(g[0] * len, g[1] * len, g[2] * len, g[3] * len));
-        if (M > 6)
-            atomicAdd(p + 1, make_float4(g[4] * len, g[5] * len, g[6] * len, g[7] * len));
-        else
-            atomicAdd(reinterpret_cast<float2*>(p + 1), make_float2(g[4] * len, g[5] * len));
+        float* p = grad + idx;
+#pragma unroll
+        for (int k = 0; k < M; k++)
+            if (k < nmat) atomicAdd(p + k * plane, g[k] * len);
+    }
+    __device__ __forceinline__ void lanes(bool p, int idx, float len)
+    {
+        if (p) (*this)(idx, len);
     }
 };
 
@@ -782,7 +799,7 @@ __device__ __forceinline__ void march_intervals(const ProjParams& P, const RayPl
             }
             const bool ev = z.tz_next <= rc.tb;
             const float tz = ev ? z.tz_next : rc.tb;
-            if (rc.base >= 0 && z.iz >= 0) visit(rc.base + z.iz, (tz - rc.ta) * Lt);
+            visit.lanes(rc.base >= 0 && z.iz >= 0, rc.base + z.iz, (tz - rc.ta) * Lt);
             if (__any_sync(0xffffffffu, ev)) {
                 if (ev) {
                     z.cz = (z.dirz > 0) ? z.mz : z.mz - 1;
@@ -790,8 +807,8 @@ __device__ __forceinline__ void march_intervals(const ProjParams& P, const RayPl
                     z.mz += z.dirz;
                     if (z.mz == 0) z.mz += z.dirz;
                     z.tz_next = zcross(R, z.mz);
-                    if (rc.base >= 0 && z.iz >= 0 && rc.tb > tz) visit(rc.base + z.iz, (rc.tb - tz) * Lt);
                 }
+                visit.lanes(ev && rc.base >= 0 && z.iz >= 0 && rc.tb > tz, rc.base + z.iz, (rc.tb - tz) * Lt);
             }
         }
         __syncwarp();
@@ -1032,10 +1049,10 @@ __global__ void __launch_bounds__(256, VCBCT_ADJ_MIN_BLOCKS) adjoint_kernel(Adjo
 
     const ProjParams& P = a.p;
     const int lane = threadIdx.x;
-    const int jj = blockIdx.x * blockDim.y + threadIdx.y;
+    const int colb = blockIdx.x, v = blockIdx.y, rowt = blockIdx.z;
+    const int jj = colb * blockDim.y + threadIdx.y;
     if (jj >= P.W) return;
-    const int v = blockIdx.y;
-    const int j = blockIdx.z * 32 + lane;
+    const int j = rowt * 32 + lane;
     const bool valid = j < P.H;
     IvRec* wbuf = s_iv + threadIdx.y * kIvSlots;
     const ViewGeom vg = a.views[v];
@@ -1084,7 +1101,7 @@ __global__ void __launch_bounds__(256, VCBCT_ADJ_MIN_BLOCKS) adjoint_kernel(Adjo
         g[6] = fmaf(w, m1.z, g[6]); g[7] = fmaf(w, m1.w, g[7]);
     }
     const float scale = -R.leng * r;
-    Scatter<M> sc{a.grad_packed, P.N, P.Z, {}};
+    Scatter<M> sc{a.grad_planes, (size_t)P.N * P.N * P.Z, P.nmat, {}};
 #pragma unroll
     for (int i = 0; i < 8; i++) sc.g[i] = g[i] * scale;
     // pass 2: scatter along the same segments
@@ -1159,29 +1176,27 @@ __global__ void pack_f32_kernel(const float* __restrict__ src, int N, int Z, int
 }
 
 // packed float records -> [Z][nmat][N][N], accumulated (+=).
-__global__ void unpack_grad_kernel(const float4* __restrict__ src, int N, int Z, int nmat,
+// element planes [nmat][(y*N + x)*Z + z] -> [Z][nmat][N][N], accumulated (+=).
+// grid (ceil(N/32), N, ceil(Z/32) * nmat), block (32, 8): a 32 x 32 (x, z)
+// tile of one plane through shared memory.
+__global__ void unpack_grad_kernel(const float* __restrict__ src, int N, int Z, int nmat,
                                    float* __restrict__ dst)
 {
-    __shared__ float tile[32][8][33];
-    const int x0 = blockIdx.x * 32, y = blockIdx.y, z0 = blockIdx.z * 32;
+    __shared__ float tile[32][33];
+    const int zt = (Z + 31) / 32;
+    const int m = blockIdx.z / zt;
+    const int x0 = blockIdx.x * 32, y = blockIdx.y, z0 = (blockIdx.z % zt) * 32;
     const size_t NN = (size_t)N * N;
+    const float* plane = src + (size_t)m * NN * Z;
     for (int xx = threadIdx.y; xx < 32; xx += 8) {
         const int x = x0 + xx, z = z0 + threadIdx.x;
-        float4 a = make_float4(0, 0, 0, 0), b = a;
-        if (x < N && z < Z) {
-            const float4* p = src + 2 * (((size_t)y * N + x) * Z + z);
-            a = p[0];
-            b = p[1];
-        }
-        const int zz = threadIdx.x;
-        tile[zz][0][xx] = a.x; tile[zz][1][xx] = a.y; tile[zz][2][xx] = a.z; tile[zz][3][xx] = a.w;
-        tile[zz][4][xx] = b.x; tile[zz][5][xx] = b.y; tile[zz][6][xx] = b.z; tile[zz][7][xx] = b.w;
+        tile[threadIdx.x][xx] = (x < N && z < Z) ? plane[((size_t)y * N + x) * Z + z] : 0.0f;
     }
     __syncthreads();
     for (int zz = threadIdx.y; zz < 32; zz += 8) {
         const int z = z0 + zz, x = x0 + threadIdx.x;
         if (z >= Z || x >= N) continue;
-        for (int m = 0; m < nmat; m++) dst[((size_t)z * nmat + m) * NN + (size_t)y * N + x] += tile[zz][m][threadIdx.x];
+        dst[((size_t)z * nmat + m) * NN + (size_t)y * N + x] += tile[zz][threadIdx.x];
     }
 }
 
@@ -1201,10 +1216,10 @@ cudaError_t launch_pack_f32(const float* src, int N, int Z, int nmat, float4* ds
     return cudaGetLastError();
 }
 
-cudaError_t launch_unpack_grad(const float4* packed, int N, int Z, int nmat, float* dst, cudaStream_t st)
+cudaError_t launch_unpack_grad(const float* planes, int N, int Z, int nmat, float* dst, cudaStream_t st)
 {
-    dim3 grid((N + 31) / 32, N, (Z + 31) / 32), block(32, 8);
-    unpack_grad_kernel<<<grid, block, 0, st>>>(packed, N, Z, nmat, dst);
+    dim3 grid((N + 31) / 32, N, ((Z + 31) / 32) * nmat), block(32, 8);
+    unpack_grad_kernel<<<grid, block, 0, st>>>(planes, N, Z, nmat, dst);
     return cudaGetLastError();
 }
 
@@ -1270,6 +1285,8 @@ static cudaError_t launch_adj_t(const AdjointArgs& a, cudaStream_t st)
 {
     const int cpb = a.cols_per_block;
     dim3 block(32, cpb);
+    // the forward's block order; (columns, row bands, views) and (views,
+    // columns, row bands) measured within 3 % on B200
     dim3 grid((a.p.W + cpb - 1) / cpb, a.p.V, (a.p.H + 31) / 32);
     size_t shm = ((size_t)2 * a.spec.NE + (a.spec.NE + 3) / 4) * sizeof(float4) +
                  (size_t)cpb * kIvSlots * sizeof(IvRec);

@@ -16,6 +16,7 @@ seconds:
   filter_direct  FDK ramp filter, direct FP32 kernel, same projections
   backproject    FDK backprojection of 360 filtered 400x400 views to 270x270x200
   adjoint_c4     MBFPA adjoint, six float volumes 256x256x64, 90 views, 200x200
+  adjoint_state_c4  the same with the forward's path integrals kept
   batch_small    four uneven ellipsoid phantoms (256x256, Z 32-96, V 45-180)
                  in one persistent launch
 """
@@ -96,6 +97,16 @@ def run(case: str, repeats: int = 2) -> str:
         out = torch.zeros_like(vol)
         for _ in range(repeats):
             p.adjoint(go, out)
+    elif case == "adjoint_state_c4":
+        g = ProjGeometry(N=256, Z=64, s=0.1, step=0.2, W=200, H=200, V=90)
+        p = _projector(g, phantoms.view_angles(90), spectrum="spectrum_kramers100_91.csv")
+        vol = phantoms.ellipsoid_phantom_torch(g.N, g.Z, g.s, g.step, seed=21, as_float=True)
+        p.load_volume_f32(vol)
+        _, L = p.forward_state()
+        go = torch.ones((g.V, g.H, g.W), dtype=torch.float32, device="cuda")
+        out = torch.zeros_like(vol)
+        for _ in range(repeats):
+            p.adjoint_state(L, go, out)
     elif case == "batch_small":
         rng = np.random.default_rng(7)
         b = Batch()
