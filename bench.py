@@ -287,6 +287,54 @@ def batched_section(stream, args):
             "batched_over_plain_speedup": plain / bat, "batched_gseg_s": nseg / (bat * 1e-3) / 1e9}
 
 
+def batched_small_section(stream):
+    """Many small phantoms (64 of 128x128xZ, Z 16-64, V 18-90, 64x64
+    detector): the regime where one launch per phantom leaves the GPU idle
+    between launches.  Plain = one projector launch per phantom issued from
+    the host; batched = the autotuned batch replayed from its CUDA graph, and
+    the persistent single-launch strategy forced."""
+    import torch
+    from virtualcbct_b200 import Batch, Projector, ProjGeometry, attenuation_table, phantoms, trig_tables
+    rng = np.random.default_rng(77)
+    mu, pdf = attenuation_table(os.path.join(DATA, "spectrum_kramers100_90.csv"), MINIDB, 6)
+    projs, outs = [], []
+    for i in range(64):
+        Z = int(rng.integers(16, 65))
+        V = int(rng.integers(18, 91))
+        g = ProjGeometry(N=128, Z=Z, s=0.25, step=0.5, W=64, H=64, V=V)
+        ang = np.deg2rad(phantoms.view_angles(V))
+        tabs = trig_tables(g.W, g.H, ang, np.zeros(V), np.zeros(V), g.pdet, g.dpn)
+        p = Projector(g, *tabs)
+        p.set_spectrum(mu, pdf, 1000.0)
+        p.load_volume(phantoms.ellipsoid_phantom_torch(g.N, Z, g.s, g.step, seed=500 + i))
+        projs.append(p)
+    nseg = sum(p.count_segments() for p in projs)
+    b_auto, b_pers = Batch(), Batch()
+    for p in projs:
+        outs.append(b_auto.add(p))
+        b_pers.add(p)
+    b_pers.configure(False, 4)
+    tuned = b_auto.autotune()
+
+    def t(f, reps=5):
+        f()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            f()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    plain = t(lambda: [p.forward(o) for p, o in zip(projs, outs)])
+    auto = t(lambda: b_auto.forward(use_graph=True))
+    pers = t(lambda: b_pers.forward(use_graph=True))
+    return {"workload": "64 ellipsoid phantoms 128x128xZ (Z 16-64), V 18-90, 64x64", "segments": nseg,
+            "autotuned": tuned, "plain_ms": plain, "batched_graph_ms": auto, "persistent_graph_ms": pers,
+            "batched_over_plain_speedup": plain / auto, "persistent_over_plain_speedup": plain / pers}
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import virtualcbct_b200 as vc
@@ -404,6 +452,7 @@ def run_ours(args, rank, world, local_rank):
     if not args.no_extras:
         extra["decomposition"] = decomposition_section(stream)
         extra["batched"] = batched_section(stream, args)
+        extra["batched_small"] = batched_small_section(stream)
 
     # measured gather rooflines: the projector's and the backprojector's
     # access patterns replayed without arithmetic on this device
