@@ -43,10 +43,11 @@ MINIDB = os.path.join(DATA, "xraydb_mini")
 
 METRIC = "MBFPA ray-voxel Gseg/s & FDK GUPS; batched vs plain; grad-step/fwd ratio @stated err"
 
-# DRAM traffic of one forward launch of this workload, from
-# profiles/mbfpa_forward_c2.md (ncu dram__bytes_read.sum + dram__bytes_write.sum,
-# scaled from the captured case as documented there).  None until captured.
-FORWARD_DRAM_BYTES = None
+# DRAM traffic of one forward launch of this workload: ncu
+# dram__bytes_read.sum + dram__bytes_write.sum of the first launch of
+# `python -m virtualcbct_b200.profile_cases forward_c2 1` (a one-pass capture
+# of the full-size launch): 3.25 GB read + 1.70 GB written.
+FORWARD_DRAM_BYTES = 4.95e9
 
 
 def workload():
