@@ -3,6 +3,7 @@
 // preparation.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -66,6 +67,10 @@ using namespace vcbct;
 
 // ===================================================================== MBFPA
 
+// Host-bound projections are computed in this many view chunks, each
+// downloaded while the next is computed.
+constexpr int kForwardChunks = 8;
+
 struct vcbct_projector {
     vcbct_proj_geometry g;
     ProjParams pp;
@@ -80,6 +85,10 @@ struct vcbct_projector {
     int NE = 0;
     int have_u16 = 0, have_f32 = 0;
     int cols_per_block = 4;
+    // download of host-bound projections, overlapped with the later views
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t chunk_done[kForwardChunks] = {};
+    cudaEvent_t copies_done = nullptr;
 };
 
 extern "C" const char* vcbct_last_error(void) { return g_last_error.c_str(); }
@@ -147,6 +156,10 @@ extern "C" int vcbct_projector_destroy(vcbct_projector* p)
     p->spec_pdf.release();
     p->grad_pk.release();
     p->counter.release();
+    if (p->copy_stream) cudaStreamDestroy(p->copy_stream);
+    for (cudaEvent_t e : p->chunk_done)
+        if (e) cudaEventDestroy(e);
+    if (p->copies_done) cudaEventDestroy(p->copies_done);
     delete p;
     return VCBCT_OK;
 }
@@ -235,19 +248,40 @@ extern "C" int vcbct_projector_forward(vcbct_projector* p, float* out, int out_o
     int rc = make_fwd_args(p, a);
     if (rc) return rc;
     const size_t nout = (size_t)p->g.n_views * p->g.proj_height * p->g.proj_width;
-    float* dout = out;
-    if (!out_on_device) {
-        // the staging buffer may hold the host volume of load_volume: use a
-        // region after it
-        VCBCT_CUDA_TRY(p->grad_pk.ensure(nout * sizeof(float)));
-        dout = p->grad_pk.as<float>();
+    if (out_on_device) {
+        a.out = out;
+        VCBCT_CUDA_TRY(launch_forward(a, st));
+        return VCBCT_OK;
     }
-    a.out = dout;
-    VCBCT_CUDA_TRY(launch_forward(a, st));
-    if (!out_on_device) {
-        VCBCT_CUDA_TRY(cudaMemcpyAsync(out, dout, nout * sizeof(float), cudaMemcpyDeviceToHost, st));
-        VCBCT_CUDA_TRY(cudaStreamSynchronize(st));
+    // Host output: project in view chunks on `st` and download each chunk on
+    // a second stream while the next one is projected.
+    VCBCT_CUDA_TRY(p->grad_pk.ensure(nout * sizeof(float)));
+    float* dout = p->grad_pk.as<float>();
+    if (!p->copy_stream) {
+        VCBCT_CUDA_TRY(cudaStreamCreateWithFlags(&p->copy_stream, cudaStreamNonBlocking));
+        for (cudaEvent_t& e : p->chunk_done) VCBCT_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        VCBCT_CUDA_TRY(cudaEventCreateWithFlags(&p->copies_done, cudaEventDisableTiming));
     }
+    const int V = p->g.n_views;
+    const size_t per_view = (size_t)p->g.proj_height * p->g.proj_width;
+    const int nch = std::min(kForwardChunks, V);
+    const ViewGeom* views = a.views;
+    for (int c = 0; c < nch; c++) {
+        const int v0 = (int)((long long)V * c / nch), v1 = (int)((long long)V * (c + 1) / nch);
+        ForwardArgs ac = a;
+        ac.views = views + v0;
+        ac.p.V = v1 - v0;
+        ac.out = dout + (size_t)v0 * per_view;
+        VCBCT_CUDA_TRY(launch_forward(ac, st));
+        VCBCT_CUDA_TRY(cudaEventRecord(p->chunk_done[c], st));
+        VCBCT_CUDA_TRY(cudaStreamWaitEvent(p->copy_stream, p->chunk_done[c], 0));
+        VCBCT_CUDA_TRY(cudaMemcpyAsync(out + (size_t)v0 * per_view, dout + (size_t)v0 * per_view,
+                                       (size_t)(v1 - v0) * per_view * sizeof(float), cudaMemcpyDeviceToHost,
+                                       p->copy_stream));
+    }
+    VCBCT_CUDA_TRY(cudaEventRecord(p->copies_done, p->copy_stream));
+    VCBCT_CUDA_TRY(cudaStreamWaitEvent(st, p->copies_done, 0));
+    VCBCT_CUDA_TRY(cudaStreamSynchronize(st));
     return VCBCT_OK;
 }
 
