@@ -267,23 +267,32 @@ __device__ __forceinline__ void split3(float x, __nv_bfloat16& a, __nv_bfloat16&
 }
 
 // A planes [3][M][Kp]: split of g = -logf(p) (times the redundancy weight).
+// grid (M, ceil(Kp / 512)), block 128: one detector row per block, four
+// consecutive columns per thread, written as 8-byte groups (Kp is a multiple
+// of 64, so every group is aligned).
 __global__ void split_a_kernel(const float* __restrict__ proj, const float* __restrict__ wts, int M, int H, int W,
                                int Kp, __nv_bfloat16* __restrict__ planes)
 {
-    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= (size_t)M * Kp) return;
-    const int r = (int)(i / Kp), k = (int)(i % Kp);
-    float g = 0.0f;
-    if (k < W) {
-        g = -logf(__ldg(proj + (size_t)r * W + k));
-        if (wts) g *= __ldg(wts + (size_t)(r / H) * W + k);
+    const int r = blockIdx.x;
+    const int k0 = 4 * (blockIdx.y * blockDim.x + threadIdx.x);
+    if (k0 >= Kp) return;
+    const float* pr = proj + (size_t)r * W;
+    const float* wr = wts ? wts + (size_t)(r / H) * W : nullptr;
+    __align__(8) __nv_bfloat16 a[4], b[4], c[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        const int k = k0 + q;
+        float g = 0.0f;
+        if (k < W) {
+            g = -logf(__ldg(pr + k));
+            if (wr) g *= __ldg(wr + k);
+        }
+        split3(g, a[q], b[q], c[q]);
     }
-    __nv_bfloat16 a, b, c;
-    split3(g, a, b, c);
-    const size_t plane = (size_t)M * Kp;
-    planes[i] = a;
-    planes[plane + i] = b;
-    planes[2 * plane + i] = c;
+    const size_t plane = (size_t)M * Kp, o = (size_t)r * Kp + k0;
+    *reinterpret_cast<uint2*>(planes + o) = *reinterpret_cast<const uint2*>(a);
+    *reinterpret_cast<uint2*>(planes + plane + o) = *reinterpret_cast<const uint2*>(b);
+    *reinterpret_cast<uint2*>(planes + 2 * plane + o) = *reinterpret_cast<const uint2*>(c);
 }
 
 // B planes [3][Np][Kp]: B[m][k] = hT[k][m] (ramp kernel + diagonal coefficient).
@@ -372,8 +381,8 @@ cudaError_t launch_ramp_gemm_bf16x3(const float* proj, float* out, const float* 
     cudaError_t e = cudaMemsetAsync(err, 0, sizeof(int), st);
     if (e != cudaSuccess) return e;
     {
-        const size_t n = (size_t)L.M * L.Kp;
-        split_a_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(proj, wts, L.M, H, W, L.Kp, ap);
+        split_a_kernel<<<dim3((unsigned)L.M, (unsigned)((L.Kp + 511) / 512)), 128, 0, st>>>(proj, wts, L.M, H, W,
+                                                                                         L.Kp, ap);
         const size_t nb = (size_t)L.Np * L.Kp;
         split_b_kernel<<<(unsigned)((nb + 255) / 256), 256, 0, st>>>(hT, W, L.Np, L.Kp, bp);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
