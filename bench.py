@@ -288,6 +288,45 @@ def batched_section(stream, args):
             "batched_over_plain_speedup": plain / bat, "batched_gseg_s": nseg / (bat * 1e-3) / 1e9}
 
 
+def iterative_section(stream):
+    """The projector program's iterative-reconstruction helpers at the
+    512x512x100 / 36-view size: sensitivity backprojection of uint16
+    projections (lengthproj) and the MLEM/TV update (IR_ImageCBCT)."""
+    import torch
+    from virtualcbct_b200 import Projector, ProjGeometry, phantoms, trig_tables
+    from virtualcbct_b200.iterative import ir_update
+    g = ProjGeometry(N=512, Z=100, s=0.05, step=0.2, W=400, H=400, V=36)
+    ang = np.deg2rad(phantoms.view_angles(g.V))
+    p = Projector(g, *trig_tables(g.W, g.H, ang, np.zeros(g.V), np.zeros(g.V), g.pdet, g.dpn))
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(3)
+    proj = torch.randint(20000, 65000, (g.V, g.H, g.W), generator=gen, device="cuda", dtype=torch.int32)
+    proj = proj.to(torch.int16)  # uint16 bits
+    npf = torch.empty((g.Z, g.N, g.N), dtype=torch.float32, device="cuda")
+    before = torch.randint(0, 3000, (g.Z, g.N, g.N), generator=gen, device="cuda", dtype=torch.int32).to(torch.int16)
+    npf_re = npf.clone()
+    out = torch.empty_like(npf)
+
+    def t(f, reps=3):
+        f()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            f()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    lp = t(lambda: p.lengthproj(proj, npf=npf))
+    npf_re.copy_(npf)
+    ir = t(lambda: ir_update(before, npf, npf_re, g.s, 0.5, 0.002, out=out), reps=10)
+    nvox = g.N * g.N * g.Z
+    return {"workload": "512x512x100, 36 views of 400x400 uint16",
+            "lengthproj_ms": lp, "lengthproj_gvox_views_s": nvox * g.V / (lp * 1e-3) / 1e9,
+            "ir_update_ms": ir, "ir_update_gvox_s": nvox / (ir * 1e-3) / 1e9}
+
+
 def batched_small_section(stream):
     """Many small phantoms (64 of 128x128xZ, Z 16-64, V 18-90, 64x64
     detector): the regime where one launch per phantom leaves the GPU idle
@@ -454,6 +493,7 @@ def run_ours(args, rank, world, local_rank):
         extra["decomposition"] = decomposition_section(stream)
         extra["batched"] = batched_section(stream, args)
         extra["batched_small"] = batched_small_section(stream)
+        extra["iterative"] = iterative_section(stream)
 
     # measured gather rooflines: the projector's and the backprojector's
     # access patterns replayed without arithmetic on this device

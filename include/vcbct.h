@@ -182,6 +182,41 @@ void reprojectionOnGPU(int ite, int reconSize, int reconSlices, unsigned short* 
                        double x_reg, double y_reg, double z_reg, float* Attenuation,
                        float* pdf_pe, int num_material, int NE, char* outputname);
 
+/* Iterative-reconstruction helpers of the projector program.
+ *
+ * Sensitivity backprojection (replaces lengthproj, lengthproj.h:1-9 /
+ * lengthproj.cpp:10-131): for every voxel of the projector's geometry, the
+ * sum over views [start_view, end_view) of (65535 - bilinear uint16
+ * projection value) x the voxel's chord length, in the reference's float
+ * accumulation order; npf float [Z][N][N] is overwritten.  proj uint16
+ * [n_views][H][W].  With ite != 0 the registration shifts are ignored, as in
+ * the reference.  Host or device buffers; host calls are synchronous. */
+int vcbct_projector_lengthproj(vcbct_projector* p, int ite, int start_view, int end_view,
+                               const uint16_t* proj, int proj_on_device, float* npf, int npf_on_device,
+                               void* stream);
+/* MLEM-type update with a total-variation penalty (replaces IR_ImageCBCT,
+ * IR_ImageCBCT.h:1-4 / IR_ImageCBCT.cpp:19-93): out = before * (wbefore +
+ * (1 - wbefore) * npf_re / (npf + weight_tv * TV(before) + 1e-6)), clamped
+ * and masked as the reference does.  Arrays [Z][N][N]; all host or all device
+ * (on_device). */
+int vcbct_ir_update(int N, int Z, double scale, const short* before, float* out, const float* npf,
+                    const float* npf_re, double wbefore, double weight_tv, double weight_prior,
+                    int on_device, void* stream);
+/* Reference-named forms, host arrays, same argument lists (the unused ones
+ * are ignored as in the reference). */
+void lengthproj(int ite, int reconSize, int reconSlices, short* reconImageshort,
+                unsigned short* ProjImageshort, float* npf_float, unsigned short* projVolume,
+                double reconScale, double reconStep, int projImgWidth, int projImgHeight,
+                int startProjNumber, int endProjNumber, double* ProjAngle, double* cosTable,
+                double* sinTable, double* XcenterShift, double* YcenterShift, double xfactor,
+                double* xalpha, double DETECTOR_PITCH_CM, double DETECTOR_PITCH_CM_AT_ISO_CENT,
+                double DIST_BTWN_SRC_AND_ISOCENT_CM, double DETECTOR_PIXEL_NUM, double x_reg,
+                double y_reg, double z_reg);
+void IR_ImageCBCT(const int ite, int reconSize, int reconSlices, double reconScale,
+                  short* reconImageshort_before, float* reconImagefloat, float* npf_float,
+                  float* npf_float_re, double wbefore, double weight_tv, double weight_prior,
+                  const int thinout);
+
 /* Forward projection that allocates no memory (no counterpart in the
  * reference).  For callers that cannot let a library call cudaMalloc: hosts
  * that own all device memory in their own fixed arena, latency-critical

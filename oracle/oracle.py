@@ -382,3 +382,65 @@ def ref_fdk_load(txt):
                 proj_ext=ext.value.decode(), recon_file=outn.value.decode(),
                 panel_class=sml.value.decode(), angles_rad=ang[:used].copy(),
                 xshift=xs[:used].copy(), yshift=ys[:used].copy())
+
+
+# ------------------------------------------------------ iterative recon --
+
+def lengthproj(g, tables, proj, ite=0, views=None):
+    """P/lengthproj.cpp:10-131 restated; proj uint16 [V][H][W] -> float [Z][N][N]."""
+    L = lib()
+    L.orc_lengthproj.restype = None
+    cosT, sinT, Xc, Yc = [np.ascontiguousarray(t, np.float64) for t in tables]
+    v0, v1 = (0, g.V) if views is None else views
+    proj = np.ascontiguousarray(proj, np.uint16)
+    npf = np.zeros((g.Z, g.N, g.N), np.float32)
+    L.orc_lengthproj(C.c_int(ite), C.c_int(g.N), C.c_int(g.Z), _ptr(proj, _u16p), _ptr(npf, _fp),
+                     C.c_double(g.s), C.c_double(g.step), C.c_int(g.W), C.c_int(g.H), C.c_int(v0), C.c_int(v1),
+                     _ptr(cosT, _dp), _ptr(sinT, _dp), _ptr(Xc, _dp), _ptr(Yc, _dp), C.c_double(g.pdet),
+                     C.c_double(g.piso), C.c_double(g.sad), C.c_double(g.dpn), C.c_double(g.x_reg),
+                     C.c_double(g.y_reg), C.c_double(g.z_reg))
+    return npf
+
+
+def ir_update(N, Z, scale, before, npf, npf_re, wbefore, wtv, wprior):
+    """P/IR_ImageCBCT.cpp:10-93 restated."""
+    L = lib()
+    L.orc_ir_update.restype = None
+    before = np.ascontiguousarray(before, np.int16)
+    npf = np.ascontiguousarray(npf, np.float32)
+    npf_re = np.ascontiguousarray(npf_re, np.float32)
+    out = np.zeros((Z, N, N), np.float32)
+    L.orc_ir_update(C.c_int(N), C.c_int(Z), C.c_double(scale), before.ctypes.data_as(C.POINTER(C.c_short)),
+                    _ptr(out, _fp), _ptr(npf, _fp), _ptr(npf_re, _fp), C.c_double(wbefore), C.c_double(wtv),
+                    C.c_double(wprior))
+    return out
+
+
+def ref_lengthproj(g, tables, proj, ite=0, views=None):
+    """The reference's own lengthproj (compiled from P/lengthproj.cpp)."""
+    L = ref_proj()
+    L.ref_lengthproj.restype = None
+    cosT, sinT, Xc, Yc = [np.ascontiguousarray(t, np.float64) for t in tables]
+    v0, v1 = (0, g.V) if views is None else views
+    proj = np.ascontiguousarray(proj, np.uint16)
+    npf = np.zeros((g.Z, g.N, g.N), np.float32)
+    L.ref_lengthproj(C.c_int(ite), C.c_int(g.N), C.c_int(g.Z), _ptr(proj, _u16p), _ptr(npf, _fp),
+                     C.c_double(g.s), C.c_double(g.step), C.c_int(g.W), C.c_int(g.H), C.c_int(v0), C.c_int(v1),
+                     _ptr(cosT, _dp), _ptr(sinT, _dp), _ptr(Xc, _dp), _ptr(Yc, _dp), C.c_double(g.pdet),
+                     C.c_double(g.piso), C.c_double(g.sad), C.c_double(g.dpn), C.c_double(g.x_reg),
+                     C.c_double(g.y_reg), C.c_double(g.z_reg))
+    return npf
+
+
+def ref_ir_update(N, Z, scale, before, npf, npf_re, wbefore, wtv, wprior):
+    """The reference's own IR_ImageCBCT (compiled from P/IR_ImageCBCT.cpp)."""
+    L = ref_proj()
+    L.ref_ir_update.restype = None
+    before = np.ascontiguousarray(before, np.int16).copy()
+    npf = np.ascontiguousarray(npf, np.float32).copy()
+    npf_re = np.ascontiguousarray(npf_re, np.float32).copy()
+    out = np.zeros((Z, N, N), np.float32)
+    L.ref_ir_update(C.c_int(N), C.c_int(Z), C.c_double(scale), before.ctypes.data_as(C.POINTER(C.c_short)),
+                    _ptr(out, _fp), _ptr(npf, _fp), _ptr(npf_re, _fp), C.c_double(wbefore), C.c_double(wtv),
+                    C.c_double(wprior))
+    return out

@@ -28,6 +28,8 @@
 #include "projectionData.h"
 #include "reprojection.h"
 #include "misc.h"
+#include "lengthproj.h"
+#include "IR_ImageCBCT.h"
 void attenuation_coefficient(char* spectrum_data_name, int num_material, float* Attenuation,
                              float* pdf_pe, int* NE, int nthin, char* mat_type);
 
@@ -144,6 +146,22 @@ int ref_proj_load(const char* txt, int* ints /* 8 */, double* dbls /* 12 */,
 }
 
 void ref_free(void* p) { std::free(p); }
+
+/* lengthproj (lengthproj.cpp:10) and IR_ImageCBCT (IR_ImageCBCT.cpp:19) as
+ * they are: arguments the reference ignores are passed as NULL / 0. */
+void ref_lengthproj(int ite, int N, int Z, unsigned short* proj, float* npf, double s, double step, int W, int H,
+                    int v0, int v1, double* cosT, double* sinT, double* Xc, double* Yc, double pdet, double piso,
+                    double sad, double dpn, double xr, double yr, double zr)
+{
+    lengthproj(ite, N, Z, nullptr, nullptr, npf, proj, s, step, W, H, v0, v1, nullptr, cosT, sinT, Xc, Yc, 0.0,
+               nullptr, pdet, piso, sad, dpn, xr, yr, zr);
+}
+
+void ref_ir_update(int N, int Z, double scale, short* before, float* out, float* npf, float* npf_re, double wbefore,
+                   double wtv, double wprior)
+{
+    IR_ImageCBCT(0, N, Z, scale, before, out, npf, npf_re, wbefore, wtv, wprior, 1);
+}
 
 }  // extern "C"
 #endif  /* REF_PROJ */

@@ -529,3 +529,130 @@ void orc_backproject(int N, int Z, int zstart, double step, double scale,
     }
 #undef FV
 }
+
+
+/* ------------------------------------------------------ iterative recon --
+ * Sensitivity backprojection, restating lengthproj (P/lengthproj.cpp:10-131)
+ * operation by operation: per voxel, the views [v0, v1) in order, float
+ * accumulation of (65535 - bilinear projection) x chord length.  npf
+ * [Z][N][N] is overwritten.  Registration shifts are zeroed for ite != 0
+ * (:18-23). */
+void orc_lengthproj(int ite, int N, int Z, const unsigned short* proj, float* npf, double s, double step,
+                    int W, int H, int v0, int v1, const double* cosT, const double* sinT,
+                    const double* Xc, const double* Yc, double pdet, double piso, double sad,
+                    double dpn, double xr, double yr, double zr)
+{
+    if (ite != 0) { xr = 0.0; yr = 0.0; zr = 0.0; }
+    const double maxpix = 65535.0; /* P/physParams.h:63 */
+#pragma omp parallel for
+    for (int jz = 0; jz < Z; jz++) {
+        double rz = Z * step * 0.5 - (jz + 0.5) * step;
+        for (int jy = 0; jy < N; jy++) {
+            double ry = N * s * 0.5 - (jy + 0.5) * s;
+            for (int jx = 0; jx < N; jx++) {
+                double rx = -N * s * 0.5 + (jx + 0.5) * s;
+                float acc = 0.0f;
+                for (int v = v0; v < v1; v++) {
+                    double sx = -sad * sinT[v] + xr;
+                    double sy = sad * cosT[v] + yr;
+                    double sz = zr;
+                    double yslope = fabs(ry - sy), xslope = fabs(rx - sx);
+                    double rr;
+                    if (xslope > yslope) {
+                        double xx0 = rx - 0.5 * s;
+                        double yy0 = (xx0 - sx) / (rx - sx) * (ry - sy) + sy;
+                        double zz0 = (xx0 - sx) / (rx - sx) * (rz - sz) + sz;
+                        double xx1 = rx + 0.5 * s;
+                        double yy1 = (xx1 - sx) / (rx - sx) * (ry - sy) + sy;
+                        double zz1 = (xx1 - sx) / (rx - sx) * (rz - sz) + sz;
+                        rr = sqrt((xx0 - xx1) * (xx0 - xx1) + (yy0 - yy1) * (yy0 - yy1) + (zz0 - zz1) * (zz0 - zz1));
+                    } else {
+                        double yy0 = ry - 0.5 * s;
+                        double xx0 = (yy0 - sy) / (ry - sy) * (rx - sx) + sx;
+                        double zz0 = (yy0 - sy) / (ry - sy) * (rz - sz) + sz;
+                        double yy1 = ry + 0.5 * s;
+                        double xx1 = (yy1 - sy) / (ry - sy) * (rx - sx) + sx;
+                        double zz1 = (yy1 - sy) / (ry - sy) * (rz - sz) + sz;
+                        rr = sqrt((xx0 - xx1) * (xx0 - xx1) + (yy0 - yy1) * (yy0 - yy1) + (zz0 - zz1) * (zz0 - zz1));
+                    }
+                    double ox = sx + pdet / piso * sinT[v] * sad;
+                    double oy = sy - pdet / piso * cosT[v] * sad;
+                    double py = (ox - rx + (sx - rx) / (sy - ry) * ry + (oy - sy) / (ox - sx) * oy) /
+                                ((sx - rx) / (sy - ry) + (oy - sy) / (ox - sx));
+                    double px = ((sx - rx) / (sy - ry) * (py - ry) + rx);
+                    double pz = ((sz - rz) / (sy - ry) * (py - ry) + rz);
+                    double bin = pdet * (dpn / H);
+                    double xshift = -(Xc[v] + H / 2.0) * bin;
+                    double yshift = -(Yc[v] + H / 2.0) * bin;
+                    double vv = -(pz - zr - yshift);
+                    double uu = (px - xr) * cosT[v] + (py - xr) * sinT[v] + xshift - (W - H) / 2 * bin;
+                    /* the reference's (int) of a non-finite or huge value
+                     * drops the view through its bounds test */
+                    if (!(fabs(vv / bin) < 1.0e9) || !(fabs(uu / bin) < 1.0e9)) continue;
+                    double vfac = vv < 0 ? -0.5 : 0.5;
+                    double ufac = uu < 0 ? -0.5 : 0.5;
+                    int vi1 = (int)(vv / bin + vfac);
+                    int ui1 = (int)(uu / bin + ufac);
+                    double dv1 = vv / bin - vi1;
+                    double du1 = uu / bin - ui1;
+                    int vi2 = vi1, ui2 = ui1;
+                    if (!(fabs(vv - vi1) < 0.000000001)) vi2 = vi1 + ((vv - vi1) > 0 ? 1 : -1);
+                    if (!(fabs(uu - ui1) < 0.000000001)) ui2 = ui1 + ((uu - ui1) > 0 ? 1 : -1);
+                    int r1 = vi1 + H / 2, r2 = vi2 + H / 2, c1 = ui1 + W / 2, c2 = ui2 + W / 2;
+                    if (r1 >= 0 && r1 < H && r2 >= 0 && r2 < H && c1 >= 0 && c1 < W && c2 >= 0 && c2 < W) {
+                        const unsigned short* pv = proj + (size_t)v * W * H;
+                        double np1 = ((1 - dv1) * pv[r1 * W + c1] + dv1 * pv[r1 * W + c2]);
+                        double np2 = ((1 - dv1) * pv[r2 * W + c1] + dv1 * pv[r2 * W + c2]);
+                        double np3 = ((1 - du1) * np1 + du1 * np2);
+                        acc += (float)((maxpix - np3) * rr);
+                    }
+                }
+                npf[((size_t)jz * N + jy) * N + jx] = acc;
+            }
+        }
+    }
+}
+
+/* IR_ImageCBCT (P/IR_ImageCBCT.cpp:10-93) restated. */
+static double orc_tv(int a, int ax, int ay, int az, int ax1, int ay1, int az1, int ayx1, int azx1, int axy1,
+                     int azy1, int axz1, int ayz1)
+{
+    double d1 = sqrt((double)((a - ax) * (a - ax) + (a - ay) * (a - ay) + (a - az) * (a - az))) + 0.00000001;
+    double d2 = sqrt((double)((a - ax1) * (a - ax1) + (ax1 - ayx1) * (ax1 - ayx1) + (ax1 - azx1) * (ax1 - azx1))) +
+                0.00000001;
+    double d3 = sqrt((double)((ay1 - axy1) * (ay1 - axy1) + (a - ay1) * (a - ay1) + (ay1 - azy1) * (ay1 - azy1))) +
+                0.00000001;
+    double d4 = sqrt((double)((az1 - axz1) * (az1 - axz1) + (az1 - ayz1) * (az1 - ayz1) + (a - az1) * (a - az1))) +
+                0.00000001;
+    return ((a - ax) + (a - ay) + (a - az)) / d1 + (a - ax1) / d2 + (a - ay1) / d3 + (a - az1) / d4;
+}
+
+void orc_ir_update(int N, int Z, double scale, const short* before, float* out, const float* npf,
+                   const float* npf_re, double wbefore, double wtv, double wprior)
+{
+    const double rmax = N * 0.5 * 1.0;
+    const size_t NN = (size_t)N * N;
+#pragma omp parallel for
+    for (int z = 0; z < Z; z++)
+        for (int y = 0; y < N; y++)
+            for (int x = 0; x < N; x++) {
+                size_t kk = (size_t)z * NN + (size_t)y * N + x;
+                double cost_tv = 0.0, cost_prior = 0.0;
+                if (z < Z - 1 && y < N - 1 && x < N - 1 && x > 0 && y > 0 && z > 0) {
+#define B(dz, dy, dx) before[kk + (long)(dz) * (long)NN + (long)(dy) * N + (dx)]
+                    cost_tv = orc_tv(B(0, 0, 0), B(0, 0, 1), B(0, 1, 0), B(1, 0, 0), B(0, 0, -1), B(0, -1, 0),
+                                     B(-1, 0, 0), B(0, 1, -1), B(1, 0, -1), B(0, -1, 1), B(1, -1, 0), B(-1, 0, 1),
+                                     B(-1, 1, 0));
+#undef B
+                }
+                double lambda = wtv * cost_tv + wprior * cost_prior + 0.000001;
+                float v = (float)(before[kk] * (wbefore + (1 - wbefore) * npf_re[kk] / (npf[kk] + lambda)));
+                if (v < 0.0) v = 0.0f;
+                else if (v > 65535 / 2) v = 5000.0f;
+                double xx = -N * scale * 0.5 + (x + 0.5) * scale;
+                double yy = N * scale * 0.5 - (y + 0.5) * scale;
+                double r = sqrt((xx) * (xx) + (yy) * (yy));
+                if (r >= rmax) v = 0.0f;
+                out[kk] = v;
+            }
+}

@@ -141,6 +141,15 @@ void orc_backproject(int N, int Z, int zstart, double step, double scale,
                      const double* sinT, const double* xshift,
                      const orc_fdk_consts* c);
 
+/* Iterative reconstruction helpers (P/lengthproj.cpp:10-131,
+ * P/IR_ImageCBCT.cpp:10-93). */
+void orc_lengthproj(int ite, int N, int Z, const unsigned short* proj, float* npf, double s, double step,
+                    int W, int H, int v0, int v1, const double* cosT, const double* sinT,
+                    const double* Xc, const double* Yc, double pdet, double piso, double sad,
+                    double dpn, double xr, double yr, double zr);
+void orc_ir_update(int N, int Z, double scale, const short* before, float* out, const float* npf,
+                   const float* npf_re, double wbefore, double wtv, double wprior);
+
 #ifdef __cplusplus
 }
 #endif

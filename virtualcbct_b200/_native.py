@@ -110,6 +110,14 @@ SIGNATURES = {
     "vcbct_mbfpa_forward_noalloc": (C.c_int, [C.POINTER(ProjGeometryC), _dp, _dp, _dp, _dp, _vp, _fp,
                                               _fp, C.c_int, C.c_double, _vp, _vp]),
     "vcbct_probe_gather": (C.c_int, [C.c_int, _dp, _vp]),
+    "vcbct_projector_lengthproj": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, _vp, C.c_int, _vp, C.c_int, _vp]),
+    "vcbct_ir_update": (C.c_int, [C.c_int, C.c_int, C.c_double, _vp, _vp, _vp, _vp, C.c_double, C.c_double,
+                                  C.c_double, C.c_int, _vp]),
+    "lengthproj": (None, [C.c_int, C.c_int, C.c_int, _vp, _vp, _fp, _vp, C.c_double, C.c_double, C.c_int,
+                          C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, _dp, _dp, C.c_double, _dp, C.c_double,
+                          C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double]),
+    "IR_ImageCBCT": (None, [C.c_int, C.c_int, C.c_int, C.c_double, _vp, _fp, _fp, _fp, C.c_double, C.c_double,
+                            C.c_double, C.c_int]),
     "vcbct_proj_trig_tables": (C.c_int, [C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, C.c_double,
                                          C.c_double, _dp, _dp, _dp, _dp]),
     "vcbct_attenuation_table": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int, C.c_int, _fp, _fp, _ip]),

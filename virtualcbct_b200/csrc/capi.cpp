@@ -366,6 +366,124 @@ static int projector_adjoint(vcbct_projector* p, const float* d_L, const float* 
     return VCBCT_OK;
 }
 
+// ----------------------------------------------------- iterative recon --
+
+extern "C" int vcbct_projector_lengthproj(vcbct_projector* p, int ite, int start_view, int end_view,
+                                          const uint16_t* proj, int proj_on_device, float* npf,
+                                          int npf_on_device, void* stream)
+{
+    if (!p || !proj || !npf) return fail(VCBCT_ERR_ARG, "NULL argument");
+    const auto& g = p->g;
+    if (start_view < 0 || end_view > g.n_views || start_view > end_view)
+        return fail(VCBCT_ERR_ARG, "view range outside [0, n_views]");
+    cudaStream_t st = (cudaStream_t)stream;
+    LpParams q{g.recon_size, g.recon_slices, g.proj_width, g.proj_height, g.recon_scale, g.recon_step,
+               g.det_pitch_cm, g.det_pitch_iso_cm, g.sad_cm, g.det_pixel_num, g.x_reg, g.y_reg, g.z_reg};
+    if (ite != 0) q.xr = q.yr = q.zr = 0.0;  // lengthproj.cpp:18-23
+    const size_t nproj = (size_t)g.n_views * g.proj_height * g.proj_width;
+    const size_t nvox = (size_t)g.recon_size * g.recon_size * g.recon_slices;
+    const size_t nscr = lengthproj_scratch_bytes(end_view - start_view);
+    // scratch: per-view constants, then (host inputs / outputs) the staged arrays
+    const size_t o_proj = (nscr + 255) / 256 * 256;
+    const size_t o_npf = o_proj + (proj_on_device ? 0 : (nproj * sizeof(uint16_t) + 255) / 256 * 256);
+    const size_t total = o_npf + (npf_on_device ? 0 : nvox * sizeof(float));
+    VCBCT_CUDA_TRY(p->stage.ensure(std::max<size_t>(total, 256)));
+    char* base = p->stage.as<char>();
+    const uint16_t* d_proj = proj;
+    float* d_npf = npf;
+    if (!proj_on_device) {
+        VCBCT_CUDA_TRY(cudaMemcpyAsync(base + o_proj, proj, nproj * sizeof(uint16_t), cudaMemcpyHostToDevice, st));
+        d_proj = reinterpret_cast<const uint16_t*>(base + o_proj);
+    }
+    if (!npf_on_device) d_npf = reinterpret_cast<float*>(base + o_npf);
+    VCBCT_CUDA_TRY(launch_lengthproj(q, p->views.as<ViewGeom>(), start_view, end_view, d_proj, d_npf, base, st));
+    if (start_view == end_view) VCBCT_CUDA_TRY(cudaMemsetAsync(d_npf, 0, nvox * sizeof(float), st));
+    if (!npf_on_device) {
+        VCBCT_CUDA_TRY(cudaMemcpyAsync(npf, d_npf, nvox * sizeof(float), cudaMemcpyDeviceToHost, st));
+        VCBCT_CUDA_TRY(cudaStreamSynchronize(st));
+    }
+    return VCBCT_OK;
+}
+
+namespace {
+struct IrScratch {
+    std::mutex mu;
+    DevBuf buf;
+};
+IrScratch& ir_scratch()
+{
+    static IrScratch s;
+    return s;
+}
+}  // namespace
+
+extern "C" int vcbct_ir_update(int N, int Z, double scale, const short* before, float* out, const float* npf,
+                               const float* npf_re, double wbefore, double weight_tv, double weight_prior,
+                               int on_device, void* stream)
+{
+    if (!before || !out || !npf || !npf_re) return fail(VCBCT_ERR_ARG, "NULL argument");
+    if (N <= 0 || Z <= 0) return fail(VCBCT_ERR_ARG, "sizes must be positive");
+    cudaStream_t st = (cudaStream_t)stream;
+    if (on_device) {
+        VCBCT_CUDA_TRY(launch_ir_update(N, Z, scale, before, out, npf, npf_re, wbefore, weight_tv, weight_prior, st));
+        return VCBCT_OK;
+    }
+    const size_t n = (size_t)N * N * Z;
+    const size_t ob = 0, oo = (n * sizeof(short) + 255) / 256 * 256, on = oo + n * sizeof(float),
+                 or_ = on + n * sizeof(float);
+    IrScratch& sc = ir_scratch();
+    std::lock_guard<std::mutex> lk(sc.mu);
+    VCBCT_CUDA_TRY(sc.buf.ensure(or_ + n * sizeof(float)));
+    char* b = sc.buf.as<char>();
+    VCBCT_CUDA_TRY(cudaMemcpyAsync(b + ob, before, n * sizeof(short), cudaMemcpyHostToDevice, st));
+    VCBCT_CUDA_TRY(cudaMemcpyAsync(b + on, npf, n * sizeof(float), cudaMemcpyHostToDevice, st));
+    VCBCT_CUDA_TRY(cudaMemcpyAsync(b + or_, npf_re, n * sizeof(float), cudaMemcpyHostToDevice, st));
+    VCBCT_CUDA_TRY(launch_ir_update(N, Z, scale, reinterpret_cast<short*>(b + ob), reinterpret_cast<float*>(b + oo),
+                                    reinterpret_cast<float*>(b + on), reinterpret_cast<float*>(b + or_), wbefore,
+                                    weight_tv, weight_prior, st));
+    VCBCT_CUDA_TRY(cudaMemcpyAsync(out, b + oo, n * sizeof(float), cudaMemcpyDeviceToHost, st));
+    VCBCT_CUDA_TRY(cudaStreamSynchronize(st));
+    return VCBCT_OK;
+}
+
+// Reference-named entry points of the iterative reconstruction helpers.
+extern "C" void lengthproj(int ite, int reconSize, int reconSlices, short* reconImageshort,
+                           unsigned short* ProjImageshort, float* npf_float, unsigned short* projVolume,
+                           double reconScale, double reconStep, int projImgWidth, int projImgHeight,
+                           int startProjNumber, int endProjNumber, double* ProjAngle, double* cosTable,
+                           double* sinTable, double* XcenterShift, double* YcenterShift, double xfactor,
+                           double* xalpha, double DETECTOR_PITCH_CM, double DETECTOR_PITCH_CM_AT_ISO_CENT,
+                           double DIST_BTWN_SRC_AND_ISOCENT_CM, double DETECTOR_PIXEL_NUM, double x_reg,
+                           double y_reg, double z_reg)
+{
+    (void)reconImageshort;
+    (void)ProjImageshort;
+    (void)ProjAngle;
+    (void)xfactor;
+    (void)xalpha;
+    vcbct_proj_geometry g{reconSize, reconSlices, reconScale, reconStep, projImgWidth, projImgHeight, endProjNumber,
+                          DETECTOR_PITCH_CM, DETECTOR_PITCH_CM_AT_ISO_CENT, DIST_BTWN_SRC_AND_ISOCENT_CM,
+                          DETECTOR_PIXEL_NUM, x_reg, y_reg, z_reg, 1};
+    vcbct_projector* p = nullptr;
+    int rc = vcbct_projector_create(&g, cosTable, sinTable, XcenterShift, YcenterShift, &p);
+    if (!rc) rc = vcbct_projector_lengthproj(p, ite, startProjNumber, endProjNumber, projVolume, 0, npf_float, 0,
+                                             nullptr);
+    if (rc) std::fprintf(stderr, "lengthproj: %s\n", vcbct_last_error());
+    if (p) vcbct_projector_destroy(p);
+}
+
+extern "C" void IR_ImageCBCT(const int ite, int reconSize, int reconSlices, double reconScale,
+                             short* reconImageshort_before, float* reconImagefloat, float* npf_float,
+                             float* npf_float_re, double wbefore, double weight_tv, double weight_prior,
+                             const int thinout)
+{
+    (void)ite;
+    (void)thinout;
+    int rc = vcbct_ir_update(reconSize, reconSlices, reconScale, reconImageshort_before, reconImagefloat, npf_float,
+                             npf_float_re, wbefore, weight_tv, weight_prior, 0, nullptr);
+    if (rc) std::fprintf(stderr, "IR_ImageCBCT: %s\n", vcbct_last_error());
+}
+
 // ------------------------------------------------------------------ batching --
 //
 // A batch is a list of (projector, device output) items.  Two launch

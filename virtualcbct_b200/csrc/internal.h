@@ -92,6 +92,20 @@ struct AdjointArgs {
 };
 cudaError_t launch_adjoint(const AdjointArgs& a, cudaStream_t st);
 
+// ------------------------------------------------------ iterative recon --
+// Geometry of lengthproj (the projector's, with the registration shifts the
+// call uses).
+struct LpParams {
+    int N, Z, W, H;
+    double s, step, pdet, piso, sad, dpn, xr, yr, zr;
+};
+size_t lengthproj_scratch_bytes(int n_views);
+cudaError_t launch_lengthproj(const LpParams& q, const ViewGeom* d_views, int v0, int v1, const uint16_t* d_proj,
+                              float* d_npf, void* d_scratch, cudaStream_t st);
+cudaError_t launch_ir_update(int N, int Z, double scale, const short* d_before, float* d_out, const float* d_npf,
+                             const float* d_npf_re, double wbefore, double weight_tv, double weight_prior,
+                             cudaStream_t st);
+
 // ------------------------------------------------------------------ FDK --
 struct FdkParams {
     int W, H, V, N, Z, zstart, xfactor, redundancy;

@@ -178,6 +178,31 @@ class Projector:
                                                       C.c_void_p(grad.data_ptr()), _stream_ptr(stream)))
         return grad
 
+    def lengthproj(self, proj, ite: int = 0, views=None, npf=None, stream=None):
+        """Sensitivity backprojection of uint16 projections [V][H][W]
+        (lengthproj.cpp:10-131): float [Z][N][N], host or device like proj."""
+        g = self.geom
+        v0, v1 = (0, g.V) if views is None else views
+        L = N.lib()
+        if _is_torch_cuda(proj):
+            import torch
+            pr = proj.contiguous()
+            if pr.dtype not in (torch.int16, torch.uint16):
+                raise ValueError("device projections must be uint16/int16 bits")
+            if npf is None:
+                npf = torch.empty((g.Z, g.N, g.N), dtype=torch.float32, device=pr.device)
+            N.check(L.vcbct_projector_lengthproj(self._h, int(ite), int(v0), int(v1), C.c_void_p(pr.data_ptr()), 1,
+                                                 C.c_void_p(npf.data_ptr()), 1, _stream_ptr(stream)))
+            return npf
+        pr = np.ascontiguousarray(proj, np.uint16)
+        if pr.shape != (g.V, g.H, g.W):
+            raise ValueError("projections must be uint16 [V][H][W]")
+        if npf is None:
+            npf = np.empty((g.Z, g.N, g.N), np.float32)
+        N.check(L.vcbct_projector_lengthproj(self._h, int(ite), int(v0), int(v1), C.c_void_p(pr.ctypes.data), 0,
+                                             C.c_void_p(npf.ctypes.data), 0, None))
+        return npf
+
     def adjoint(self, grad_out, grad=None, stream=None):
         """Accumulate d loss / d volume (float [Z][nmat][N][N], device) for a
         device d loss / d projection ``grad_out`` [V][H][W]."""
