@@ -314,6 +314,39 @@ int vcbct_proj_deck_load_volume(const vcbct_proj_deck* deck, uint16_t* volume,
 int vcbct_flexmap_read(const char* path, int capacity, double* angles_rad, double* xshift,
                        double* yshift, int* n_entries);
 
+/* ---------------------------------------------------- phantom generator */
+
+/* Element volumes from organ-labelled voxel phantoms, as
+ * ICRPphantoms_2mmslice/To_material_distribution_for512_random.cpp does:
+ * vcbct_phantom_tables_read parses the media CSV ("id,H,C,N,O,Na,Mg,P,S,Cl,
+ * K,Ca,Fe,I" mass percentages) and the organ CSV ("organ,medium,density"),
+ * jitters H, C, N (and P, Ca above 0.09 %) of every medium but 53 with
+ * N(mu, 0.1 mu) draws and closes the sum with O (renormalising when O < 0),
+ * draws (and, as the reference does, does not use) a jittered density per
+ * organ, all from the C library's rand() sequence for `seed` (the reference
+ * runs with the default seed 1) in the reference's order, and fills
+ * table[v] = (short)(percent x density x 10) for H, C, N, O, P, Ca of the
+ * last organ row numbered v (0 for numbers without a row; the reference
+ * leaves those voxels uninitialised).  vcbct_organs_to_elements maps an
+ * organ-number volume uint8 [Z][slice_voxels] to uint16
+ * [Z][6][slice_voxels], the projector's input layout; host or device
+ * buffers (on_device), synchronous. */
+#define VCBCT_MAX_MEDIA 100
+#define VCBCT_MAX_ORGANS 150
+typedef struct {
+    int n_media, n_organs;
+    int media_id[VCBCT_MAX_MEDIA];
+    float media[VCBCT_MAX_MEDIA][6];          /* jittered H, C, N, O, P, Ca [%] */
+    int organ[VCBCT_MAX_ORGANS];
+    int organ_medium[VCBCT_MAX_ORGANS];
+    float organ_density[VCBCT_MAX_ORGANS];    /* g/cm3 */
+    uint16_t table[256][6];
+} vcbct_phantom_tables;
+int vcbct_phantom_tables_read(const char* media_csv, const char* organs_csv, unsigned seed,
+                              vcbct_phantom_tables* t);
+int vcbct_organs_to_elements(const uint8_t* ids, long long slice_voxels, int Z,
+                             const vcbct_phantom_tables* t, uint16_t* out, int on_device, void* stream);
+
 /* -------------------------------------------------------------------- FDK */
 
 /* Geometry of filterSinogram / reconstructImage.  The reference fixes

@@ -444,3 +444,25 @@ def ref_ir_update(N, Z, scale, before, npf, npf_re, wbefore, wtv, wprior):
                     _ptr(out, _fp), _ptr(npf, _fp), _ptr(npf_re, _fp), C.c_double(wbefore), C.c_double(wtv),
                     C.c_double(wprior))
     return out
+
+
+def have_icrp_convert() -> bool:
+    return os.path.exists(os.path.join(HERE, "_ref", "icrp_convert"))
+
+
+def ref_icrp_convert(workdir, organ_ids, media_csv, organs_csv):
+    """Run the reference's converter (ICRPphantoms_2mmslice/
+    To_material_distribution_for512_random.cpp, male branch) in `workdir` on
+    an organ-number volume uint8 [100][271][543]; returns its element volume
+    int16 [6][100][271][543] (the whole-volume test.raw it writes)."""
+    import shutil
+    organ_ids = np.ascontiguousarray(organ_ids, np.uint8)
+    assert organ_ids.shape == (100, 271, 543)
+    organ_ids.tofile(os.path.join(workdir, "AM_skin_543x271_700_800.raw"))
+    shutil.copy(media_csv, os.path.join(workdir, "AM_media.csv"))
+    shutil.copy(organs_csv, os.path.join(workdir, "AM_organs.csv"))
+    os.makedirs(os.path.join(workdir, "AM_MD"), exist_ok=True)
+    os.makedirs(os.path.join(workdir, "AM_ED"), exist_ok=True)
+    subprocess.run([os.path.join(HERE, "_ref", "icrp_convert")], cwd=workdir, check=True,
+                   stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+    return np.fromfile(os.path.join(workdir, "test.raw"), np.int16).reshape(6, 100, 271, 543)

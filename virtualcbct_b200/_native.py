@@ -80,6 +80,13 @@ class FdkDeckC(C.Structure):
                 ("yshift", C.c_double * FDK_MAX_VIEWS)]
 
 
+class PhantomTablesC(C.Structure):
+    """vcbct_phantom_tables."""
+    _fields_ = [("n_media", C.c_int), ("n_organs", C.c_int), ("media_id", C.c_int * 100),
+                ("media", (C.c_float * 6) * 100), ("organ", C.c_int * 150), ("organ_medium", C.c_int * 150),
+                ("organ_density", C.c_float * 150), ("table", (C.c_uint16 * 6) * 256)]
+
+
 _vp = C.c_void_p
 _dp = C.POINTER(C.c_double)
 _fp = C.POINTER(C.c_float)
@@ -125,6 +132,9 @@ SIGNATURES = {
     "vcbct_proj_deck_load_volume": (C.c_int, [C.POINTER(ProjDeckC), _vp, _ip]),
     "vcbct_flexmap_read": (C.c_int, [C.c_char_p, C.c_int, _dp, _dp, _dp, _ip]),
     "vcbct_fdk_deck_read": (C.c_int, [C.c_char_p, C.POINTER(FdkDeckC)]),
+    "vcbct_phantom_tables_read": (C.c_int, [C.c_char_p, C.c_char_p, C.c_uint, C.POINTER(PhantomTablesC)]),
+    "vcbct_organs_to_elements": (C.c_int, [_vp, C.c_longlong, C.c_int, C.POINTER(PhantomTablesC), _vp, C.c_int,
+                                           _vp]),
     "vcbct_fdk_default_geometry": (None, [C.POINTER(FdkGeometryC)]),
     "vcbct_fdk_create": (C.c_int, [C.POINTER(FdkGeometryC), _dp, _dp, _dp, C.POINTER(_vp)]),
     "vcbct_fdk_destroy": (C.c_int, [_vp]),

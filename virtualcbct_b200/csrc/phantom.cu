@@ -1,0 +1,217 @@
+// phantom.cu -- element volumes from organ-labelled voxel phantoms, the
+// conversion of ICRPphantoms_2mmslice/To_material_distribution_for512_random.cpp:
+//
+//  - host: the media table (mass percentages of H, C, N, O, P, Ca per medium)
+//    and the organ table (organ number -> medium, density) are read from the
+//    reference's CSV files and jittered with the reference's Gaussian draws
+//    (:14-24, :117-165, :178-198), consuming the C library's rand() sequence
+//    for the given seed in the reference's order, through a private
+//    random_r state so the process's rand() is untouched;
+//  - device: each voxel's organ number is mapped to its six element values
+//    (short)(percent x density x 10) (:212-226) by a table lookup, writing the
+//    projector's [Z][6][rows][cols] uint16 layout.
+#include "internal.h"
+
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+
+namespace vcbct {
+namespace {
+
+// Uniform0 / rand_gauss0 of the reference (:14-24) on a private state.
+struct RefRng {
+    struct random_data data;
+    char state[128];
+    explicit RefRng(unsigned seed)
+    {
+        std::memset(&data, 0, sizeof data);
+        std::memset(state, 0, sizeof state);
+        initstate_r(seed, state, sizeof state, &data);
+    }
+    double uniform()
+    {
+        int32_t r = 0;
+        random_r(&data, &r);
+        return ((double)r + 1.0) / ((double)RAND_MAX + 2.0);
+    }
+    double gauss(double mu, double sigma)
+    {
+        const double PI = 3.14159265;
+        const double u1 = uniform();  // the operand order g++ evaluates
+        const double u2 = uniform();
+        const double z = std::sqrt(-2.0 * std::log(u1)) * std::sin(2.0 * PI * u2);
+        return mu + sigma * z;
+    }
+};
+
+__global__ void organs_to_elements_kernel(const uint8_t* __restrict__ ids, long long slice, int Z,
+                                          const uint16_t* __restrict__ table, uint16_t* __restrict__ out)
+{
+    __shared__ uint16_t t[256 * 6];
+    for (int i = threadIdx.x; i < 256 * 6; i += blockDim.x) t[i] = table[i];
+    __syncthreads();
+    const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int z = blockIdx.y;
+    if (n >= slice || z >= Z) return;
+    const int id = ids[(long long)z * slice + n];
+    uint16_t* o = out + (long long)z * 6 * slice + n;
+#pragma unroll
+    for (int m = 0; m < 6; m++) o[(long long)m * slice] = t[id * 6 + m];
+}
+
+}  // namespace
+}  // namespace vcbct
+
+using namespace vcbct;
+
+extern "C" int vcbct_phantom_tables_read(const char* media_csv, const char* organs_csv, unsigned seed,
+                                         vcbct_phantom_tables* t)
+{
+    if (!media_csv || !organs_csv || !t) return fail(VCBCT_ERR_ARG, "NULL argument");
+    std::memset(t, 0, sizeof *t);
+    RefRng rng(seed);
+    FILE* fp = std::fopen(media_csv, "r");
+    if (!fp) return fail(VCBCT_ERR_IO, std::string("cannot open ") + media_csv);
+    int n = 0;
+    for (;;) {
+        int id;
+        float w[13];
+        const int r = std::fscanf(fp, "%d,%f,%f,%f,%f,%f,%f,%f,%f,%f,%f,%f,%f,%f", &id, &w[0], &w[1], &w[2], &w[3],
+                                  &w[4], &w[5], &w[6], &w[7], &w[8], &w[9], &w[10], &w[11], &w[12]);
+        if (r == EOF) break;
+        if (r != 14) {
+            std::fclose(fp);
+            return fail(VCBCT_ERR_IO, std::string(media_csv) + ": malformed row " + std::to_string(n + 1));
+        }
+        if (n >= VCBCT_MAX_MEDIA) {
+            std::fclose(fp);
+            return fail(VCBCT_ERR_LIMIT, "more media than VCBCT_MAX_MEDIA");
+        }
+        // columns H C N O Na Mg P S Cl K Ca Fe I; keep H C N O P Ca
+        float H = w[0], Cc = w[1], Nn = w[2], O = w[3], P = w[6], Ca = w[10];
+        if (id != 53) {  // medium 53 (air) is not jittered (:119)
+            double sigma = double(H * 0.1), mu = double(H);
+            H = (float)(rng.gauss(mu, sigma));
+            if (H < 0.0) H = 0.0;
+            sigma = double(Cc * 0.1);
+            mu = double(Cc);
+            Cc = (float)(rng.gauss(mu, sigma));
+            if (Cc < 0.0) Cc = 0.0;
+            sigma = double(Nn * 0.1);
+            mu = double(Nn);
+            Nn = (float)(rng.gauss(mu, sigma));
+            if (Nn < 0.0) Nn = 0.0;
+            if (P > 0.09) {
+                sigma = double(P * 0.1);
+                mu = double(P);
+                P = (float)(rng.gauss(mu, sigma));
+                if (P < 0.0) P = 0.0;
+            }
+            if (Ca > 0.09) {
+                sigma = double(Ca * 0.1);
+                mu = double(Ca);
+                Ca = (float)(rng.gauss(mu, sigma));
+                if (Ca < 0.0) Ca = 0.0;
+            }
+        }
+        O = 100 - H - Cc - Nn - P - Ca;  // oxygen closes the sum (:151-162)
+        if (O < 0.0) {
+            const double s = (H + Cc + Nn + P + Ca) * 0.01;
+            O = 0.0;
+            H = H / s;
+            Cc = Cc / s;
+            Nn = Nn / s;
+            P = P / s;
+            Ca = Ca / s;
+        }
+        t->media_id[n] = id;
+        float* m = t->media[n];
+        m[0] = H;
+        m[1] = Cc;
+        m[2] = Nn;
+        m[3] = O;
+        m[4] = P;
+        m[5] = Ca;
+        n++;
+    }
+    std::fclose(fp);
+    t->n_media = n;
+
+    fp = std::fopen(organs_csv, "r");
+    if (!fp) return fail(VCBCT_ERR_IO, std::string("cannot open ") + organs_csv);
+    int k = 0;
+    for (;;) {
+        int organ, medium;
+        float dens;
+        const int r = std::fscanf(fp, "%d,%d,%f", &organ, &medium, &dens);
+        if (r == EOF) break;
+        if (r != 3) {
+            std::fclose(fp);
+            return fail(VCBCT_ERR_IO, std::string(organs_csv) + ": malformed row " + std::to_string(k + 1));
+        }
+        if (k >= VCBCT_MAX_ORGANS) {
+            std::fclose(fp);
+            return fail(VCBCT_ERR_LIMIT, "more organs than VCBCT_MAX_ORGANS");
+        }
+        // the reference draws a jittered density here (:180-195) but writes
+        // the tabulated one (:218-223); the draws still advance the sequence
+        if (medium != 53) {
+            if (medium <= 2) (void)rng.gauss(double(dens * 0.9), double(dens * 0.05));
+            else (void)rng.gauss(double(dens), double(dens * 0.05));
+        }
+        t->organ[k] = organ;
+        t->organ_medium[k] = medium;
+        t->organ_density[k] = dens;
+        k++;
+    }
+    std::fclose(fp);
+    t->n_organs = k;
+
+    // voxel value -> six element values; the last organ row with that number
+    // wins (:214-225); numbers without a row stay 0
+    for (int j = 0; j < k; j++) {
+        const int v = t->organ[j];
+        const int mi = t->organ_medium[j] - 1;  // media are indexed by id - 1 (:218)
+        if (v < 0 || v > 255) continue;
+        if (mi < 0 || mi >= t->n_media) return fail(VCBCT_ERR_ARG, "organ row names a medium that is not listed");
+        for (int e = 0; e < 6; e++) t->table[v][e] = (uint16_t)(short)(t->media[mi][e] * t->organ_density[j] * 10);
+    }
+    return VCBCT_OK;
+}
+
+extern "C" int vcbct_organs_to_elements(const uint8_t* ids, long long slice_voxels, int Z,
+                                        const vcbct_phantom_tables* t, uint16_t* out, int on_device, void* stream)
+{
+    if (!ids || !t || !out) return fail(VCBCT_ERR_ARG, "NULL argument");
+    if (slice_voxels <= 0 || Z <= 0) return fail(VCBCT_ERR_ARG, "sizes must be positive");
+    if (Z > 65535) return fail(VCBCT_ERR_LIMIT, "more than 65535 slices");
+    cudaStream_t st = (cudaStream_t)stream;
+    const size_t nid = (size_t)slice_voxels * Z, nout = nid * 6;
+    void* buf = nullptr;
+    const size_t o_tab = 0, o_ids = 256 * 6 * sizeof(uint16_t), o_out = (o_ids + (on_device ? 0 : nid) + 255) / 256 * 256;
+    const size_t bytes = o_out + (on_device ? 0 : nout * sizeof(uint16_t));
+    VCBCT_CUDA_TRY(cudaMalloc(&buf, bytes));
+    char* b = static_cast<char*>(buf);
+    cudaError_t e = cudaMemcpyAsync(b + o_tab, t->table, 256 * 6 * sizeof(uint16_t), cudaMemcpyHostToDevice, st);
+    const uint8_t* d_ids = ids;
+    uint16_t* d_out = out;
+    if (e == cudaSuccess && !on_device) {
+        e = cudaMemcpyAsync(b + o_ids, ids, nid, cudaMemcpyHostToDevice, st);
+        d_ids = reinterpret_cast<const uint8_t*>(b + o_ids);
+        d_out = reinterpret_cast<uint16_t*>(b + o_out);
+    }
+    if (e == cudaSuccess) {
+        dim3 grid((unsigned)((slice_voxels + 255) / 256), (unsigned)Z);
+        organs_to_elements_kernel<<<grid, 256, 0, st>>>(d_ids, slice_voxels, Z,
+                                                        reinterpret_cast<const uint16_t*>(b + o_tab), d_out);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess && !on_device) e = cudaMemcpyAsync(out, d_out, nout * sizeof(uint16_t), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaFree(buf);
+    if (e != cudaSuccess) return cuda_fail(e, "organs_to_elements");
+    return VCBCT_OK;
+}
