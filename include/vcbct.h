@@ -104,6 +104,25 @@ int vcbct_projector_load_volume_f32(vcbct_projector* p, const float* volume, int
  * in-kernel instead of one launch + D2H copy per energy bin. */
 int vcbct_projector_forward(vcbct_projector* p, float* out, int out_on_device, void* stream);
 
+/* Detector noise of the projections the projector writes (no reference
+ * counterpart in the projector; the model is the reference's gaussiannoise,
+ * prior_weight_production.cpp:24-38, in count units): kind 1 turns every
+ * intensity I into n' / i0 with n = i0 * I and n' = n + sqrt(n) z (z standard
+ * normal from a counter-based generator keyed by `seed` and the pixel's
+ * index, so reproducible and independent of launch shape), clamped to
+ * [0, max_counts]; kind 0 turns it off (default).  Applied in the forward
+ * kernel's epilogue. */
+int vcbct_projector_set_noise(vcbct_projector* p, int kind, double i0, double max_counts,
+                              unsigned long long seed);
+/* The counter-based generator of the noise options: Philox-4x32-10 (Salmon
+ * et al., SC 2011) of counter ctr[4] under key[2] (host function, for
+ * reproducing the draws). */
+void vcbct_philox4x32_10(const uint32_t* ctr, const uint32_t* key, uint32_t* out);
+/* The reference's gaussiannoise on projections in its own units (value =
+ * max_pixvalue - counts), float [n]; host or device; synchronous for host. */
+int vcbct_gaussian_noise(float* proj, size_t n, double max_pixvalue, unsigned long long seed,
+                         int on_device, void* stream);
+
 /* Per-ray element path integrals L[V][H][W][nmat] (float, cm x density
  * units) -- the decomposition state; device pointer. */
 int vcbct_projector_path_integrals(vcbct_projector* p, float* d_L, void* stream);

@@ -85,6 +85,9 @@ struct vcbct_projector {
     int NE = 0;
     int have_u16 = 0, have_f32 = 0;
     int cols_per_block = 4;
+    int noise_kind = 0;
+    double noise_i0 = 0.0, noise_max = 0.0;
+    unsigned long long noise_seed = 0;
     // download of host-bound projections, overlapped with the later views
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t chunk_done[kForwardChunks] = {};
@@ -237,6 +240,45 @@ static int make_fwd_args(vcbct_projector* p, ForwardArgs& a)
     a.vol_f32 = p->have_f32 ? p->vol_f32.as<float4>() : nullptr;
     a.err_flag = reinterpret_cast<int*>(p->counter.as<char>() + 8);
     a.cols_per_block = p->cols_per_block;
+    a.noise_kind = p->noise_kind;
+    a.noise_i0 = p->noise_i0;
+    a.noise_max = p->noise_max;
+    a.noise_seed = p->noise_seed;
+    a.view_offset = 0;
+    return VCBCT_OK;
+}
+
+extern "C" int vcbct_projector_set_noise(vcbct_projector* p, int kind, double i0, double max_counts,
+                                         unsigned long long seed)
+{
+    if (!p) return fail(VCBCT_ERR_ARG, "NULL projector");
+    if (kind != 0 && kind != 1) return fail(VCBCT_ERR_ARG, "noise kind must be 0 (none) or 1 (Gaussian counts)");
+    if (kind == 1 && (!(i0 > 0.0) || !(max_counts > 0.0)))
+        return fail(VCBCT_ERR_ARG, "i0 and max_counts must be positive");
+    p->noise_kind = kind;
+    p->noise_i0 = i0;
+    p->noise_max = max_counts;
+    p->noise_seed = seed;
+    return VCBCT_OK;
+}
+
+extern "C" int vcbct_gaussian_noise(float* proj, size_t n, double max_pixvalue, unsigned long long seed,
+                                    int on_device, void* stream)
+{
+    if (!proj) return fail(VCBCT_ERR_ARG, "NULL argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    if (on_device) {
+        VCBCT_CUDA_TRY(launch_gaussian_noise(proj, n, max_pixvalue, seed, st));
+        return VCBCT_OK;
+    }
+    float* d = nullptr;
+    VCBCT_CUDA_TRY(cudaMalloc(&d, std::max<size_t>(n, 1) * sizeof(float)));
+    cudaError_t e = cudaMemcpyAsync(d, proj, n * sizeof(float), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = launch_gaussian_noise(d, n, max_pixvalue, seed, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(proj, d, n * sizeof(float), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaFree(d);
+    if (e != cudaSuccess) return cuda_fail(e, "gaussian noise");
     return VCBCT_OK;
 }
 
@@ -270,6 +312,7 @@ extern "C" int vcbct_projector_forward(vcbct_projector* p, float* out, int out_o
         const int v0 = (int)((long long)V * c / nch), v1 = (int)((long long)V * (c + 1) / nch);
         ForwardArgs ac = a;
         ac.views = views + v0;
+        ac.view_offset = v0;
         ac.p.V = v1 - v0;
         ac.out = dout + (size_t)v0 * per_view;
         VCBCT_CUDA_TRY(launch_forward(ac, st));

@@ -63,8 +63,15 @@ struct ForwardArgs {
     unsigned long long* seg_count;  // (or nullptr)
     int* err_flag;           // device fault flag
     int cols_per_block;
+    // detector noise on `out` (kind 0: none, 1: Gaussian counts)
+    int noise_kind;
+    int view_offset;         // global index of view 0 of this launch (noise counters)
+    double noise_i0, noise_max;
+    unsigned long long noise_seed;
 };
 cudaError_t launch_forward(const ForwardArgs& a, cudaStream_t st);
+cudaError_t launch_gaussian_noise(float* proj, size_t n, double max_pixvalue, unsigned long long seed,
+                                  cudaStream_t st);
 
 // One phantom of a batched forward projection (u16 volume, no counter).
 struct BatchItem {

@@ -22,6 +22,7 @@
 //    voxel cells carried as integers plus a small fractional offset so that no
 //    FP32 value has to resolve a large coordinate near a plane.
 #include "internal.h"
+#include "noise.cuh"
 
 #include <cfloat>
 #include <climits>
@@ -942,7 +943,14 @@ __device__ __forceinline__ void forward_tile(const ForwardArgs& a, const float4*
         for (int i = 0; i < M; i++)
             if (i < P.nmat) a.L_out[o * P.nmat + i] = L[i];
     }
-    if (a.out) a.out[o] = spectral_sum<M>(s_mu, s_pdf, a.spec.NE, L) * R.leng;
+    if (a.out) {
+        float I = spectral_sum<M>(s_mu, s_pdf, a.spec.NE, L) * R.leng;
+        if (a.noise_kind == 1) {
+            const uint64_t gidx = ((uint64_t)(v + a.view_offset) * P.H + (P.H - 1 - j)) * P.W + jj;
+            I = noisy_intensity(I, a.noise_i0, a.noise_max, gidx, a.noise_seed);
+        }
+        a.out[o] = I;
+    }
 }
 
 __device__ __forceinline__ IvRec* iv_buffer(float4* smem, int NEmax)

@@ -1,0 +1,51 @@
+// noise.cu -- the reference's Gaussian detector noise (gaussiannoise,
+// Release_CBCT_Projection_CM/prior_weight_production.cpp:24-38) on device
+// projections in its units (value = MAX_PIXVALUE - counts): per pixel,
+// n = max - p, n += N(0, sqrt(n)), p = max - n clamped to [0, max].  The
+// reference draws its normals from one rand() stream in pixel order; here
+// each pixel has its own counter-based draw (noise.cuh), so the result is
+// the same distribution, reproducible for a seed and independent of the
+// launch shape.
+#include "internal.h"
+#include "noise.cuh"
+
+namespace vcbct {
+namespace {
+
+__global__ void gaussian_noise_kernel(float* __restrict__ p, size_t n, double maxv, unsigned long long seed)
+{
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        double nstar = maxv - p[i];
+        const double sigma = sqrt(nstar);
+        nstar = nstar + sigma * normal_draw(i, 1u, seed);
+        float v = (float)(maxv - nstar);
+        if (maxv - nstar < 0) v = 0.0f;
+        if (maxv - nstar > maxv) v = (float)maxv;
+        p[i] = v;
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_gaussian_noise(float* proj, size_t n, double max_pixvalue, unsigned long long seed,
+                                  cudaStream_t st)
+{
+    if (n == 0) return cudaSuccess;
+    int dev = 0, sms = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return e;
+    const size_t want = (n + 255) / 256;
+    const unsigned blocks = (unsigned)(want < (size_t)sms * 16 ? want : (size_t)sms * 16);
+    gaussian_noise_kernel<<<blocks, 256, 0, st>>>(proj, n, max_pixvalue, seed);
+    return cudaGetLastError();
+}
+
+}  // namespace vcbct
+
+extern "C" void vcbct_philox4x32_10(const uint32_t* ctr, const uint32_t* key, uint32_t* out)
+{
+    uint32_t c[4] = {ctr[0], ctr[1], ctr[2], ctr[3]};
+    vcbct::philox4x32_10(c, key[0], key[1]);
+    for (int i = 0; i < 4; i++) out[i] = c[i];
+}

@@ -178,6 +178,12 @@ class Projector:
                                                       C.c_void_p(grad.data_ptr()), _stream_ptr(stream)))
         return grad
 
+    def set_noise(self, i0: float = 0.0, max_counts: float = 65535.0, seed: int = 0):
+        """Gaussian detector noise on the projections (i0 = counts of an
+        unattenuated ray; i0 = 0 turns it off)."""
+        kind = 1 if i0 > 0 else 0
+        N.check(N.lib().vcbct_projector_set_noise(self._h, kind, float(i0), float(max_counts), int(seed)))
+
     def lengthproj(self, proj, ite: int = 0, views=None, npf=None, stream=None):
         """Sensitivity backprojection of uint16 projections [V][H][W]
         (lengthproj.cpp:10-131): float [Z][N][N], host or device like proj."""
