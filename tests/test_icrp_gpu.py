@@ -13,14 +13,14 @@ def _tables(tmp_path, seed=3):
     rng = np.random.default_rng(seed)
     media = tmp_path / "media.csv"
     rows = []
-    for i in range(1, 31):
+    for i in range(1, 53):  # media are indexed by id - 1: ids 1..53
         w = rng.uniform(0, 20, size=13)
         w[4:6] = 0.0
         rows.append(",".join([str(i)] + [f"{x:.3f}" for x in w]))
     rows.append("53,0,0,70,30,0,0,0,0,0,0,0,0,0")  # air, not jittered
     media.write_text("\n".join(rows) + "\n")
     organs = tmp_path / "organs.csv"
-    orows = [f"{k},{int(rng.integers(1, 31))},{rng.uniform(0.2, 1.9):.3f}" for k in range(1, 141)]
+    orows = [f"{k},{int(rng.integers(1, 53))},{rng.uniform(0.2, 1.9):.3f}" for k in range(1, 141)]
     orows.append("141,53,0.001")
     organs.write_text("\n".join(orows) + "\n")
     return PhantomTables(str(media), str(organs), seed=7)
