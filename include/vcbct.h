@@ -326,6 +326,13 @@ int vcbct_proj_deck_read(const char* txt_path, vcbct_proj_deck* deck);
  * number goes to *n_incomplete (may be NULL) and a warning to stderr. */
 int vcbct_proj_deck_load_volume(const vcbct_proj_deck* deck, uint16_t* volume,
                                 int* n_incomplete);
+/* The deck's slice files streamed straight into a projector's device volume
+ * (the projector's geometry must have the deck's N, used_slices and mat_num):
+ * slabs of slices are read into pinned memory while the previous slab is
+ * copied and re-laid out on the device.  Same values and missing-file rule as
+ * vcbct_proj_deck_load_volume; synchronous. */
+int vcbct_projector_load_deck(vcbct_projector* p, const vcbct_proj_deck* deck, int* n_incomplete,
+                              void* stream);
 /* Flexmap "angle[deg] xshift yshift class" lines (projectionData.cpp:
  * 164-171): angles_rad = angle * pi / 180.  Entries beyond `capacity` return
  * VCBCT_ERR_LIMIT (the reference writes past its arrays); a malformed line

@@ -84,3 +84,39 @@ def test_proj_then_cbct2_from_decks(cuda, tmp_path, monkeypatch):
     diff = np.abs(vi.astype(np.int32) - rv.astype(np.int16).astype(np.int32))
     assert diff.max() <= 1, f"{(diff > 1).sum()} voxels differ by more than 1 LSB"
     assert np.abs(vi).max() > 0
+
+
+def test_load_deck_streams_the_same_volume(cuda, tmp_path, monkeypatch):
+    """Projector.load_deck (slabs of slices streamed to the GPU) loads what
+    the host reader assembles, including the missing / short file rule."""
+    import torch
+    tmp = str(tmp_path)
+    monkeypatch.chdir(tmp)
+    N, slices, V, W, H = 40, 30, 4, 32, 24
+    vol_all = phantoms.random_volume(N, slices, seed=4, hi=900)
+    for i in range(slices):
+        if i == 13:
+            continue                                   # missing: repeats slice 12
+        raw = vol_all[i].tobytes()
+        if i == 17:
+            raw = raw[: len(raw) // 2]                 # short: tail from slice 16
+        open(os.path.join(tmp, f"elem_{i:03d}.raw"), "wb").write(raw)
+    angles = np.array([float(f"{a:.5f}") for a in phantoms.view_angles(V)])
+    decks.write_flexmap(os.path.join(tmp, "v.flexmap"), angles)
+    decks.write_proj_deck(os.path.join(tmp, "p.txt"), spectrum="s.csv", total_proj=V, proj_width=W,
+                          proj_height=H, angle_file="v.flexmap", mat_prefix="elem", z_ic=15, output_name="o",
+                          scale=(0.25, 0.25, 0.5), recon_size=N, recon_slices=slices, mat_num=6, mat_type="human",
+                          xfactor=1000.0, reg=(0.0, 0.0, 0.0))
+    d = decks.read_proj_deck("p.txt")
+    host_vol, bad = decks.load_proj_volume(d)
+    g = ProjGeometry(N=N, Z=d["used_slices"], s=0.25, step=0.5, W=W, H=H, V=V, z_reg=d["z_reg"])
+    ang = angles * 3.141592653589793238462643383279 / 180.0
+    tabs = trig_tables(W, H, ang, np.zeros(V), np.zeros(V), g.pdet, g.dpn)
+    mu, pdf = attenuation_table(os.path.join(DATA, "spectrum_kramers100_90.csv"), os.path.join(DATA, "xraydb_mini"), 6)
+    from virtualcbct_b200 import Projector
+    a, b = Projector(g, *tabs), Projector(g, *tabs)
+    for p in (a, b):
+        p.set_spectrum(mu, pdf, 1000.0)
+    a.load_volume(host_vol)
+    assert b.load_deck(d) == bad == 2
+    assert torch.equal(a.forward(), b.forward())

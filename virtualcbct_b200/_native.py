@@ -133,6 +133,7 @@ SIGNATURES = {
     "vcbct_attenuation_table": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int, C.c_int, _fp, _fp, _ip]),
     "vcbct_proj_deck_read": (C.c_int, [C.c_char_p, C.POINTER(ProjDeckC)]),
     "vcbct_proj_deck_load_volume": (C.c_int, [C.POINTER(ProjDeckC), _vp, _ip]),
+    "vcbct_projector_load_deck": (C.c_int, [_vp, C.POINTER(ProjDeckC), _ip, _vp]),
     "vcbct_flexmap_read": (C.c_int, [C.c_char_p, C.c_int, _dp, _dp, _dp, _ip]),
     "vcbct_fdk_deck_read": (C.c_int, [C.c_char_p, C.POINTER(FdkDeckC)]),
     "vcbct_phantom_tables_read": (C.c_int, [C.c_char_p, C.c_char_p, C.c_uint, C.POINTER(PhantomTablesC)]),

@@ -9,12 +9,15 @@
 #include <cstdio>
 #include <fstream>
 #include <map>
+#include <memory>
 #include <sstream>
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
 #include <vector>
+
+#include <sys/stat.h>
 
 #include "internal.h"
 
@@ -88,6 +91,10 @@ struct vcbct_projector {
     int noise_kind = 0;
     double noise_i0 = 0.0, noise_max = 0.0;
     unsigned long long noise_seed = 0;
+    // streaming deck loader: pinned slab buffers and their copy events
+    uint16_t* pin = nullptr;
+    size_t pin_bytes = 0;
+    cudaEvent_t slab_copied[2] = {};
     // download of host-bound projections, overlapped with the later views
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t chunk_done[kForwardChunks] = {};
@@ -159,6 +166,9 @@ extern "C" int vcbct_projector_destroy(vcbct_projector* p)
     p->spec_pdf.release();
     p->grad_pk.release();
     p->counter.release();
+    if (p->pin) cudaFreeHost(p->pin);
+    for (cudaEvent_t e : p->slab_copied)
+        if (e) cudaEventDestroy(e);
     if (p->copy_stream) cudaStreamDestroy(p->copy_stream);
     for (cudaEvent_t e : p->chunk_done)
         if (e) cudaEventDestroy(e);
@@ -225,6 +235,72 @@ extern "C" int vcbct_projector_load_volume_f32(vcbct_projector* p, const float* 
     VCBCT_CUDA_TRY(launch_pack_f32(src, g.recon_size, g.recon_slices, g.num_material, p->vol_f32.as<float4>(), st));
     p->have_f32 = 1;
     p->have_u16 = 0;
+    return VCBCT_OK;
+}
+
+// Slice files of a projector deck streamed into the packed volume: slabs of
+// kDeckSlab slices are read into one of two pinned buffers while the other is
+// copied to the device and re-laid out there, so disk reads, the copy and the
+// re-layout overlap.  Missing or short files keep the previous slice's values
+// (zeros for the first), as the reference's reused read buffer does
+// (projectionData.cpp:187-215).
+constexpr int kDeckSlab = 8;
+
+extern "C" int vcbct_projector_load_deck(vcbct_projector* p, const vcbct_proj_deck* d, int* n_incomplete,
+                                         void* stream)
+{
+    if (!p || !d) return fail(VCBCT_ERR_ARG, "NULL argument");
+    const auto& g = p->g;
+    if (d->recon_size != g.recon_size || d->used_slices != g.recon_slices || d->mat_num != g.num_material)
+        return fail(VCBCT_ERR_ARG, "deck volume (N, used slices, mat_num) differs from the projector's geometry");
+    cudaStream_t st = (cudaStream_t)stream;
+    const size_t slice = (size_t)g.recon_size * g.recon_size * g.num_material;
+    const size_t slab = (size_t)kDeckSlab * slice;
+    if (p->pin_bytes < 2 * slab * sizeof(uint16_t)) {
+        if (p->pin) cudaFreeHost(p->pin);
+        p->pin = nullptr;
+        p->pin_bytes = 0;
+        VCBCT_CUDA_TRY(cudaHostAlloc((void**)&p->pin, 2 * slab * sizeof(uint16_t), cudaHostAllocDefault));
+        p->pin_bytes = 2 * slab * sizeof(uint16_t);
+    }
+    for (cudaEvent_t& e : p->slab_copied)
+        if (!e) VCBCT_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    VCBCT_CUDA_TRY(p->stage.ensure(2 * slab * sizeof(uint16_t)));
+    VCBCT_CUDA_TRY(p->vol_u16.ensure(packed_u16_bytes(g.recon_size, g.recon_slices)));
+    std::vector<uint16_t> zeros(slice, 0);
+    const uint16_t* prev = zeros.data();
+    int bad = 0;
+    char name[600];
+    const int Z = g.recon_slices;
+    for (int z0 = 0, b = 0; z0 < Z; z0 += kDeckSlab, b++) {
+        const int k = b & 1, nz = std::min(kDeckSlab, Z - z0);
+        uint16_t* host = p->pin + (size_t)k * slab;
+        if (b >= 2) VCBCT_CUDA_TRY(cudaEventSynchronize(p->slab_copied[k]));  // buffer k copied out
+        for (int t = 0; t < nz; t++) {
+            uint16_t* dst = host + (size_t)t * slice;
+            std::snprintf(name, sizeof name, "%s_%03d.raw", d->mat_prefix, d->slice_first + z0 + t);
+            size_t got = 0;
+            FILE* fp = std::fopen(name, "rb");
+            if (fp) {
+                got = std::fread(dst, 1, slice * sizeof(uint16_t), fp) / sizeof(uint16_t);
+                std::fclose(fp);
+            }
+            if (got < slice) {
+                std::fprintf(stderr, fp ? "WARNING: pixel data size unmatch (%s)\n" : "data file: %s not found\n", name);
+                std::memcpy(dst + got, prev + got, (slice - got) * sizeof(uint16_t));
+                bad++;
+            }
+            prev = dst;
+        }
+        uint16_t* dev = p->stage.as<uint16_t>() + (size_t)k * slab;
+        VCBCT_CUDA_TRY(cudaMemcpyAsync(dev, host, (size_t)nz * slice * sizeof(uint16_t), cudaMemcpyHostToDevice, st));
+        VCBCT_CUDA_TRY(cudaEventRecord(p->slab_copied[k], st));
+        VCBCT_CUDA_TRY(launch_pack_u16_slab(dev, g.recon_size, nz, z0, Z, g.num_material, p->vol_u16.as<uint4>(), st));
+    }
+    VCBCT_CUDA_TRY(cudaStreamSynchronize(st));
+    p->have_u16 = 1;
+    p->have_f32 = 0;
+    if (n_incomplete) *n_incomplete = bad;
     return VCBCT_OK;
 }
 
@@ -863,6 +939,61 @@ extern "C" int vcbct_proj_trig_tables(int W, int H, int V, const double* angles,
     return VCBCT_OK;
 }
 
+// The x-ray DB tables (photo / Compton / Rayleigh, 6 elements + energy per
+// row) parsed once per directory and kept for later calls; a change of a
+// file's size or modification time re-reads them.
+struct XrayDb {
+    std::vector<double> e;     // MeV
+    std::vector<double> t[3];  // [row][6]
+    std::string stamp;
+};
+
+static int xray_db(const char* dbdir, std::shared_ptr<const XrayDb>* out)
+{
+    static std::mutex mu;
+    static std::map<std::string, std::shared_ptr<const XrayDb>> cache;
+    const char* names[3] = {"photo_5keVto150keV.csv", "comp_5keVto150keV.csv", "rayl_5keVto150keV.csv"};
+    std::string stamp;
+    for (int t = 0; t < 3; t++) {
+        struct stat sb;
+        const std::string path = std::string(dbdir) + "/" + names[t];
+        if (stat(path.c_str(), &sb) != 0) return fail(VCBCT_ERR_IO, "cannot open " + path);
+        stamp += std::to_string((long long)sb.st_size) + ":" + std::to_string((long long)sb.st_mtime) + ";";
+    }
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = cache.find(dbdir);
+    if (it != cache.end() && it->second->stamp == stamp) {
+        *out = it->second;
+        return VCBCT_OK;
+    }
+    auto dbp = std::make_shared<XrayDb>();
+    XrayDb& db = *dbp;
+    db.stamp = stamp;
+    for (int t = 0; t < 3; t++) {
+        std::string path = std::string(dbdir) + "/" + names[t];
+        FILE* f = std::fopen(path.c_str(), "r");
+        if (!f) return fail(VCBCT_ERR_IO, "cannot open " + path);
+        char line[512];
+        if (!std::fgets(line, sizeof line, f)) {
+            std::fclose(f);
+            return fail(VCBCT_ERR_IO, "empty " + path);
+        }
+        while (std::fgets(line, sizeof line, f)) {
+            double v[7];
+            if (std::sscanf(line, "%lf,%lf,%lf,%lf,%lf,%lf,%lf", &v[0], &v[1], &v[2], &v[3], &v[4], &v[5], &v[6]) != 7) continue;
+            for (int k = 0; k < 6; k++) db.t[t].push_back(v[k]);
+            if (t == 0) db.e.push_back(v[6] / 1000 / 1000);
+        }
+        std::fclose(f);
+    }
+    const size_t nrow = db.e.size();
+    if (nrow == 0 || db.t[1].size() != 6 * nrow || db.t[2].size() != 6 * nrow)
+        return fail(VCBCT_ERR_IO, "x-ray DB tables are inconsistent");
+    cache[dbdir] = dbp;
+    *out = dbp;
+    return VCBCT_OK;
+}
+
 // Spectrum + x-ray DB lookup, following attenuation_coefficient
 // (prior_weight_production.cpp:200-523): bin midpoints in MeV (float sum of
 // the CSV's lo/hi), optional merging of nthin bins, pdf normalised in float,
@@ -911,29 +1042,14 @@ extern "C" int vcbct_attenuation_table(const char* spectrum_csv, const char* dbd
     const float sum = (float)sum_t;
     for (int i = 0; i < NE; i++) pdf[i] = pdf_t[i] / sum;
 
-    const char* names[3] = {"photo_5keVto150keV.csv", "comp_5keVto150keV.csv", "rayl_5keVto150keV.csv"};
-    std::vector<double> db_e;
-    std::vector<double> db[3];
-    for (int t = 0; t < 3; t++) {
-        std::string path = std::string(dbdir) + "/" + names[t];
-        FILE* f = std::fopen(path.c_str(), "r");
-        if (!f) return fail(VCBCT_ERR_IO, "cannot open " + path);
-        char line[512];
-        if (!std::fgets(line, sizeof line, f)) {
-            std::fclose(f);
-            return fail(VCBCT_ERR_IO, "empty " + path);
-        }
-        while (std::fgets(line, sizeof line, f)) {
-            double v[7];
-            if (std::sscanf(line, "%lf,%lf,%lf,%lf,%lf,%lf,%lf", &v[0], &v[1], &v[2], &v[3], &v[4], &v[5], &v[6]) != 7) continue;
-            for (int k = 0; k < 6; k++) db[t].push_back(v[k]);
-            if (t == 0) db_e.push_back(v[6] / 1000 / 1000);
-        }
-        std::fclose(f);
+    std::shared_ptr<const XrayDb> dbp;
+    {
+        int rc = xray_db(dbdir, &dbp);
+        if (rc) return rc;
     }
+    const std::vector<double>& db_e = dbp->e;
+    const std::vector<double>* db = dbp->t;
     const size_t nrow = db_e.size();
-    if (nrow == 0 || db[1].size() != 6 * nrow || db[2].size() != 6 * nrow)
-        return fail(VCBCT_ERR_IO, "x-ray DB tables are inconsistent");
     for (int k = 0; k < nmat; k++) {
         for (int i = 0; i < NE; i++) {
             const double E = (double)e_t[i];

@@ -40,10 +40,6 @@ int main(int argc, char** argv)
     int nread = 0;
     if (vcbct_flexmap_read(d.angle_file, V, ang.data(), xs.data(), ys.data(), &nread)) return die("flexmap");
 
-    const size_t nvox = (size_t)d.used_slices * d.mat_num * d.recon_size * d.recon_size;
-    std::vector<uint16_t> vol(nvox);
-    int incomplete = 0;
-    if (vcbct_proj_deck_load_volume(&d, vol.data(), &incomplete)) return die("volume");
     std::fprintf(stderr, "matImage num = %d, center = %d, z_reg = %f\n", d.used_slices, d.z_ic_local, d.z_reg);
 
     std::vector<double> c(V), s(V), xc(V), yc(V);
@@ -58,7 +54,9 @@ int main(int argc, char** argv)
     if (vcbct_projector_create(&g, c.data(), s.data(), xc.data(), yc.data(), &p)) return die("initialize");
     std::vector<float> out((size_t)V * d.proj_height * d.proj_width);
     int rc = vcbct_projector_set_spectrum(p, mu.data(), pdf.data(), ne, d.xfactor);
-    if (!rc) rc = vcbct_projector_load_volume(p, vol.data(), 0, nullptr);
+    int incomplete = 0;
+    // slice files streamed to the GPU (reads overlap the copies and re-layout)
+    if (!rc) rc = vcbct_projector_load_deck(p, &d, &incomplete, nullptr);
     if (!rc) rc = vcbct_projector_forward(p, out.data(), 0, nullptr);
     if (rc) {
         vcbct_projector_destroy(p);

@@ -39,6 +39,8 @@ struct ProjParams {
 size_t packed_u16_bytes(int N, int Z);
 size_t packed_f32_bytes(int N, int Z);
 
+cudaError_t launch_pack_u16_slab(const uint16_t* src, int N, int nz, int zoff, int Z, int nmat, uint4* dst,
+                                 cudaStream_t st);
 cudaError_t launch_pack_u16(const uint16_t* src, int N, int Z, int nmat, uint4* dst,
                             cudaStream_t st);
 cudaError_t launch_pack_f32(const float* src, int N, int Z, int nmat, float4* dst,

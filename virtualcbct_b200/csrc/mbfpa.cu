@@ -1130,7 +1130,9 @@ __global__ void __launch_bounds__(256, VCBCT_ADJ_MIN_BLOCKS) adjoint_kernel(Adjo
 // ------------------------------------------------------- layout kernels --
 // Reference layout [Z][nmat][N][N] -> packed z-fastest records.
 // grid (ceil(N/32), N, ceil(Z/32)), block (32, 8).
-__global__ void pack_u16_kernel(const uint16_t* __restrict__ src, int N, int Z, int nmat,
+// A slab of nz slices [zoff, zoff + nz) of a Z-slice volume: src holds the
+// slab [nz][nmat][N][N], dst the whole packed volume.
+__global__ void pack_u16_kernel(const uint16_t* __restrict__ src, int N, int nz, int zoff, int Z, int nmat,
                                 uint4* __restrict__ dst)
 {
     __shared__ uint16_t tile[32][8][33];
@@ -1140,21 +1142,21 @@ __global__ void pack_u16_kernel(const uint16_t* __restrict__ src, int N, int Z, 
         const int z = z0 + zz, x = x0 + threadIdx.x;
         for (int m = 0; m < 8; m++) {
             uint16_t v = 0;
-            if (m < nmat && z < Z && x < N) v = src[((size_t)z * nmat + m) * NN + (size_t)y * N + x];
+            if (m < nmat && z < nz && x < N) v = src[((size_t)z * nmat + m) * NN + (size_t)y * N + x];
             tile[zz][m][threadIdx.x] = v;
         }
     }
     __syncthreads();
     for (int xx = threadIdx.y; xx < 32; xx += 8) {
         const int x = x0 + xx, z = z0 + threadIdx.x;
-        if (x >= N || z >= Z) continue;
+        if (x >= N || z >= nz) continue;
         const int zz = threadIdx.x;
         uint4 r;
         r.x = (uint32_t)tile[zz][0][xx] | ((uint32_t)tile[zz][1][xx] << 16);
         r.y = (uint32_t)tile[zz][2][xx] | ((uint32_t)tile[zz][3][xx] << 16);
         r.z = (uint32_t)tile[zz][4][xx] | ((uint32_t)tile[zz][5][xx] << 16);
         r.w = (uint32_t)tile[zz][6][xx] | ((uint32_t)tile[zz][7][xx] << 16);
-        dst[((size_t)y * N + x) * Z + z] = r;
+        dst[((size_t)y * N + x) * Z + zoff + z] = r;
     }
 }
 
@@ -1213,7 +1215,15 @@ __global__ void unpack_grad_kernel(const float* __restrict__ src, int N, int Z, 
 cudaError_t launch_pack_u16(const uint16_t* src, int N, int Z, int nmat, uint4* dst, cudaStream_t st)
 {
     dim3 grid((N + 31) / 32, N, (Z + 31) / 32), block(32, 8);
-    pack_u16_kernel<<<grid, block, 0, st>>>(src, N, Z, nmat, dst);
+    pack_u16_kernel<<<grid, block, 0, st>>>(src, N, Z, 0, Z, nmat, dst);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pack_u16_slab(const uint16_t* src, int N, int nz, int zoff, int Z, int nmat, uint4* dst,
+                                 cudaStream_t st)
+{
+    dim3 grid((N + 31) / 32, N, (nz + 31) / 32), block(32, 8);
+    pack_u16_kernel<<<grid, block, 0, st>>>(src, N, nz, zoff, Z, nmat, dst);
     return cudaGetLastError();
 }
 

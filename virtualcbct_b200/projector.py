@@ -98,6 +98,15 @@ class Projector:
             N.check(L.vcbct_projector_load_volume(self._h, C.c_void_p(v.ctypes.data), 0, None))
             self.loaded = None
 
+    def load_deck(self, deck: dict, stream=None) -> int:
+        """Stream a projector deck's slice files (``decks.read_proj_deck``)
+        into the device volume; returns the number of missing or short
+        slice files."""
+        bad = C.c_int(0)
+        N.check(N.lib().vcbct_projector_load_deck(self._h, C.byref(deck["_c"]), C.byref(bad), _stream_ptr(stream)))
+        self.loaded = None
+        return int(bad.value)
+
     def load_volume_f32(self, vol, stream=None):
         """float32 [Z][nmat][N][N] element volume (host numpy or CUDA torch)."""
         self._check_vol(vol, "float32")
