@@ -403,11 +403,13 @@ def batched_small_section(stream):
         p.load_volume(phantoms.ellipsoid_phantom_torch(g.N, Z, g.s, g.step, seed=500 + i))
         projs.append(p)
     nseg = sum(p.count_segments() for p in projs)
-    b_auto, b_pers = Batch(), Batch()
+    b_auto, b_pers, b_flat = Batch(), Batch(), Batch()
     for p in projs:
         outs.append(b_auto.add(p))
         b_pers.add(p)
-    b_pers.configure(False, 4)
+        b_flat.add(p)
+    b_pers.configure(Batch.PERSISTENT, 4)
+    b_flat.configure(Batch.FLAT, 4)
     tuned = b_auto.autotune()
 
     def t(f, reps=5):
@@ -424,9 +426,11 @@ def batched_small_section(stream):
     plain = t(lambda: [p.forward(o) for p, o in zip(projs, outs)])
     auto = t(lambda: b_auto.forward(use_graph=True))
     pers = t(lambda: b_pers.forward(use_graph=True))
+    flat = t(lambda: b_flat.forward(use_graph=True))
     return {"workload": "64 ellipsoid phantoms 128x128xZ (Z 16-64), V 18-90, 64x64", "segments": nseg,
             "autotuned": tuned, "plain_ms": plain, "batched_graph_ms": auto, "persistent_graph_ms": pers,
-            "batched_over_plain_speedup": plain / auto, "persistent_over_plain_speedup": plain / pers}
+            "flat_graph_ms": flat, "batched_over_plain_speedup": plain / auto,
+            "persistent_over_plain_speedup": plain / pers, "flat_over_plain_speedup": plain / flat}
 
 
 def run_ours(args, rank, world, local_rank):

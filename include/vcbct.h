@@ -153,9 +153,10 @@ int vcbct_projector_adjoint_state(vcbct_projector* p, const float* d_L, const fl
  * volume and a spectrum, each with its own device output [V][H][W]; the items
  * may differ in volume size, view count and detector.  vcbct_batch_forward
  * projects all of them either in one persistent launch that balances the
- * uneven work through a global tile counter (the default), or as per-item
- * launches on two branches forked from `stream` (chosen by
- * vcbct_batch_autotune when faster); with use_graph != 0 the launch sequence
+ * uneven work through a global tile counter (the default), as per-item
+ * launches on two branches forked from `stream`, or in one flat launch with a
+ * block per tile of every item (vcbct_batch_autotune picks the fastest);
+ * with use_graph != 0 the launch sequence
  * is captured into a CUDA graph on the first call and replayed on later calls
  * (the items must not change in between; adding an item rebuilds it). */
 typedef struct vcbct_batch vcbct_batch;
@@ -163,16 +164,17 @@ int vcbct_batch_create(vcbct_batch** out);
 int vcbct_batch_add(vcbct_batch* b, vcbct_projector* p, float* d_out);
 int vcbct_batch_forward(vcbct_batch* b, int use_graph, void* stream);
 int vcbct_batch_destroy(vcbct_batch* b);
-/* Fix the launch strategy (per_item 0: persistent, 1: per-item launches) and
- * the columns per block (1, 2, 4 or 8) instead of the defaults (0, 4). */
-int vcbct_batch_configure(vcbct_batch* b, int per_item, int cols_per_block);
+/* Fix the launch strategy (0: persistent launch, 1: per-item launches on two
+ * branches, 2: one flat launch with a block per tile of every item) and the
+ * columns per block (1, 2, 4 or 8) instead of the defaults (0, 4). */
+int vcbct_batch_configure(vcbct_batch* b, int strategy, int cols_per_block);
 
 /* Autotuner: time the launch-shape candidates (columns of the detector per
  * thread block: 2, 4, 8; for a batch also the two launch strategies) on the
  * object's own data and keep the fastest, per geometry signature; with the
  * environment variable VCBCT_TUNE_CACHE naming a file the choices persist
- * across processes.  *chosen = columns per block, plus 100 when a batch uses
- * per-item launches.  d_out receives a projection. */
+ * across processes.  *chosen = columns per block + 100 x the batch strategy.
+ * d_out receives a projection. */
 int vcbct_projector_autotune(vcbct_projector* p, float* d_out, void* stream, int* chosen);
 int vcbct_batch_autotune(vcbct_batch* b, void* stream, int* chosen);
 

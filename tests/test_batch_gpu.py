@@ -29,17 +29,17 @@ def test_batched_equals_plain_launches(cuda):
     plain = [p.forward().cpu().numpy() for p in ps]
     b = Batch()
     outs = [b.add(p) for p in ps]
-    for per_item, cpb in ((False, 4), (True, 4), (False, 2), (True, 8)):
-        b.configure(per_item, cpb)
+    for strategy, cpb in ((0, 4), (1, 4), (2, 4), (0, 2), (1, 8), (2, 8), (2, 2)):
+        b.configure(strategy, cpb)
         for use_graph in (False, True, True):
             for o in outs:
                 o.fill_(float("nan"))
             b.forward(use_graph=use_graph)
             torch.cuda.synchronize()
             for o, ref in zip(outs, plain):
-                assert np.array_equal(o.cpu().numpy(), ref), (per_item, cpb, use_graph)
+                assert np.array_equal(o.cpu().numpy(), ref), (strategy, cpb, use_graph)
     c = b.autotune()
-    assert c % 100 in (2, 4, 8) and c // 100 in (0, 1)
+    assert c % 100 in (2, 4, 8) and c // 100 in (0, 1, 2)
     b.forward(use_graph=True)
     torch.cuda.synchronize()
     for o, ref in zip(outs, plain):

@@ -605,16 +605,20 @@ extern "C" void IR_ImageCBCT(const int ite, int reconSize, int reconSlices, doub
 
 // ------------------------------------------------------------------ batching --
 //
-// A batch is a list of (projector, device output) items.  Two launch
+// A batch is a list of (projector, device output) items.  Three launch
 // strategies, picked by vcbct_batch_autotune:
 //  - persistent: one launch of batch_forward_kernel over every item's tiles
 //    (counter reset + kernel);
 //  - per-item: each item's own forward_kernel launch, spread over two
 //    branches that fork from and join to the caller's stream, so one item's
-//    tail overlaps the next item's start.
+//    tail overlaps the next item's start;
+//  - flat: one launch of flat_batch_kernel with a block per tile of every
+//    item (up to kFlatItems items per launch, their arguments in the
+//    launch's parameter block).
 // Either launch sequence is captured once into a CUDA graph and replayed.
 
 constexpr int kBatchBranches = 2;
+static_assert(sizeof(FlatBatch) <= 32000, "the flat batch parameter block exceeds the kernel parameter limit");
 
 struct vcbct_batch {
     std::vector<vcbct_projector*> proj;
@@ -624,7 +628,8 @@ struct vcbct_batch {
     long long total = 0;
     int NEmax = 0, nmat_max = 0;
     int cols_per_block = 4, blocks = 0;
-    int per_item = 0;   // 1: per-item launches instead of the persistent one
+    int strategy = 0;   // 0: persistent launch, 1: per-item launches, 2: single flat launch
+    std::vector<FlatBatch> flat;  // strategy 2: the launches' parameter blocks
     bool dirty = true;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -674,13 +679,13 @@ extern "C" int vcbct_batch_add(vcbct_batch* b, vcbct_projector* p, float* d_out)
     return VCBCT_OK;
 }
 
-extern "C" int vcbct_batch_configure(vcbct_batch* b, int per_item, int cols_per_block)
+extern "C" int vcbct_batch_configure(vcbct_batch* b, int strategy, int cols_per_block)
 {
     if (!b) return fail(VCBCT_ERR_ARG, "NULL batch");
-    if ((per_item != 0 && per_item != 1) ||
+    if ((strategy < 0 || strategy > 2) ||
         !(cols_per_block == 1 || cols_per_block == 2 || cols_per_block == 4 || cols_per_block == 8))
-        return fail(VCBCT_ERR_ARG, "per_item must be 0 or 1 and cols_per_block 1, 2, 4 or 8");
-    b->per_item = per_item;
+        return fail(VCBCT_ERR_ARG, "strategy must be 0, 1 or 2 and cols_per_block 1, 2, 4 or 8");
+    b->strategy = strategy;
     b->cols_per_block = cols_per_block;
     b->dirty = true;
     return VCBCT_OK;
@@ -710,6 +715,22 @@ static int batch_build(vcbct_batch* b)
         b->nmat_max = std::max(b->nmat_max, p->g.num_material);
     }
     b->total = u;
+    // parameter blocks of the flat strategy, kFlatItems items each
+    b->flat.clear();
+    for (size_t i0 = 0; i0 < it.size(); i0 += kFlatItems) {
+        FlatBatch fb{};
+        const size_t n = std::min<size_t>(kFlatItems, it.size() - i0);
+        fb.nitems = (int)n;
+        long long t = 0;
+        for (size_t i = 0; i < n; i++) {
+            fb.fa[i] = it[i0 + i].fa;
+            fb.ncolb[i] = it[i0 + i].ncolb;
+            fb.begin[i] = t;
+            t += (long long)it[i0 + i].ncolb * it[i0 + i].fa.p.V * ((it[i0 + i].fa.p.H + 31) / 32);
+        }
+        fb.begin[n] = t;
+        b->flat.push_back(fb);
+    }
     VCBCT_CUDA_TRY(b->items.ensure(sizeof(BatchItem) * it.size()));
     VCBCT_CUDA_TRY(cudaMemcpy(b->items.p, it.data(), sizeof(BatchItem) * it.size(), cudaMemcpyHostToDevice));
     VCBCT_CUDA_TRY(b->counter.ensure(64));
@@ -725,7 +746,12 @@ static int batch_build(vcbct_batch* b)
 
 static int batch_launch(vcbct_batch* b, cudaStream_t st)
 {
-    if (!b->per_item) {
+    if (b->strategy == 2) {
+        for (const FlatBatch& fb : b->flat)
+            VCBCT_CUDA_TRY(launch_flat_batch(fb, b->NEmax, b->nmat_max, b->cols_per_block, st));
+        return VCBCT_OK;
+    }
+    if (b->strategy == 0) {
         VCBCT_CUDA_TRY(launch_batch_forward(b->items.as<BatchItem>(), (int)b->proj.size(), b->total, b->NEmax,
                                             b->nmat_max, b->cols_per_block, b->blocks,
                                             b->counter.as<unsigned long long>(), st));
@@ -892,13 +918,13 @@ extern "C" int vcbct_batch_autotune(vcbct_batch* b, void* stream, int* chosen)
         key << ":" << p->g.recon_size << "x" << p->g.recon_slices << "x" << p->g.n_views << "x" << p->g.proj_width
             << "x" << p->g.proj_height;
     auto it = g_tune.find(key.str());
-    int bestc = b->cols_per_block + 100 * b->per_item;
+    int bestc = b->cols_per_block + 100 * b->strategy;
     if (it == g_tune.end()) {
         cudaStream_t st = (cudaStream_t)stream;
         float best = 1e30f;
-        for (int mode : {0, 1}) {
+        for (int mode : {0, 1, 2}) {
             for (int c : {2, 4, 8}) {
-                b->per_item = mode;
+                b->strategy = mode;
                 b->cols_per_block = c;
                 b->dirty = true;
                 float ms = time_ms([&]() { vcbct_batch_forward(b, 0, stream); }, st, 1);
@@ -912,7 +938,7 @@ extern "C" int vcbct_batch_autotune(vcbct_batch* b, void* stream, int* chosen)
     } else {
         bestc = it->second;
     }
-    b->per_item = bestc >= 100 ? 1 : 0;
+    b->strategy = bestc / 100;
     b->cols_per_block = bestc % 100;
     b->dirty = true;
     if (chosen) *chosen = bestc;

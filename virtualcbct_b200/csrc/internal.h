@@ -75,6 +75,16 @@ cudaError_t launch_forward(const ForwardArgs& a, cudaStream_t st);
 cudaError_t launch_gaussian_noise(float* proj, size_t n, double max_pixvalue, unsigned long long seed,
                                   cudaStream_t st);
 
+// Items of one single-launch batch, passed in the kernel's parameter block.
+constexpr int kFlatItems = 40;
+struct FlatBatch {
+    int nitems;
+    int ncolb[kFlatItems];
+    long long begin[kFlatItems + 1];  // first tile of each item; begin[nitems] = total
+    ForwardArgs fa[kFlatItems];
+};
+cudaError_t launch_flat_batch(const FlatBatch& b, int NEmax, int nmat_max, int cols_per_block, cudaStream_t st);
+
 // One phantom of a batched forward projection (u16 volume, no counter).
 struct BatchItem {
     ForwardArgs fa;

@@ -987,6 +987,35 @@ __global__ void VCBCT_FWD_BOUNDS forward_kernel(ForwardArgs a)
     forward_tile<M, F32VOL, COUNT>(a, s_mu, s_pdf, iv_buffer(smem, a.spec.NE), blockIdx.y, blockIdx.z, blockIdx.x);
 }
 
+// Single-launch batched forward projection: one block per work tile of every
+// item, the items' arguments in the launch's parameter block.  A block finds
+// its item by a binary search over the items' first tiles; the index only
+// depends on blockIdx, so the item's arguments are read from the parameter
+// bank like forward_kernel's and cost no registers per thread.
+template <int M>
+__global__ void VCBCT_FWD_BOUNDS flat_batch_kernel(const __grid_constant__ FlatBatch b)
+{
+    extern __shared__ float4 smem[];
+    const long long u = blockIdx.x;
+    int lo = 0, hi = b.nitems - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (b.begin[mid] <= u) lo = mid;
+        else hi = mid - 1;
+    }
+    const ForwardArgs& fa = b.fa[lo];
+    float4* s_mu = smem;
+    float* s_pdf = reinterpret_cast<float*>(smem + 2 * fa.spec.NE);
+    load_spectrum(fa.spec, s_mu, s_pdf);
+    __syncthreads();
+    const long long w = u - b.begin[lo];
+    const int colb = (int)(w % b.ncolb[lo]);
+    const long long rest = w / b.ncolb[lo];
+    const int v = (int)(rest % fa.p.V);
+    const int rowt = (int)(rest / fa.p.V);
+    forward_tile<M, false, false>(fa, s_mu, s_pdf, iv_buffer(smem, fa.spec.NE), v, rowt, colb);
+}
+
 // Persistent batched forward projection: every block repeatedly takes the
 // next work tile from a global counter.  Tiles are numbered item by item,
 // and within an item by row band, then view, then column block (the order of
@@ -1274,6 +1303,21 @@ cudaError_t launch_batch_forward(const BatchItem* d_items, int nitems, long long
     return cudaGetLastError();
 }
 
+cudaError_t launch_flat_batch(const FlatBatch& b, int NEmax, int nmat_max, int cols_per_block, cudaStream_t st)
+{
+    const long long total = b.begin[b.nitems];
+    if (total <= 0) return cudaSuccess;
+    if (total > 0x7fffffffLL) return cudaErrorInvalidValue;
+    dim3 block(32, cols_per_block);
+    size_t shm = ((size_t)2 * NEmax + (NEmax + 3) / 4) * sizeof(float4) +
+                 (size_t)cols_per_block * kIvSlots * sizeof(IvRec);
+    auto k = (nmat_max <= 6) ? flat_batch_kernel<6> : flat_batch_kernel<8>;
+    // (the shared-memory attribute is set by batch_blocks_per_sm, before any
+    // stream capture)
+    k<<<(unsigned)total, block, shm, st>>>(b);
+    return cudaGetLastError();
+}
+
 int batch_blocks_per_sm(int nmat_max, int cols_per_block, int NEmax)
 {
     size_t shm = ((size_t)2 * NEmax + (NEmax + 3) / 4) * sizeof(float4) +
@@ -1281,6 +1325,9 @@ int batch_blocks_per_sm(int nmat_max, int cols_per_block, int NEmax)
     int n = 0;
     auto k = (nmat_max <= 6) ? batch_forward_kernel<6> : batch_forward_kernel<8>;
     if (shm > 48 * 1024 && cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm) != cudaSuccess)
+        return 0;
+    auto kf = (nmat_max <= 6) ? flat_batch_kernel<6> : flat_batch_kernel<8>;
+    if (shm > 48 * 1024 && cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm) != cudaSuccess)
         return 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, 32 * cols_per_block, shm);
     return n;

@@ -267,14 +267,17 @@ class Batch:
         N.check(N.lib().vcbct_batch_forward(self._h, int(bool(use_graph)), _stream_ptr(stream)))
         return [o for _, o in self._items]
 
-    def configure(self, per_item: bool = False, cols_per_block: int = 4):
-        """Fix the launch strategy: one persistent launch (per_item=False) or
-        per-item launches on two graph branches; and the columns per block."""
-        N.check(N.lib().vcbct_batch_configure(self._h, int(bool(per_item)), int(cols_per_block)))
+    PERSISTENT, PER_ITEM, FLAT = 0, 1, 2
+
+    def configure(self, strategy: int = 0, cols_per_block: int = 4):
+        """Fix the launch strategy: Batch.PERSISTENT (one persistent launch),
+        Batch.PER_ITEM (per-item launches on two graph branches) or
+        Batch.FLAT (one launch, a block per tile); and the columns per block."""
+        N.check(N.lib().vcbct_batch_configure(self._h, int(strategy), int(cols_per_block)))
 
     def autotune(self, stream=None) -> int:
-        """Time both strategies x {2, 4, 8} columns per block and keep the
-        fastest; returns columns per block, +100 for per-item launches."""
+        """Time the three strategies x {2, 4, 8} columns per block and keep
+        the fastest; returns columns per block + 100 x strategy."""
         c = C.c_int(0)
         N.check(N.lib().vcbct_batch_autotune(self._h, _stream_ptr(stream), C.byref(c)))
         return c.value
