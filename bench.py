@@ -16,8 +16,9 @@ All inputs are seeded synthetic data in the reference's formats.
 
 A step = one forward projection of the whole stack (every ray, every bin).
 `value` is measured with the volume resident in HBM; `e2e` repeats the step
-through the C ABI with pinned host buffers (volume upload + re-layout +
-projection + download inside the timed region).
+through the C ABI (vcbct_projector_project) with pinned host buffers: volume
+upload + re-layout + projection + download inside the timed region, the
+upload and download overlapped with the projection by detector row band.
 
 Usage:  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 For N > 1 run under torch.distributed.run: every rank projects its own copy
@@ -492,9 +493,9 @@ def run_ours(args, rank, world, local_rank):
     h = P._h
     sp = C.c_void_p(stream.cuda_stream)
 
-    def e2e_step():
-        vc._native.check(lib.vcbct_projector_load_volume(h, C.c_void_p(vol_np.ctypes.data), 0, sp))
-        vc._native.check(lib.vcbct_projector_forward(h, C.c_void_p(out_np.ctypes.data), 0, sp))
+    def e2e_step():  # host volume in, host projections out: one reprojectionOnGPU call's work
+        vc._native.check(lib.vcbct_projector_project(h, C.c_void_p(vol_np.ctypes.data),
+                                                     C.c_void_p(out_np.ctypes.data), sp))
 
     for _ in range(2):
         e2e_step()

@@ -104,6 +104,17 @@ int vcbct_projector_load_volume_f32(vcbct_projector* p, const float* volume, int
  * in-kernel instead of one launch + D2H copy per energy bin. */
 int vcbct_projector_forward(vcbct_projector* p, float* out, int out_on_device, void* stream);
 
+/* vcbct_projector_load_volume + vcbct_projector_forward from host memory to
+ * host memory in one call, the work of one reprojectionOnGPU call
+ * (reprojectionOnGPU.cu:838-1056 with its volume upload, :867): the
+ * volume [Z][nmat][N][N] goes up in slabs of slices while the detector is
+ * projected in bands of 32 rows, each band as soon as the slices it reads are
+ * in, and each band's rows come back while later bands are projected (the
+ * download overlaps only into page-locked `out`).  Returns when `out` is
+ * written; the volume stays loaded.  Results are bitwise those of the
+ * two-call form. */
+int vcbct_projector_project(vcbct_projector* p, const uint16_t* volume, float* out, void* stream);
+
 /* Detector noise of the projections the projector writes (no reference
  * counterpart in the projector; the model is the reference's gaussiannoise,
  * prior_weight_production.cpp:24-38, in count units): kind 1 turns every

@@ -102,6 +102,7 @@ SIGNATURES = {
     "vcbct_projector_load_volume": (C.c_int, [_vp, _vp, C.c_int, _vp]),
     "vcbct_projector_load_volume_f32": (C.c_int, [_vp, _vp, C.c_int, _vp]),
     "vcbct_projector_forward": (C.c_int, [_vp, _vp, C.c_int, _vp]),
+    "vcbct_projector_project": (C.c_int, [_vp, _vp, _vp, _vp]),
     "vcbct_projector_path_integrals": (C.c_int, [_vp, _vp, _vp]),
     "vcbct_projector_count_segments": (C.c_int, [_vp, C.POINTER(C.c_ulonglong), _vp]),
     "vcbct_projector_adjoint": (C.c_int, [_vp, _vp, _vp, _vp]),

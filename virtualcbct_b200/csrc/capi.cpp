@@ -5,6 +5,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <climits>
 #include <cmath>
 #include <cstdio>
 #include <fstream>
@@ -99,6 +100,18 @@ struct vcbct_projector {
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t chunk_done[kForwardChunks] = {};
     cudaEvent_t copies_done = nullptr;
+    // host-to-host projection (vcbct_projector_project): upload stream, an
+    // event per uploaded slab and per projected row band, and the slices each
+    // row band reads (computed once per view set)
+    cudaStream_t up_stream = nullptr;
+    cudaStream_t band_stream = nullptr;  // every other row band, so one band's tail overlaps the next
+    cudaStream_t pack_stream = nullptr;  // re-layout of uploaded slabs, at the highest priority
+    std::vector<cudaEvent_t> slab_copied_ev;
+    cudaEvent_t up_start = nullptr, up_done = nullptr, bands_done = nullptr;
+    std::vector<cudaEvent_t> slab_ready, band_done;
+    std::vector<int> band_span;  // [2 * bands]: first and last slice (Z, -1: reads none)
+    int band_V = -1;
+    DevBuf band_dev;
 };
 
 extern "C" const char* vcbct_last_error(void) { return g_last_error.c_str(); }
@@ -158,6 +171,9 @@ extern "C" int vcbct_projector_create(const vcbct_proj_geometry* g, const double
 extern "C" int vcbct_projector_destroy(vcbct_projector* p)
 {
     if (!p) return VCBCT_OK;
+    if (p->up_stream) cudaStreamSynchronize(p->up_stream);
+    if (p->band_stream) cudaStreamSynchronize(p->band_stream);
+    if (p->pack_stream) cudaStreamSynchronize(p->pack_stream);
     p->views.release();
     p->vol_u16.release();
     p->vol_f32.release();
@@ -173,6 +189,15 @@ extern "C" int vcbct_projector_destroy(vcbct_projector* p)
     for (cudaEvent_t e : p->chunk_done)
         if (e) cudaEventDestroy(e);
     if (p->copies_done) cudaEventDestroy(p->copies_done);
+    if (p->up_stream) cudaStreamDestroy(p->up_stream);
+    if (p->band_stream) cudaStreamDestroy(p->band_stream);
+    if (p->pack_stream) cudaStreamDestroy(p->pack_stream);
+    for (cudaEvent_t e : p->slab_copied_ev) cudaEventDestroy(e);
+    for (cudaEvent_t e : {p->up_start, p->up_done, p->bands_done})
+        if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : p->slab_ready) cudaEventDestroy(e);
+    for (cudaEvent_t e : p->band_done) cudaEventDestroy(e);
+    p->band_dev.release();
     delete p;
     return VCBCT_OK;
 }
@@ -402,6 +427,203 @@ extern "C" int vcbct_projector_forward(vcbct_projector* p, float* out, int out_o
     VCBCT_CUDA_TRY(cudaStreamWaitEvent(st, p->copies_done, 0));
     VCBCT_CUDA_TRY(cudaStreamSynchronize(st));
     return VCBCT_OK;
+}
+
+// Slices each detector row band of 32 rows reads, over all views (once per
+// view set; a small launch and a synchronisation of `st`).
+static int band_footprints(vcbct_projector* p, cudaStream_t st)
+{
+    const int nb = (p->pp.H + 31) / 32;
+    if (p->band_V == p->pp.V && (int)p->band_span.size() == 2 * nb) return VCBCT_OK;
+    std::vector<int> span(2 * (size_t)nb);
+    for (int b = 0; b < nb; b++) {
+        span[2 * b] = p->pp.Z;
+        span[2 * b + 1] = -1;
+    }
+    VCBCT_CUDA_TRY(p->band_dev.ensure(span.size() * sizeof(int)));
+    VCBCT_CUDA_TRY(cudaMemcpyAsync(p->band_dev.p, span.data(), span.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+    VCBCT_CUDA_TRY(launch_band_footprint(p->pp, p->views.as<ViewGeom>(), p->band_dev.as<int>(), st));
+    VCBCT_CUDA_TRY(cudaMemcpyAsync(span.data(), p->band_dev.p, span.size() * sizeof(int), cudaMemcpyDeviceToHost, st));
+    VCBCT_CUDA_TRY(cudaStreamSynchronize(st));
+    p->band_span = span;
+    p->band_V = p->pp.V;
+    return VCBCT_OK;
+}
+
+static int grow_events(std::vector<cudaEvent_t>& ev, size_t n)
+{
+    while (ev.size() < n) {
+        cudaEvent_t e;
+        VCBCT_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        ev.push_back(e);
+    }
+    return VCBCT_OK;
+}
+
+// Host volume in, host projections out (the whole of reprojectionOnGPU's
+// work), with the volume's upload overlapped with the projection: the volume
+// goes up in slabs of kDeckSlab slices on one stream, each slab re-laid out
+// as it lands on another of the highest priority (so that its blocks take the
+// first free slots among the projection's, and the copies never wait for
+// them); the detector is projected in row bands of 32 rows (all
+// views per launch), each band launched as soon as the slabs it reads are in
+// (its slice footprint is computed once per view set; bands alternate between
+// two streams so that one band's last blocks overlap the next band's first),
+// and each band's rows are downloaded on another stream while later bands are
+// projected.  Bands
+// are taken greedily, the one that needs the fewest slabs not yet requested
+// first, and slabs are uploaded in the order the bands request them.  The
+// result is bitwise that of vcbct_projector_load_volume + _forward.
+static int project_host(vcbct_projector* p, const uint16_t* vol, float* out, cudaStream_t st)
+{
+    const auto& g = p->g;
+    if (p->NE <= 0) return fail(VCBCT_ERR_STATE, "no spectrum set");
+    ForwardArgs a;
+    p->have_u16 = 1;  // the volume is (re)written below
+    p->have_f32 = 0;
+    int rc = make_fwd_args(p, a);
+    if (rc) return rc;
+    if (!p->copy_stream) {
+        VCBCT_CUDA_TRY(cudaStreamCreateWithFlags(&p->copy_stream, cudaStreamNonBlocking));
+        for (cudaEvent_t& e : p->chunk_done) VCBCT_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        VCBCT_CUDA_TRY(cudaEventCreateWithFlags(&p->copies_done, cudaEventDisableTiming));
+    }
+    if (!p->up_stream) {
+        VCBCT_CUDA_TRY(cudaStreamCreateWithFlags(&p->up_stream, cudaStreamNonBlocking));
+        VCBCT_CUDA_TRY(cudaEventCreateWithFlags(&p->up_start, cudaEventDisableTiming));
+        VCBCT_CUDA_TRY(cudaEventCreateWithFlags(&p->up_done, cudaEventDisableTiming));
+        VCBCT_CUDA_TRY(cudaStreamCreateWithFlags(&p->band_stream, cudaStreamNonBlocking));
+        VCBCT_CUDA_TRY(cudaEventCreateWithFlags(&p->bands_done, cudaEventDisableTiming));
+        int least = 0, greatest = 0;
+        VCBCT_CUDA_TRY(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+        VCBCT_CUDA_TRY(cudaStreamCreateWithPriority(&p->pack_stream, cudaStreamNonBlocking, greatest));
+    }
+    rc = band_footprints(p, st);
+    if (rc) return rc;
+    const int Z = g.recon_slices, H = g.proj_height, W = g.proj_width, V = g.n_views;
+    const int nb = (H + 31) / 32, nslab = (Z + kDeckSlab - 1) / kDeckSlab;
+    const size_t slice = (size_t)g.recon_size * g.recon_size * g.num_material;
+    const size_t nout = (size_t)V * H * W;
+    VCBCT_CUDA_TRY(p->stage.ensure(vol_elems(g) * sizeof(uint16_t)));
+    VCBCT_CUDA_TRY(p->vol_u16.ensure(packed_u16_bytes(g.recon_size, Z)));
+    VCBCT_CUDA_TRY(p->grad_pk.ensure(nout * sizeof(float)));
+    rc = grow_events(p->slab_ready, nslab);
+    if (!rc) rc = grow_events(p->slab_copied_ev, nslab);
+    if (!rc) rc = grow_events(p->band_done, nb);
+    if (rc) return rc;
+    a.vol_u16 = p->vol_u16.as<uint4>();
+    uint16_t* stage = p->stage.as<uint16_t>();
+    float* dout = p->grad_pk.as<float>();
+    // downloads per band overlap only into page-locked memory (a copy into
+    // pageable memory holds the calling thread); otherwise they follow the
+    // last band
+    cudaPointerAttributes at{};
+    const bool out_locked = cudaPointerGetAttributes(&at, out) == cudaSuccess && at.type == cudaMemoryTypeHost;
+    cudaGetLastError();
+    // the upload overwrites buffers earlier work on `st` may still read
+    VCBCT_CUDA_TRY(cudaEventRecord(p->up_start, st));
+    VCBCT_CUDA_TRY(cudaStreamWaitEvent(p->up_stream, p->up_start, 0));
+    VCBCT_CUDA_TRY(cudaStreamWaitEvent(p->copy_stream, p->up_start, 0));
+    VCBCT_CUDA_TRY(cudaStreamWaitEvent(p->band_stream, p->up_start, 0));
+    const cudaStream_t cs[2] = {st, p->band_stream};
+
+    std::vector<int> pos(nslab, -1);  // upload position of each slab
+    int issued = 0;
+    auto upload = [&](int s) -> int {
+        const int z0 = s * kDeckSlab, nz = std::min(kDeckSlab, Z - z0);
+        uint16_t* dev = stage + (size_t)z0 * slice;
+        VCBCT_CUDA_TRY(cudaMemcpyAsync(dev, vol + (size_t)z0 * slice, (size_t)nz * slice * sizeof(uint16_t),
+                                       cudaMemcpyHostToDevice, p->up_stream));
+        VCBCT_CUDA_TRY(cudaEventRecord(p->slab_copied_ev[issued], p->up_stream));
+        VCBCT_CUDA_TRY(cudaStreamWaitEvent(p->pack_stream, p->slab_copied_ev[issued], 0));
+        VCBCT_CUDA_TRY(launch_pack_u16_slab(dev, g.recon_size, nz, z0, Z, g.num_material, p->vol_u16.as<uint4>(),
+                                            p->pack_stream));
+        VCBCT_CUDA_TRY(cudaEventRecord(p->slab_ready[issued], p->pack_stream));
+        pos[s] = issued++;
+        return VCBCT_OK;
+    };
+    auto download = [&](int b) -> int {
+        const int j1 = std::min(H, 32 * b + 32), r0 = H - j1, nr = j1 - 32 * b;  // rows H-1-j
+        const size_t pitch = (size_t)H * W * sizeof(float);
+        VCBCT_CUDA_TRY(cudaStreamWaitEvent(p->copy_stream, p->band_done[b], 0));
+        VCBCT_CUDA_TRY(cudaMemcpy2DAsync(out + (size_t)r0 * W, pitch, dout + (size_t)r0 * W, pitch,
+                                         (size_t)nr * W * sizeof(float), V, cudaMemcpyDeviceToHost, p->copy_stream));
+        return VCBCT_OK;
+    };
+    std::vector<char> done(nb, 0);
+    std::vector<int> order;
+    for (int step = 0; step < nb; step++) {
+        int best = -1, best_new = INT_MAX;
+        for (int b = 0; b < nb; b++) {
+            if (done[b]) continue;
+            int need = 0;
+            if (p->band_span[2 * b + 1] >= 0)
+                for (int s = p->band_span[2 * b] / kDeckSlab; s <= p->band_span[2 * b + 1] / kDeckSlab; s++)
+                    need += pos[s] < 0;
+            if (need < best_new) {
+                best = b;
+                best_new = need;
+            }
+        }
+        done[best] = 1;
+        int wait = -1;
+        if (p->band_span[2 * best + 1] >= 0) {
+            for (int s = p->band_span[2 * best] / kDeckSlab; s <= p->band_span[2 * best + 1] / kDeckSlab; s++) {
+                if (pos[s] < 0) {
+                    rc = upload(s);
+                    if (rc) return rc;
+                }
+                wait = std::max(wait, pos[s]);
+            }
+        }
+        const cudaStream_t bs = cs[step & 1];
+        if (wait >= 0) VCBCT_CUDA_TRY(cudaStreamWaitEvent(bs, p->slab_ready[wait], 0));
+        ForwardArgs ab = a;
+        ab.out = dout;
+        ab.band0 = best;
+        ab.nbands = 1;
+        VCBCT_CUDA_TRY(launch_forward(ab, bs));
+        VCBCT_CUDA_TRY(cudaEventRecord(p->band_done[best], bs));
+        order.push_back(best);
+        if (out_locked) {
+            rc = download(best);
+            if (rc) return rc;
+        }
+    }
+    for (int s = 0; s < nslab; s++)  // slices no band reads still form the loaded volume
+        if (pos[s] < 0) {
+            rc = upload(s);
+            if (rc) return rc;
+        }
+    if (!out_locked)
+        for (int b : order) {
+            rc = download(b);
+            if (rc) return rc;
+        }
+    VCBCT_CUDA_TRY(cudaEventRecord(p->up_done, p->pack_stream));  // after every copy and re-layout
+    VCBCT_CUDA_TRY(cudaEventRecord(p->bands_done, p->band_stream));
+    VCBCT_CUDA_TRY(cudaEventRecord(p->copies_done, p->copy_stream));
+    VCBCT_CUDA_TRY(cudaStreamWaitEvent(st, p->up_done, 0));
+    VCBCT_CUDA_TRY(cudaStreamWaitEvent(st, p->bands_done, 0));
+    VCBCT_CUDA_TRY(cudaStreamWaitEvent(st, p->copies_done, 0));
+    VCBCT_CUDA_TRY(cudaStreamSynchronize(st));
+    return VCBCT_OK;
+}
+
+extern "C" int vcbct_projector_project(vcbct_projector* p, const uint16_t* vol, float* out, void* stream)
+{
+    if (!p || !vol || !out) return fail(VCBCT_ERR_ARG, "NULL argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    const int rc = project_host(p, vol, out, st);
+    if (rc) {  // nothing may still read `vol` or write `out` after a failed call
+        cudaStreamSynchronize(st);
+        if (p->up_stream) cudaStreamSynchronize(p->up_stream);
+        if (p->pack_stream) cudaStreamSynchronize(p->pack_stream);
+        if (p->band_stream) cudaStreamSynchronize(p->band_stream);
+        if (p->copy_stream) cudaStreamSynchronize(p->copy_stream);
+        p->have_u16 = 0;
+    }
+    return rc;
 }
 
 extern "C" int vcbct_projector_path_integrals(vcbct_projector* p, float* d_L, void* stream)
@@ -1165,9 +1387,8 @@ extern "C" void reprojectionOnGPU(int ite, int reconSize, int reconSlices, unsig
     p->g.n_views = V;
     p->pp.V = V;
     int rc = vcbct_projector_set_spectrum(p, Attenuation, pdf_pe, NE, xfactor);
-    if (!rc) rc = vcbct_projector_load_volume(p, reconImageshort, 0, nullptr);
     std::vector<float> out((size_t)V * projImgHeight * projImgWidth);
-    if (!rc) rc = vcbct_projector_forward(p, out.data(), 0, nullptr);
+    if (!rc) rc = vcbct_projector_project(p, reconImageshort, out.data(), nullptr);
     p->g.n_views = saveV;
     p->pp.V = saveV;
     if (rc) {

@@ -68,10 +68,15 @@ struct ForwardArgs {
     // detector noise on `out` (kind 0: none, 1: Gaussian counts)
     int noise_kind;
     int view_offset;         // global index of view 0 of this launch (noise counters)
+    int band0, nbands;       // detector row bands [band0, band0 + nbands) of 32 rows (nbands 0: all)
     double noise_i0, noise_max;
     unsigned long long noise_seed;
 };
 cudaError_t launch_forward(const ForwardArgs& a, cudaStream_t st);
+// Slice range [span[2b], span[2b+1]] the forward projection of detector row
+// band b (rows 32b..32b+31, all views) can read; span must hold (Z, -1) per
+// band on entry (bands that read nothing keep it).
+cudaError_t launch_band_footprint(const ProjParams& P, const ViewGeom* d_views, int* d_span, cudaStream_t st);
 cudaError_t launch_gaussian_noise(float* proj, size_t n, double max_pixvalue, unsigned long long seed,
                                   cudaStream_t st);
 

@@ -984,7 +984,48 @@ __global__ void VCBCT_FWD_BOUNDS forward_kernel(ForwardArgs a)
     float* s_pdf = reinterpret_cast<float*>(smem + 2 * a.spec.NE);
     load_spectrum(a.spec, s_mu, s_pdf);
     __syncthreads();
-    forward_tile<M, F32VOL, COUNT>(a, s_mu, s_pdf, iv_buffer(smem, a.spec.NE), blockIdx.y, blockIdx.z, blockIdx.x);
+    forward_tile<M, F32VOL, COUNT>(a, s_mu, s_pdf, iv_buffer(smem, a.spec.NE), blockIdx.y, a.band0 + blockIdx.z,
+                                   blockIdx.x);
+}
+
+// Slices each detector row band can read, reduced over the band's rays of
+// every view.  Conservative: the z cells of the ray's line over the
+// iterations [klo - 1, khi] it marches (the warp-wide march reads nothing
+// outside them), one cell of margin each way, and the first segment's slice.
+// grid: (ceil(W / 8), V, ceil(H / 32)); block: (32, 8).
+__global__ void __launch_bounds__(256) band_footprint_kernel(ProjParams P, const ViewGeom* __restrict__ views,
+                                                             int* __restrict__ span)
+{
+    const int jj = blockIdx.x * 8 + threadIdx.y, j = blockIdx.z * 32 + threadIdx.x;
+    int lo = INT_MAX, hi = -1;
+    if (jj < P.W && j < P.H) {
+        RayPlan R;
+        ray_setup(P, views[blockIdx.y], j, jj, R);
+        if (R.active) {
+            if (R.first_idx >= 0) {
+                const int z = R.first_idx % P.Z;
+                lo = min(lo, z);
+                hi = max(hi, z);
+            }
+            if (R.klo <= R.khi) {
+                const int nzm = (int)(P.Z * 0.5);
+                const double za = R.Z0 + R.Z1 * (double)(R.klo - 1), zb = R.Z0 + R.Z1 * (double)R.khi;
+                const double zmin = fmin(za, zb), zmax = fmax(za, zb);
+                // slice q = nzm - 1 - floor(z) (q = -1 reads slice 0)
+                const double qlo = (double)(nzm - 2) - floor(zmax), qhi = (double)nzm - floor(zmin);
+                if (qhi >= -1.0 && qlo <= (double)(P.Z - 1)) {
+                    lo = min(lo, (int)fmax(0.0, qlo));
+                    hi = max(hi, (int)fmax(0.0, fmin(qhi, (double)(P.Z - 1))));
+                }
+            }
+        }
+    }
+    lo = __reduce_min_sync(0xffffffffu, lo);
+    hi = __reduce_max_sync(0xffffffffu, hi);
+    if (threadIdx.x == 0 && hi >= 0) {
+        atomicMin(span + 2 * blockIdx.z, lo);
+        atomicMax(span + 2 * blockIdx.z + 1, hi);
+    }
 }
 
 // Single-launch batched forward projection: one block per work tile of every
@@ -1275,7 +1316,7 @@ static cudaError_t launch_fwd_t(const ForwardArgs& a, cudaStream_t st)
 {
     const int cpb = a.cols_per_block;
     dim3 block(32, cpb);
-    dim3 grid((a.p.W + cpb - 1) / cpb, a.p.V, (a.p.H + 31) / 32);
+    dim3 grid((a.p.W + cpb - 1) / cpb, a.p.V, a.nbands > 0 ? a.nbands : (a.p.H + 31) / 32);
     size_t shm = ((size_t)2 * a.spec.NE + (a.spec.NE + 3) / 4) * sizeof(float4) +
                  (size_t)cpb * kIvSlots * sizeof(IvRec);
     auto k = forward_kernel<M, F32VOL, COUNT>;
@@ -1331,6 +1372,13 @@ int batch_blocks_per_sm(int nmat_max, int cols_per_block, int NEmax)
         return 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, 32 * cols_per_block, shm);
     return n;
+}
+
+cudaError_t launch_band_footprint(const ProjParams& P, const ViewGeom* d_views, int* d_span, cudaStream_t st)
+{
+    dim3 grid((P.W + 7) / 8, P.V, (P.H + 31) / 32), block(32, 8);
+    band_footprint_kernel<<<grid, block, 0, st>>>(P, d_views, d_span);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_forward(const ForwardArgs& a, cudaStream_t st)

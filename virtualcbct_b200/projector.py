@@ -139,6 +139,23 @@ class Projector:
             N.check(L.vcbct_projector_forward(self._h, C.c_void_p(out.ctypes.data), 0, None))
         return out
 
+    def project(self, vol, out=None):
+        """Host uint16 volume [Z][nmat][N][N] in, host projections float
+        [V][H][W] out, in one call (``vcbct_projector_project``): the volume's
+        upload overlaps the projection.  Bitwise ``load_volume`` + ``forward``;
+        the volume stays loaded."""
+        g = self.geom
+        self._check_vol(vol, "uint16")
+        v = np.ascontiguousarray(vol, np.uint16)
+        if out is None:
+            out = np.empty((g.V, g.H, g.W), np.float32)
+        if out.dtype != np.float32 or not out.flags.c_contiguous or out.size != g.V * g.H * g.W:
+            raise ValueError("host out must be contiguous float32 [V][H][W]")
+        N.check(N.lib().vcbct_projector_project(self._h, C.c_void_p(v.ctypes.data), C.c_void_p(out.ctypes.data),
+                                                None))
+        self.loaded = None
+        return out
+
     def path_integrals(self, stream=None):
         import torch
         g = self.geom
