@@ -323,9 +323,149 @@ def iterative_section(stream):
     npf_re.copy_(npf)
     ir = t(lambda: ir_update(before, npf, npf_re, g.s, 0.5, 0.002, out=out), reps=10)
     nvox = g.N * g.N * g.Z
-    return {"workload": "512x512x100, 36 views of 400x400 uint16",
-            "lengthproj_ms": lp, "lengthproj_gvox_views_s": nvox * g.V / (lp * 1e-3) / 1e9,
-            "ir_update_ms": ir, "ir_update_gvox_s": nvox / (ir * 1e-3) / 1e9}
+    peak, peak_kind = measured_peaks()
+    ir_bytes = 14.0 * nvox  # short before + float npf, npf_re, out (neighbours from cache)
+    res = {"workload": "512x512x100, 36 views of 400x400 uint16",
+           "lengthproj_ms": lp, "lengthproj_gvox_views_s": nvox * g.V / (lp * 1e-3) / 1e9,
+           "lengthproj_bound": "fp64 (the reference's double arithmetic, about 8 divisions per voxel-view)",
+           "ir_update_ms": ir, "ir_update_gvox_s": nvox / (ir * 1e-3) / 1e9,
+           "ir_update_roofline": {"bound": "hbm", "achieved": ir_bytes / (ir * 1e-3) / 1e9, "peak": peak,
+                                  "unit": "GB/s", "frac": ir_bytes / (ir * 1e-3) / 1e9 / peak,
+                                  "peak_kind": peak_kind, "bytes": "14 B per voxel"}}
+    try:  # the reference's own lengthproj / IR_ImageCBCT (oracle/_ref), all host threads
+        import oracle as O
+        if O.have_reference():
+            tabs = trig_tables(g.W, g.H, ang, np.zeros(g.V), np.zeros(g.V), g.pdet, g.dpn)
+            proj_h = proj.cpu().numpy().view(np.uint16)
+            t0 = time.perf_counter()
+            O.ref_lengthproj(g, tabs, proj_h, views=(0, 2))
+            lp_cpu = (time.perf_counter() - t0) * g.V / 2
+            b_h, n_h, r_h = before.cpu().numpy(), npf.cpu().numpy(), npf_re.cpu().numpy()
+            t0 = time.perf_counter()
+            O.ref_ir_update(g.N, g.Z, g.s, b_h, n_h, r_h, 0.5, 0.002, 0.0)
+            ir_cpu = time.perf_counter() - t0
+            res["cpu_baseline"] = {"lengthproj_ms": lp_cpu * 1e3, "ir_update_ms": ir_cpu * 1e3,
+                                   "cores": os.cpu_count(), "kind": "reference",
+                                   "sample": "lengthproj on 2 of 36 views (extrapolated), "
+                                             "IR_ImageCBCT on the whole volume"}
+    except Exception as e:  # informative, never fatal
+        res["cpu_baseline"] = {"sample": f"unavailable: {e}"}
+    return res
+
+
+def noise_section(stream, P, out):
+    """Detector noise: the reference-unit kernel (gaussiannoise) over a
+    360 x 400 x 400 stack, and the cost of the fused epilogue in the
+    projector (forward with noise minus forward without)."""
+    import ctypes as C
+
+    import torch
+    import virtualcbct_b200 as vc
+    n = out.numel()
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(9)
+    base = 5000.0 + 55000.0 * torch.rand(n, generator=gen, device="cuda")
+    y = base.clone()
+    lib = vc.lib()
+
+    def ev(f, reps):
+        f()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            f()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    sp = C.c_void_p(stream.cuda_stream)
+    k_ms = ev(lambda: vc._native.check(lib.vcbct_gaussian_noise(C.c_void_p(y.data_ptr()), n, 65535.0, 7, 1, sp)),
+              20)
+    plain = ev(lambda: P.forward(out), 3)
+    P.set_noise(2.0e5, 65535.0 * 40, seed=3)
+    noisy = ev(lambda: P.forward(out), 3)
+    P.set_noise(0.0)
+    peak, peak_kind = measured_peaks()
+    gbs = 8.0 * n / (k_ms * 1e-3) / 1e9
+    res = {"workload": "360 x 400 x 400 float projections",
+           "kernel_ms": k_ms, "kernel_gpix_s": n / (k_ms * 1e-3) / 1e9,
+           "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s", "frac": gbs / peak,
+                        "peak_kind": peak_kind, "bytes": "8 B per pixel (read + write)"},
+           "forward_ms": plain, "forward_with_noise_ms": noisy}
+    try:
+        import oracle as O
+        if O.have_reference():
+            m = 4_000_000
+            h = base[:m].cpu().numpy()
+            t0 = time.perf_counter()
+            O.ref_gaussiannoise(h, 1)
+            secs = time.perf_counter() - t0
+            res["cpu_baseline"] = {"value": m / secs / 1e9, "unit": "Gpix/s", "cores": 1, "kind": "reference",
+                                   "sample": f"gaussiannoise() on {m} pixels ({secs:.2f} s)"}
+    except Exception as e:
+        res["cpu_baseline"] = {"sample": f"unavailable: {e}"}
+    return res
+
+
+def phantom_section(stream):
+    """Phantom generator: organ numbers -> six element values (the ICRP
+    conversion's lookup) over a 512 x 512 x 200 organ volume, with seeded
+    synthetic media / organ tables in the reference's CSV formats."""
+    import torch
+    from virtualcbct_b200.icrp import PhantomTables, organs_to_elements
+    tmp = tempfile.mkdtemp(prefix="vcbct_icrp_")
+    try:
+        rng = np.random.default_rng(3)
+        rows = [",".join([str(i)] + [f"{x:.3f}" for x in np.r_[rng.uniform(0, 20, 4), 0, 0,
+                                                                  rng.uniform(0, 2, 7)]]) for i in range(1, 53)]
+        rows.append("53,0,0,70,30,0,0,0,0,0,0,0,0,0")
+        media = os.path.join(tmp, "media.csv")
+        organs = os.path.join(tmp, "organs.csv")
+        with open(media, "w") as f:
+            f.write("\n".join(rows) + "\n")
+        with open(organs, "w") as f:
+            f.write("\n".join(f"{k},{int(rng.integers(1, 53))},{rng.uniform(0.2, 1.9):.3f}"
+                              for k in range(1, 141)) + "\n141,53,0.001\n")
+        tabs = PhantomTables(media, organs, seed=1)
+        gen = torch.Generator(device="cuda")
+        gen.manual_seed(4)
+        Z, R = 200, 512
+        ids = torch.randint(0, 142, (Z, R, R), generator=gen, device="cuda", dtype=torch.int32).to(torch.uint8)
+        out = torch.empty((Z, 6, R, R), dtype=torch.int16, device="cuda")
+        organs_to_elements(ids, tabs, out, stream)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(10):
+            organs_to_elements(ids, tabs, out, stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / 10
+        nvox = Z * R * R
+        peak, peak_kind = measured_peaks()
+        gbs = 13.0 * nvox / (ms * 1e-3) / 1e9
+        res = {"workload": "512 x 512 x 200 organ numbers -> 6 x uint16", "ms": ms,
+               "gvox_s": nvox / (ms * 1e-3) / 1e9,
+               "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s", "frac": gbs / peak,
+                            "peak_kind": peak_kind, "bytes": "13 B per voxel (1 read, 12 written)"}}
+        try:
+            import oracle as O
+            if O.have_icrp_convert():
+                ids_h = np.random.default_rng(5).integers(0, 142, size=(100, 271, 543)).astype(np.uint8)
+                t0 = time.perf_counter()
+                O.ref_icrp_convert(tmp, ids_h, media, organs)
+                secs = time.perf_counter() - t0
+                res["cpu_baseline"] = {"value": ids_h.size / secs / 1e9, "unit": "Gvox/s", "cores": 1,
+                                       "kind": "reference",
+                                       "sample": f"the reference converter on its 543x271x100 volume, whole "
+                                                 f"program incl. its file I/O ({secs:.2f} s)"}
+        except Exception as e:
+            res["cpu_baseline"] = {"sample": f"unavailable: {e}"}
+        return res
+    finally:
+        import shutil
+        shutil.rmtree(tmp, ignore_errors=True)
 
 
 def deck_load_section():
@@ -554,6 +694,8 @@ def run_ours(args, rank, world, local_rank):
         extra["batched_small"] = batched_small_section(stream)
         extra["iterative"] = iterative_section(stream)
         extra["deck_load"] = deck_load_section()
+        extra["noise"] = noise_section(stream, P, out)
+        extra["phantom"] = phantom_section(stream)
 
     # measured gather rooflines: the projector's and the backprojector's
     # access patterns replayed without arithmetic on this device

@@ -368,8 +368,9 @@ int vcbct_flexmap_read(const char* path, int capacity, double* angles_rad, doubl
  * last organ row numbered v (0 for numbers without a row; the reference
  * leaves those voxels uninitialised).  vcbct_organs_to_elements maps an
  * organ-number volume uint8 [Z][slice_voxels] to uint16
- * [Z][6][slice_voxels], the projector's input layout; host or device
- * buffers (on_device), synchronous. */
+ * [Z][6][slice_voxels], the projector's input layout; host buffers
+ * (on_device 0: synchronous) or device buffers (on_device 1: asynchronous on
+ * `stream`, no allocation). */
 #define VCBCT_MAX_MEDIA 100
 #define VCBCT_MAX_ORGANS 150
 typedef struct {

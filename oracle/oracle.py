@@ -446,6 +446,16 @@ def ref_ir_update(N, Z, scale, before, npf, npf_re, wbefore, wtv, wprior):
     return out
 
 
+def ref_gaussiannoise(proj, seed=1):
+    """The reference's gaussiannoise (prior_weight_production.cpp:24-38)
+    after srand(seed), on a copy of float proj (in its 65535-based units)."""
+    L = ref_proj()
+    L.ref_gaussiannoise.restype = None
+    out = np.ascontiguousarray(proj, np.float32).copy()
+    L.ref_gaussiannoise(_ptr(out, _fp), C.c_int(out.size), C.c_uint(seed))
+    return out
+
+
 def have_icrp_convert() -> bool:
     return os.path.exists(os.path.join(HERE, "_ref", "icrp_convert"))
 

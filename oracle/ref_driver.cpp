@@ -30,6 +30,7 @@
 #include "misc.h"
 #include "lengthproj.h"
 #include "IR_ImageCBCT.h"
+int gaussiannoise(float* ProjImagefloat, int NN);  // prior_weight_production.cpp:24 (no header)
 void attenuation_coefficient(char* spectrum_data_name, int num_material, float* Attenuation,
                              float* pdf_pe, int* NE, int nthin, char* mat_type);
 
@@ -161,6 +162,13 @@ void ref_ir_update(int N, int Z, double scale, short* before, float* out, float*
                    double wtv, double wprior)
 {
     IR_ImageCBCT(0, N, Z, scale, before, out, npf, npf_re, wbefore, wtv, wprior, 1);
+}
+
+/* gaussiannoise (prior_weight_production.cpp:24-38) after srand(seed). */
+void ref_gaussiannoise(float* proj, int n, unsigned seed)
+{
+    srand(seed);
+    gaussiannoise(proj, n);
 }
 
 }  // extern "C"

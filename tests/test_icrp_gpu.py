@@ -38,3 +38,9 @@ def test_organs_to_elements_matches_host_lookup(cuda, tmp_path):
     assert np.array_equal(host, ref)
     dev = organs_to_elements(torch.from_numpy(ids).to(cuda), t).cpu().numpy().view(np.uint16)
     assert np.array_equal(dev, ref)
+    # slices of a multiple of 8 voxels take the 8-voxels-per-thread path
+    ids8 = rng.integers(0, 256, size=(5, 32, 48)).astype(np.uint8)
+    ref8 = tab[ids8].transpose(0, 3, 1, 2)
+    dev8 = organs_to_elements(torch.from_numpy(ids8).to(cuda), t).cpu().numpy().view(np.uint16)
+    assert np.array_equal(dev8, ref8)
+    assert np.array_equal(organs_to_elements(ids8, t), ref8)

@@ -9,7 +9,8 @@
 //    random_r state so the process's rand() is untouched;
 //  - device: each voxel's organ number is mapped to its six element values
 //    (short)(percent x density x 10) (:212-226) by a table lookup, writing the
-//    projector's [Z][6][rows][cols] uint16 layout.
+//    projector's [Z][6][rows][cols] uint16 layout (HBM-bound: 1 byte read and
+//    12 written per voxel).
 #include "internal.h"
 
 #include <cmath>
@@ -47,19 +48,66 @@ struct RefRng {
     }
 };
 
-__global__ void organs_to_elements_kernel(const uint8_t* __restrict__ ids, long long slice, int Z,
-                                          const uint16_t* __restrict__ table, uint16_t* __restrict__ out)
+// The element table travels in the launch's parameter block (3 KB), so the
+// device path needs no allocation; it is copied to shared memory, where the
+// lanes' data-dependent lookups are served.
+struct OrganTable {
+    uint16_t t[256 * 6];
+};
+
+// grid: (ceil(slice / (256 * PER)), Z); block 256.  PER voxels per thread:
+// 8 when slice % 8 == 0 (8-byte id loads, 16-byte stores per element plane),
+// else 1.
+template <int PER>
+__global__ void __launch_bounds__(256) organs_to_elements_kernel(const uint8_t* __restrict__ ids, long long slice,
+                                                                 const __grid_constant__ OrganTable tab,
+                                                                 uint16_t* __restrict__ out)
 {
     __shared__ uint16_t t[256 * 6];
-    for (int i = threadIdx.x; i < 256 * 6; i += blockDim.x) t[i] = table[i];
+    for (int i = threadIdx.x; i < 256 * 6; i += blockDim.x) t[i] = tab.t[i];
     __syncthreads();
-    const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long n = ((long long)blockIdx.x * blockDim.x + threadIdx.x) * PER;
     const int z = blockIdx.y;
-    if (n >= slice || z >= Z) return;
-    const int id = ids[(long long)z * slice + n];
+    if (n >= slice) return;
+    const uint8_t* src = ids + (long long)z * slice + n;
     uint16_t* o = out + (long long)z * 6 * slice + n;
+    if constexpr (PER == 8) {
+        const uint2 v = *reinterpret_cast<const uint2*>(src);
+        int id[8];
 #pragma unroll
-    for (int m = 0; m < 6; m++) o[(long long)m * slice] = t[id * 6 + m];
+        for (int k = 0; k < 4; k++) {
+            id[k] = (v.x >> (8 * k)) & 255;
+            id[4 + k] = (v.y >> (8 * k)) & 255;
+        }
+#pragma unroll
+        for (int m = 0; m < 6; m++) {
+            uint4 w;
+            w.x = (uint32_t)t[id[0] * 6 + m] | ((uint32_t)t[id[1] * 6 + m] << 16);
+            w.y = (uint32_t)t[id[2] * 6 + m] | ((uint32_t)t[id[3] * 6 + m] << 16);
+            w.z = (uint32_t)t[id[4] * 6 + m] | ((uint32_t)t[id[5] * 6 + m] << 16);
+            w.w = (uint32_t)t[id[6] * 6 + m] | ((uint32_t)t[id[7] * 6 + m] << 16);
+            *reinterpret_cast<uint4*>(o + (long long)m * slice) = w;
+        }
+    } else {
+        const int id = *src;
+#pragma unroll
+        for (int m = 0; m < 6; m++) o[(long long)m * slice] = t[id * 6 + m];
+    }
+}
+
+static cudaError_t launch_organs(const uint8_t* ids, long long slice, int Z, const OrganTable& tab, uint16_t* out,
+                                 cudaStream_t st)
+{
+    const bool vec = slice % 8 == 0 && (reinterpret_cast<uintptr_t>(ids) & 7) == 0 &&
+                     (reinterpret_cast<uintptr_t>(out) & 15) == 0;
+    if (vec) {
+        dim3 grid((unsigned)((slice / 8 + 255) / 256), (unsigned)Z);
+        organs_to_elements_kernel<8><<<grid, 256, 0, st>>>(ids, slice, tab, out);
+    } else {
+        dim3 grid((unsigned)((slice + 255) / 256), (unsigned)Z);
+        organs_to_elements_kernel<1><<<grid, 256, 0, st>>>(ids, slice, tab, out);
+    }
+    return cudaGetLastError();
 }
 
 }  // namespace
@@ -189,27 +237,22 @@ extern "C" int vcbct_organs_to_elements(const uint8_t* ids, long long slice_voxe
     if (slice_voxels <= 0 || Z <= 0) return fail(VCBCT_ERR_ARG, "sizes must be positive");
     if (Z > 65535) return fail(VCBCT_ERR_LIMIT, "more than 65535 slices");
     cudaStream_t st = (cudaStream_t)stream;
+    OrganTable tab;
+    std::memcpy(tab.t, t->table, sizeof tab.t);
+    if (on_device) {  // asynchronous on `stream`, no allocation
+        VCBCT_CUDA_TRY(launch_organs(ids, slice_voxels, Z, tab, out, st));
+        return VCBCT_OK;
+    }
     const size_t nid = (size_t)slice_voxels * Z, nout = nid * 6;
     void* buf = nullptr;
-    const size_t o_tab = 0, o_ids = 256 * 6 * sizeof(uint16_t), o_out = (o_ids + (on_device ? 0 : nid) + 255) / 256 * 256;
-    const size_t bytes = o_out + (on_device ? 0 : nout * sizeof(uint16_t));
-    VCBCT_CUDA_TRY(cudaMalloc(&buf, bytes));
+    const size_t o_out = (nid + 255) / 256 * 256;
+    VCBCT_CUDA_TRY(cudaMalloc(&buf, o_out + nout * sizeof(uint16_t)));
     char* b = static_cast<char*>(buf);
-    cudaError_t e = cudaMemcpyAsync(b + o_tab, t->table, 256 * 6 * sizeof(uint16_t), cudaMemcpyHostToDevice, st);
-    const uint8_t* d_ids = ids;
-    uint16_t* d_out = out;
-    if (e == cudaSuccess && !on_device) {
-        e = cudaMemcpyAsync(b + o_ids, ids, nid, cudaMemcpyHostToDevice, st);
-        d_ids = reinterpret_cast<const uint8_t*>(b + o_ids);
-        d_out = reinterpret_cast<uint16_t*>(b + o_out);
-    }
-    if (e == cudaSuccess) {
-        dim3 grid((unsigned)((slice_voxels + 255) / 256), (unsigned)Z);
-        organs_to_elements_kernel<<<grid, 256, 0, st>>>(d_ids, slice_voxels, Z,
-                                                        reinterpret_cast<const uint16_t*>(b + o_tab), d_out);
-        e = cudaGetLastError();
-    }
-    if (e == cudaSuccess && !on_device) e = cudaMemcpyAsync(out, d_out, nout * sizeof(uint16_t), cudaMemcpyDeviceToHost, st);
+    uint8_t* d_ids = reinterpret_cast<uint8_t*>(b);
+    uint16_t* d_out = reinterpret_cast<uint16_t*>(b + o_out);
+    cudaError_t e = cudaMemcpyAsync(d_ids, ids, nid, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = launch_organs(d_ids, slice_voxels, Z, tab, d_out, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, d_out, nout * sizeof(uint16_t), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     cudaFree(buf);
     if (e != cudaSuccess) return cuda_fail(e, "organs_to_elements");

@@ -19,6 +19,11 @@ seconds:
   adjoint_state_c4  the same with the forward's path integrals kept
   batch_small    four uneven ellipsoid phantoms (256x256, Z 32-96, V 45-180)
                  in one persistent launch
+  lengthproj_c1  sensitivity backprojection of 36 uint16 400x400 views to
+                 512x512x100 (iterative reconstruction)
+  ir_update_c1   MLEM/TV update of a 512x512x100 short volume
+  noise_c2       reference-unit Gaussian noise on 360 x 400 x 400 floats
+  phantom_512    organ numbers -> element values, 512x512x200
 """
 from __future__ import annotations
 
@@ -120,6 +125,54 @@ def run(case: str, repeats: int = 2) -> str:
             b.add(p)
         for _ in range(repeats):
             out = b.forward(use_graph=False)[0]
+    elif case in ("lengthproj_c1", "ir_update_c1"):
+        from .iterative import ir_update
+        g = ProjGeometry(N=512, Z=100, s=0.05, step=0.2, W=400, H=400, V=36)
+        p = _projector(g, phantoms.view_angles(g.V))
+        gen = torch.Generator(device="cuda")
+        gen.manual_seed(3)
+        proj = torch.randint(20000, 65000, (g.V, g.H, g.W), generator=gen, device="cuda",
+                             dtype=torch.int32).to(torch.int16)
+        npf = torch.empty((g.Z, g.N, g.N), dtype=torch.float32, device="cuda")
+        p.lengthproj(proj, npf=npf)
+        before = torch.randint(0, 3000, (g.Z, g.N, g.N), generator=gen, device="cuda",
+                               dtype=torch.int32).to(torch.int16)
+        out = npf
+        for _ in range(repeats):
+            if case == "lengthproj_c1":
+                p.lengthproj(proj, npf=npf)
+            else:
+                out = ir_update(before, npf, npf, g.s, 0.5, 0.002)
+    elif case == "noise_c2":
+        import ctypes as C
+
+        from . import _native as N
+        gen = torch.Generator(device="cuda")
+        gen.manual_seed(9)
+        out = 5000.0 + 55000.0 * torch.rand(360 * 400 * 400, generator=gen, device="cuda")
+        for _ in range(repeats):
+            N.check(N.lib().vcbct_gaussian_noise(C.c_void_p(out.data_ptr()), out.numel(), 65535.0, 7, 1, None))
+    elif case == "phantom_512":
+        import tempfile
+
+        from .icrp import PhantomTables, organs_to_elements
+        rng = np.random.default_rng(3)
+        with tempfile.TemporaryDirectory() as tmp:
+            media, organs = os.path.join(tmp, "m.csv"), os.path.join(tmp, "o.csv")
+            with open(media, "w") as f:
+                for i in range(1, 53):
+                    f.write(",".join([str(i)] + [f"{x:.3f}" for x in rng.uniform(0, 20, 13)]) + "\n")
+                f.write("53,0,0,70,30,0,0,0,0,0,0,0,0,0\n")
+            with open(organs, "w") as f:
+                for k in range(1, 141):
+                    f.write(f"{k},{int(rng.integers(1, 53))},{rng.uniform(0.2, 1.9):.3f}\n")
+            tabs = PhantomTables(media, organs)
+        gen = torch.Generator(device="cuda")
+        gen.manual_seed(4)
+        ids = torch.randint(0, 141, (200, 512, 512), generator=gen, device="cuda", dtype=torch.int32).to(torch.uint8)
+        out = torch.empty((200, 6, 512, 512), dtype=torch.int16, device="cuda")
+        for _ in range(repeats):
+            organs_to_elements(ids, tabs, out)
     else:
         raise SystemExit(f"unknown case {case!r}; see the module docstring")
     torch.cuda.synchronize()
