@@ -5,23 +5,38 @@
 // reference draws its normals from one rand() stream in pixel order; here
 // each pixel has its own counter-based draw (noise.cuh), so the result is
 // the same distribution, reproducible for a seed and independent of the
-// launch shape.
+// launch shape.  Computed in single precision: the noise of a count n has
+// width sqrt(n), far above float's rounding of values up to 65535.
 #include "internal.h"
 #include "noise.cuh"
 
 namespace vcbct {
 namespace {
 
-__global__ void gaussian_noise_kernel(float* __restrict__ p, size_t n, double maxv, unsigned long long seed)
+__device__ __forceinline__ float ref_unit_noise(float p, float maxv, float z)
 {
-    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        double nstar = maxv - p[i];
-        const double sigma = sqrt(nstar);
-        nstar = nstar + sigma * normal_draw(i, 1u, seed);
-        float v = (float)(maxv - nstar);
-        if (maxv - nstar < 0) v = 0.0f;
-        if (maxv - nstar > maxv) v = (float)maxv;
-        p[i] = v;
+    float nstar = maxv - p;
+    // sqrt(n) from the reciprocal square root (within 2 ulp; NaN for n < 0
+    // as the reference's sqrt gives)
+    const float sigma = nstar == 0.0f ? 0.0f : nstar * rsqrtf(nstar);
+    nstar = nstar + sigma * z;
+    float v = maxv - nstar;
+    if (maxv - nstar < 0.0f) v = 0.0f;
+    if (maxv - nstar > maxv) v = maxv;
+    return v;
+}
+
+// One thread per four pixels (one counter draw, four normals).
+__global__ void gaussian_noise_kernel(float* __restrict__ p, size_t n, float maxv, unsigned long long seed)
+{
+    const size_t nq = (n + 3) / 4;
+    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += (size_t)gridDim.x * blockDim.x) {
+        const float4 z = normal_quad(q, 1u, seed);
+        const float zz[4] = {z.x, z.y, z.z, z.w};
+        const size_t i = 4 * q;
+#pragma unroll
+        for (int k = 0; k < 4; k++)
+            if (i + k < n) p[i + k] = ref_unit_noise(p[i + k], maxv, zz[k]);
     }
 }
 
@@ -35,9 +50,9 @@ cudaError_t launch_gaussian_noise(float* proj, size_t n, double max_pixvalue, un
     cudaError_t e = cudaGetDevice(&dev);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (e != cudaSuccess) return e;
-    const size_t want = (n + 255) / 256;
+    const size_t want = ((n + 3) / 4 + 255) / 256;
     const unsigned blocks = (unsigned)(want < (size_t)sms * 16 ? want : (size_t)sms * 16);
-    gaussian_noise_kernel<<<blocks, 256, 0, st>>>(proj, n, max_pixvalue, seed);
+    gaussian_noise_kernel<<<blocks, 256, 0, st>>>(proj, n, (float)max_pixvalue, seed);
     return cudaGetLastError();
 }
 

@@ -4,7 +4,8 @@
 // "Parallel random numbers: as easy as 1, 2, 3", SC 2011), keyed by a
 // 64-bit seed and counted by the pixel's global index, so a pixel's draw
 // does not depend on the launch shape or on the other pixels; normals by
-// the Box-Muller transform.
+// the Box-Muller transform in single precision (noise of a count n has width
+// sqrt(n), so float's 1e-7 relative rounding is far below it).
 #pragma once
 #include <cstdint>
 
@@ -47,29 +48,55 @@ __host__ __device__ __forceinline__ void philox4x32(uint64_t ctr, uint32_t strea
     out[3] = c[3];
 }
 
-// A standard normal draw for pixel `index` (double precision Box-Muller on
-// two 32-bit uniforms in (0, 1)).
-__device__ __forceinline__ double normal_draw(uint64_t index, uint32_t stream_id, uint64_t seed)
+// Box-Muller on two 32-bit random words, in single precision with the fast
+// hardware logarithm and sine/cosine: two independent standard normals.  The
+// uniforms take the words' top 23 bits (u1 in (0, 1], so the radius is
+// finite; u2's angle centred on zero, where the fast sine/cosine are
+// accurate to ~1e-6 absolute, far below what noise statistics can see).
+__device__ __forceinline__ float2 box_muller(uint32_t a, uint32_t b)
+{
+    const float u1 = 2.0f - __uint_as_float(0x3f800000u | (a >> 9));        // (0, 1]
+    const float u2 = __uint_as_float(0x3f800000u | (b >> 9)) - 1.5f;        // [-0.5, 0.5)
+    const float r = sqrtf(-2.0f * __logf(u1));
+    float s, c;
+    __sincosf(6.283185307179586f * u2, &s, &c);
+    return make_float2(r * c, r * s);
+}
+
+// Four standard normals for pixels 4q .. 4q + 3 from one counter draw:
+// words 0, 1 give pixels 4q (cosine) and 4q + 1 (sine), words 2, 3 pixels
+// 4q + 2 and 4q + 3.
+__device__ __forceinline__ float4 normal_quad(uint64_t q, uint32_t stream_id, uint64_t seed)
 {
     uint32_t w[4];
-    philox4x32(index, stream_id, seed, w);
-    const double u1 = ((double)w[0] + 0.5) * 2.3283064365386963e-10;  // 2^-32
-    const double u2 = ((double)w[1] + 0.5) * 2.3283064365386963e-10;
-    return sqrt(-2.0 * log(u1)) * sinpi(2.0 * u2);
+    philox4x32(q, stream_id, seed, w);
+    const float2 a = box_muller(w[0], w[1]), b = box_muller(w[2], w[3]);
+    return make_float4(a.x, a.y, b.x, b.y);
+}
+
+// The standard normal of pixel `index` (its part of its quad's draw, with
+// only its own Box-Muller pair evaluated).
+__device__ __forceinline__ float normal_draw(uint64_t index, uint32_t stream_id, uint64_t seed)
+{
+    uint32_t w[4];
+    philox4x32(index >> 2, stream_id, seed, w);
+    const bool hi = (index & 2) != 0;
+    const float2 z = box_muller(hi ? w[2] : w[0], hi ? w[3] : w[1]);
+    return (index & 1) ? z.y : z.x;
 }
 
 // Detector counts of an intensity, with Gaussian noise of the count's
 // square-root width (the reference's model, prior_weight_production.cpp:24-38,
 // in count units): n = i0 * I, n' = n + sqrt(n) z, clamped to [0, max_counts];
 // returns n' / i0.
-__device__ __forceinline__ float noisy_intensity(float I, double i0, double max_counts, uint64_t index,
+__device__ __forceinline__ float noisy_intensity(float I, float i0, float max_counts, uint64_t index,
                                                  uint64_t seed)
 {
-    const double n = i0 * (double)I;
-    double m = n + sqrt(n > 0.0 ? n : 0.0) * normal_draw(index, 0u, seed);
-    if (m < 0.0) m = 0.0;
+    const float n = i0 * I;
+    float m = n + sqrtf(n > 0.0f ? n : 0.0f) * normal_draw(index, 0u, seed);
+    if (m < 0.0f) m = 0.0f;
     if (m > max_counts) m = max_counts;
-    return (float)(m / i0);
+    return m / i0;
 }
 
 }  // namespace vcbct

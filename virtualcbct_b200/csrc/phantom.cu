@@ -48,12 +48,18 @@ struct RefRng {
     }
 };
 
-// The element table travels in the launch's parameter block (3 KB), so the
-// device path needs no allocation; it is copied to shared memory, where the
-// lanes' data-dependent lookups are served.
+// The element table travels in the launch's parameter block (4 KB), so the
+// device path needs no allocation: one 16-byte row per organ number (six
+// uint16 elements and two pads), copied to shared memory, where each voxel's
+// data-dependent lookup is one 16-byte read.
 struct OrganTable {
-    uint16_t t[256 * 6];
+    uint4 row[256];
 };
+
+__device__ __forceinline__ uint32_t elem_word(const uint4& r, int w)
+{
+    return w == 0 ? r.x : (w == 1 ? r.y : r.z);
+}
 
 // grid: (ceil(slice / (256 * PER)), Z); block 256.  PER voxels per thread:
 // 8 when slice % 8 == 0 (8-byte id loads, 16-byte stores per element plane),
@@ -63,8 +69,8 @@ __global__ void __launch_bounds__(256) organs_to_elements_kernel(const uint8_t* 
                                                                  const __grid_constant__ OrganTable tab,
                                                                  uint16_t* __restrict__ out)
 {
-    __shared__ uint16_t t[256 * 6];
-    for (int i = threadIdx.x; i < 256 * 6; i += blockDim.x) t[i] = tab.t[i];
+    __shared__ uint4 t[256];
+    t[threadIdx.x] = tab.row[threadIdx.x];
     __syncthreads();
     const long long n = ((long long)blockIdx.x * blockDim.x + threadIdx.x) * PER;
     const int z = blockIdx.y;
@@ -73,25 +79,26 @@ __global__ void __launch_bounds__(256) organs_to_elements_kernel(const uint8_t* 
     uint16_t* o = out + (long long)z * 6 * slice + n;
     if constexpr (PER == 8) {
         const uint2 v = *reinterpret_cast<const uint2*>(src);
-        int id[8];
+        uint4 r[8];
 #pragma unroll
         for (int k = 0; k < 4; k++) {
-            id[k] = (v.x >> (8 * k)) & 255;
-            id[4 + k] = (v.y >> (8 * k)) & 255;
+            r[k] = t[(v.x >> (8 * k)) & 255];
+            r[4 + k] = t[(v.y >> (8 * k)) & 255];
         }
 #pragma unroll
         for (int m = 0; m < 6; m++) {
+            const uint32_t sel = (m & 1) ? 0x7632u : 0x5410u;  // high or low halves of the two words
             uint4 w;
-            w.x = (uint32_t)t[id[0] * 6 + m] | ((uint32_t)t[id[1] * 6 + m] << 16);
-            w.y = (uint32_t)t[id[2] * 6 + m] | ((uint32_t)t[id[3] * 6 + m] << 16);
-            w.z = (uint32_t)t[id[4] * 6 + m] | ((uint32_t)t[id[5] * 6 + m] << 16);
-            w.w = (uint32_t)t[id[6] * 6 + m] | ((uint32_t)t[id[7] * 6 + m] << 16);
+            w.x = __byte_perm(elem_word(r[0], m >> 1), elem_word(r[1], m >> 1), sel);
+            w.y = __byte_perm(elem_word(r[2], m >> 1), elem_word(r[3], m >> 1), sel);
+            w.z = __byte_perm(elem_word(r[4], m >> 1), elem_word(r[5], m >> 1), sel);
+            w.w = __byte_perm(elem_word(r[6], m >> 1), elem_word(r[7], m >> 1), sel);
             *reinterpret_cast<uint4*>(o + (long long)m * slice) = w;
         }
     } else {
-        const int id = *src;
+        const uint4 r = t[*src];
 #pragma unroll
-        for (int m = 0; m < 6; m++) o[(long long)m * slice] = t[id * 6 + m];
+        for (int m = 0; m < 6; m++) o[(long long)m * slice] = (uint16_t)(elem_word(r, m >> 1) >> (16 * (m & 1)));
     }
 }
 
@@ -238,7 +245,12 @@ extern "C" int vcbct_organs_to_elements(const uint8_t* ids, long long slice_voxe
     if (Z > 65535) return fail(VCBCT_ERR_LIMIT, "more than 65535 slices");
     cudaStream_t st = (cudaStream_t)stream;
     OrganTable tab;
-    std::memcpy(tab.t, t->table, sizeof tab.t);
+    std::memset(&tab, 0, sizeof tab);
+    for (int v = 0; v < 256; v++) {
+        const uint16_t* e = t->table[v];
+        tab.row[v] = make_uint4((uint32_t)e[0] | ((uint32_t)e[1] << 16), (uint32_t)e[2] | ((uint32_t)e[3] << 16),
+                                (uint32_t)e[4] | ((uint32_t)e[5] << 16), 0u);
+    }
     if (on_device) {  // asynchronous on `stream`, no allocation
         VCBCT_CUDA_TRY(launch_organs(ids, slice_voxels, Z, tab, out, st));
         return VCBCT_OK;
