@@ -63,6 +63,14 @@ def test_reference_unit_gaussian_noise(cuda):
     y2 = x.clone()
     N.check(N.lib().vcbct_gaussian_noise(C.c_void_p(y2.data_ptr()), y2.numel(), maxv, 7, 1, None))
     assert torch.equal(y, y2)
+    # a stack that is not 16-byte aligned (the per-pixel path) gets the same draws
+    big = torch.empty(1 + 1001, dtype=torch.float32, device=cuda)
+    a = x[:1001].clone()
+    big[1:] = a
+    mis = big[1:]
+    N.check(N.lib().vcbct_gaussian_noise(C.c_void_p(a.data_ptr()), a.numel(), maxv, 9, 1, None))
+    N.check(N.lib().vcbct_gaussian_noise(C.c_void_p(mis.data_ptr()), mis.numel(), maxv, 9, 1, None))
+    assert torch.equal(a, mis)
     # values whose count is 0: p stays at max; counts above max clamp p to 0
     e = torch.tensor([maxv, -1.0e6], dtype=torch.float32, device=cuda)
     N.check(N.lib().vcbct_gaussian_noise(C.c_void_p(e.data_ptr()), 2, maxv, 1, 1, None))

@@ -26,17 +26,28 @@ __device__ __forceinline__ float ref_unit_noise(float p, float maxv, float z)
     return v;
 }
 
-// One thread per four pixels (one counter draw, four normals).
+// One thread per four pixels (one counter draw, four normals); VEC when
+// the stack is 16-byte aligned.
+template <bool VEC>
 __global__ void gaussian_noise_kernel(float* __restrict__ p, size_t n, float maxv, unsigned long long seed)
 {
     const size_t nq = (n + 3) / 4;
     for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += (size_t)gridDim.x * blockDim.x) {
         const float4 z = normal_quad(q, 1u, seed);
-        const float zz[4] = {z.x, z.y, z.z, z.w};
         const size_t i = 4 * q;
+        if (VEC && i + 4 <= n) {  // one 16-byte load and store per quad
+            float4 v = *reinterpret_cast<const float4*>(p + i);
+            v.x = ref_unit_noise(v.x, maxv, z.x);
+            v.y = ref_unit_noise(v.y, maxv, z.y);
+            v.z = ref_unit_noise(v.z, maxv, z.z);
+            v.w = ref_unit_noise(v.w, maxv, z.w);
+            *reinterpret_cast<float4*>(p + i) = v;
+        } else {
+            const float zz[4] = {z.x, z.y, z.z, z.w};
 #pragma unroll
-        for (int k = 0; k < 4; k++)
-            if (i + k < n) p[i + k] = ref_unit_noise(p[i + k], maxv, zz[k]);
+            for (int k = 0; k < 4; k++)
+                if (i + k < n) p[i + k] = ref_unit_noise(p[i + k], maxv, zz[k]);
+        }
     }
 }
 
@@ -52,7 +63,10 @@ cudaError_t launch_gaussian_noise(float* proj, size_t n, double max_pixvalue, un
     if (e != cudaSuccess) return e;
     const size_t want = ((n + 3) / 4 + 255) / 256;
     const unsigned blocks = (unsigned)(want < (size_t)sms * 16 ? want : (size_t)sms * 16);
-    gaussian_noise_kernel<<<blocks, 256, 0, st>>>(proj, n, (float)max_pixvalue, seed);
+    if ((reinterpret_cast<uintptr_t>(proj) & 15) == 0)
+        gaussian_noise_kernel<true><<<blocks, 256, 0, st>>>(proj, n, (float)max_pixvalue, seed);
+    else
+        gaussian_noise_kernel<false><<<blocks, 256, 0, st>>>(proj, n, (float)max_pixvalue, seed);
     return cudaGetLastError();
 }
 
