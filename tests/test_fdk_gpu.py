@@ -74,16 +74,24 @@ def test_fdk_chain_short_volume_within_one_lsb(cuda):
 
 
 @pytest.mark.parametrize("V,H,W,xshift", [(6, 40, 48, 0.0), (4, 8, 400, 0.0), (3, 100, 400, 16.0),
-                                          (2, 70, 256, 2.0)])
+                                          (2, 70, 256, 2.0), (3, 10, 50, 0.0),
+                                          # wider than one 512-column accumulator: column tiles
+                                          (2, 12, 600, 0.0), (2, 9, 800, 8.0), (2, 5, 1030, 0.0)])
 def test_bf16x3_tensor_core_filter_matches_fp64(cuda, V, H, W, xshift):
     """The tcgen05 BF16 3-term split GEMM against the FP64 filter; the same
-    tolerance as the direct FP32 path (1e-5 of the output scale)."""
+    tolerance as the direct FP32 path (1e-5 of the output scale) up to 800
+    columns (the widest detector of the workloads).  The tensor cores' FP32
+    accumulation error grows with the number of K steps; at 1030 columns it
+    reaches about 1.1e-5 of the scale, so that width is held to 3e-5 (it
+    checks the three column tiles)."""
     from virtualcbct_b200 import FILTER_BF16X3
+    tol = 1e-5 if W <= 800 else 3e-5
     g, proj, ang, xs = _case(V=V, H=H, W=W, seed=W + V, xshift=xshift)
     f = Fdk(g, ang, xs, np.zeros(g.V))
     gpu = f.filter(proj, method=FILTER_BF16X3)
     d64 = O.filter_sinogram(proj, xs, np.zeros(g.V), O.fdk_consts(g.piso), mode=1)
     assert np.isfinite(gpu).all()
-    assert np.abs(gpu - d64).max() <= 1e-5 * np.abs(d64).max()
+    assert np.abs(gpu - d64).max() <= tol * np.abs(d64).max()
     direct = f.filter(proj, method=FILTER_DIRECT_F32)
-    assert np.abs(gpu - direct).max() <= 1e-5 * np.abs(d64).max()
+    assert np.abs(direct - d64).max() <= 1e-5 * np.abs(d64).max()
+    assert np.abs(gpu - direct).max() <= tol * np.abs(d64).max()

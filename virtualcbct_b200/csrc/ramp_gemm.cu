@@ -9,9 +9,10 @@
 // with i + j <= 2 (G0B0 G0B1 G1B0 G0B2 G1B1 G2B0) are accumulated in FP32 in
 // tensor memory, which keeps about 24 significant bits.
 //
-// One CTA computes a 128-row x W-column output tile (W <= 512): warp 0 issues
+// One CTA computes a 128-row x NT-column output tile (NT <= 512; wider
+// detectors take several column tiles): warp 0 issues
 // TMA loads into a 3-stage shared-memory ring (128B swizzle, K-major), warp 1
-// issues tcgen05.mma from a single thread into a 128 x Np FP32 accumulator in
+// issues tcgen05.mma from a single thread into a 128 x NT FP32 accumulator in
 // tensor memory, warps 2-5 read the accumulator back (tcgen05.ld), apply the
 // cosine factor and store.  No cluster multicast is used.  Every mbarrier
 // wait is bounded; on timeout the kernel raises a device flag and returns.
@@ -120,24 +121,28 @@ __device__ __forceinline__ void umma_commit(uint64_t* bar)
                  : "memory");
 }
 
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v)
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v)
 {
-    uint32_t r[16];
+    uint32_t r[32];
     asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
         : "r"(taddr));
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-    for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
+    for (int i = 0; i < 32; i++) v[i] = __uint_as_float(r[i]);
 }
 
 struct GemmArgs {
     float* out;
     const FilterView* views;
     float pitch, sad;
-    int M, H, W, Np, Kp, ktiles, stages;
+    int M, H, W, NT, Kp, ktiles, stages;  // NT: output columns per CTA (blockIdx.y selects the column tile)
+    int vec;                              // rows of `out` 16-byte aligned (W % 4 == 0, aligned base)
     int* err;
 };
 
@@ -149,7 +154,7 @@ ramp_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant_
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     const int S = g.stages;
     const uint32_t a_bytes = BM * BK * 2;
-    const uint32_t b_bytes = (uint32_t)g.Np * BK * 2;
+    const uint32_t b_bytes = (uint32_t)g.NT * BK * 2;
     uint8_t* stage_base = smem;
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem + (size_t)S * (a_bytes + b_bytes));
     uint64_t* full = bars;
@@ -159,8 +164,9 @@ ramp_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant_
 
     const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
     const int m0 = blockIdx.x * BM;
-    const int N1 = g.Np < 256 ? g.Np : 256;
-    const int N2 = g.Np - N1;
+    const int n0 = blockIdx.y * g.NT;
+    const int N1 = g.NT < 256 ? g.NT : 256;
+    const int N2 = g.NT - N1;
     const int nk = 6 * g.ktiles;
 
     if (threadIdx.x == 0) {
@@ -191,8 +197,8 @@ ramp_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant_
             uint8_t* sb = sa + a_bytes;
             mbar_expect_tx(&full[s], a_bytes + b_bytes);
             tma_load_3d(sa, &tmA, &full[s], kt * BK, m0, c_terms[term][0]);
-            tma_load_3d(sb, &tmB, &full[s], kt * BK, 0, c_terms[term][1]);
-            tma_load_3d(sb + (size_t)(g.Np / 2) * BK * 2, &tmB, &full[s], kt * BK, g.Np / 2, c_terms[term][1]);
+            tma_load_3d(sb, &tmB, &full[s], kt * BK, n0, c_terms[term][1]);
+            tma_load_3d(sb + (size_t)(g.NT / 2) * BK * 2, &tmB, &full[s], kt * BK, n0 + g.NT / 2, c_terms[term][1]);
         }
     } else if (warp == 1 && lane == 0) {
         // MMA issuer
@@ -231,19 +237,31 @@ ramp_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant_
                 pos2 = fabsf(fv.ycs + (float)n) * g.pitch;
                 xcs = fv.xcs;
             }
-            const float sad2 = g.sad * g.sad;
-            for (int c = 0; c < g.Np; c += 16) {
-                float v16[16];
-                tmem_ld16(taddr + ((uint32_t)(32 * q) << 16) + (uint32_t)c, v16);
-                if (row < g.M) {
-                    float* o = g.out + (size_t)row * g.W;
+            // cosine factor sad / sqrt(sad^2 + pos1^2 + pos2^2) from the
+            // reciprocal square root (2 ulp), stored 16 bytes at a time
+            const float sad = g.sad, base2 = fmaf(pos2, pos2, sad * sad);
+            for (int c = 0; c < g.NT; c += 32) {
+                float v32[32];
+                tmem_ld32(taddr + ((uint32_t)(32 * q) << 16) + (uint32_t)c, v32);
+                const int mb = n0 + c;
+                if (row < g.M && mb < g.W) {
+                    float* o = g.out + (size_t)row * g.W + mb;
 #pragma unroll
-                    for (int i = 0; i < 16; i++) {
-                        const int m = c + i;
-                        if (m < g.W) {
-                            const float pos1 = fabsf(xcs + (float)m) * g.pitch;
-                            o[m] = v16[i] * (g.sad / sqrtf(sad2 + pos1 * pos1 + pos2 * pos2));
-                        }
+                    for (int i = 0; i < 32; i++) {
+                        const float pos1 = fabsf(xcs + (float)(mb + i)) * g.pitch;
+                        v32[i] *= sad * rsqrtf(fmaf(pos1, pos1, base2));
+                    }
+                    // columns of this tile only (the last 32-column chunk may
+                    // run past NT into unwritten accumulator columns)
+                    const int lim = min(g.W - mb, g.NT - c);
+                    if (g.vec && lim >= 32) {
+#pragma unroll
+                        for (int i = 0; i < 32; i += 4)
+                            *reinterpret_cast<float4*>(o + i) = make_float4(v32[i], v32[i + 1], v32[i + 2], v32[i + 3]);
+                    } else {
+#pragma unroll
+                        for (int i = 0; i < 32; i++)
+                            if (i < lim) o[i] = v32[i];
                     }
                 }
             }
@@ -341,8 +359,11 @@ bool make_map(CUtensorMap* map, void* base, int rows, int Kp, int box_rows)
               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// Output columns are split into ntiles tiles of NT <= 512 columns (one
+// tensor-memory accumulator of 128 x NT FP32 each); B is padded to
+// Np = ntiles * NT rows.
 struct Layout {
-    int M, Np, Kp, stages;
+    int M, Np, NT, ntiles, Kp, stages;
     size_t a_off, b_off, err_off, total, smem;
 };
 
@@ -350,9 +371,12 @@ Layout layout_for(int V, int H, int W)
 {
     Layout L{};
     L.M = V * H;
-    L.Np = (W + 15) / 16 * 16;
+    const int n16 = (W + 15) / 16 * 16;
+    L.ntiles = (n16 + 511) / 512;
+    L.NT = ((n16 + L.ntiles - 1) / L.ntiles + 15) / 16 * 16;
+    L.Np = L.ntiles * L.NT;
     L.Kp = (W + BK - 1) / BK * BK;
-    const size_t stage = (size_t)BM * BK * 2 + (size_t)L.Np * BK * 2;
+    const size_t stage = (size_t)BM * BK * 2 + (size_t)L.NT * BK * 2;
     L.stages = (int)((225 * 1024 - 1024 - 128) / stage);
     if (L.stages > 3) L.stages = 3;
     L.smem = 1024 + (size_t)L.stages * stage + 8 * (2 * L.stages + 1) + 16;
@@ -371,7 +395,7 @@ cudaError_t launch_ramp_gemm_bf16x3(const float* proj, float* out, const float* 
                                     const float* wts, float pitch, float sad, int V, int H, int W, void* workspace,
                                     cudaStream_t st)
 {
-    if (W < 16 || W > 512) return cudaErrorInvalidValue;
+    if (W < 16 || W > 4096) return cudaErrorInvalidValue;
     const Layout L = layout_for(V, H, W);
     if (L.stages < 2) return cudaErrorInvalidValue;
     uint8_t* ws = static_cast<uint8_t*>(workspace);
@@ -388,12 +412,13 @@ cudaError_t launch_ramp_gemm_bf16x3(const float* proj, float* out, const float* 
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
     CUtensorMap tmA, tmB;
-    if (!make_map(&tmA, ap, L.M, L.Kp, BM) || !make_map(&tmB, bp, L.Np, L.Kp, L.Np / 2))
+    if (!make_map(&tmA, ap, L.M, L.Kp, BM) || !make_map(&tmB, bp, L.Np, L.Kp, L.NT / 2))
         return cudaErrorInvalidValue;
-    GemmArgs g{out, views, pitch, sad, L.M, H, W, L.Np, L.Kp, L.Kp / BK, L.stages, err};
+    const int vec = (W % 4 == 0 && (reinterpret_cast<uintptr_t>(out) & 15) == 0) ? 1 : 0;
+    GemmArgs g{out, views, pitch, sad, L.M, H, W, L.NT, L.Kp, L.Kp / BK, L.stages, vec, err};
     e = cudaFuncSetAttribute(ramp_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem);
     if (e != cudaSuccess) return e;
-    ramp_gemm_kernel<<<(L.M + BM - 1) / BM, kThreads, L.smem, st>>>(tmA, tmB, g);
+    ramp_gemm_kernel<<<dim3((L.M + BM - 1) / BM, L.ntiles), kThreads, L.smem, st>>>(tmA, tmB, g);
     return cudaGetLastError();
 }
 
