@@ -110,6 +110,35 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+def bp_update_counts(fg, ang, xs):
+    """Voxel-view updates of a backprojection: all (N^2 Z V, the unit of
+    GUPS), inside the circular mask, and effective (inside the mask with the
+    projected detector column and row on the detector; the others are
+    skipped).  The kernel's geometry restated in float64 (edge cases at the
+    detector border may count one either way)."""
+    N, Z, V, W, H = fg.N, fg.Z, fg.V, fg.W, fg.H
+    R = (N - 1) / 2.0
+    y, x = np.mgrid[0:N, 0:N].astype(np.float64)
+    m = (y - R) ** 2 + (x - R) ** 2 <= R * R
+    cp = N / 2.0 - 0.5
+    xx = ((x - cp) * fg.scale)[m]
+    yy = (-(y - cp) * fg.scale)[m]
+    pitch = fg.piso * fg.mpn / W
+    px = fg.pdet * fg.mpn / W
+    eff = 0
+    for th in range(V):
+        cs, sn = np.cos(ang[th]), np.sin(ang[th])
+        L2 = 1.0 - (-xx * sn + yy * cs) / fg.sad
+        g = 1.0 / (L2 * pitch)
+        uu = np.floor((W // 2) + xs[th] / px - 0.5 + (xx * cs + yy * sn) * g)
+        ok = (uu >= 0) & (uu <= W - 1)
+        gz = g[ok]
+        lo = np.ceil((-(H // 2) / gz - fg.zstart) / fg.step)
+        hi = np.ceil(((H - H // 2) / gz - fg.zstart) / fg.step)
+        eff += int(np.clip(np.minimum(hi, Z) - np.maximum(lo, 0), 0, None).sum())
+    return N * N * Z * V, int(m.sum()) * Z * V, eff
+
+
 def measured_peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -235,6 +264,71 @@ def decomposition_section(stream):
     return {"workload": "6 x FP32 256x256x64 (1x1x2 mm), 90 views, 200x200 (2 mm), 91 bins",
             "forward_ms": fwd, "step_ms": step, "step_over_forward": step / fwd,
             "loss": float(loss.item())}
+
+
+def decomposition_fullscale_section(stream):
+    """Config 5 at full size, one of its four phantoms: six FP32 element
+    volumes 512x512x400 (0.5x0.5x1 mm), 720 views of 800x800 (0.5 mm), 111-bin
+    120 kV spectrum; one decomposition step (the per-ray path integrals, 11 GB,
+    kept from the forward launch) and one with them re-marched, vs a plain
+    forward; FDK (BF16x3 filter in two column tiles + backprojection) of the
+    projections to 512x512x400."""
+    import torch
+    from virtualcbct_b200 import (FILTER_BF16X3, Fdk, FdkGeometry, Projector, ProjGeometry, attenuation_table,
+                                  phantoms, trig_tables)
+    from virtualcbct_b200.autograd import decomposition_step
+    g = ProjGeometry(N=512, Z=400, s=0.05, step=0.1, W=800, H=800, V=720)
+    ang = np.deg2rad(phantoms.view_angles(g.V))
+    tabs = trig_tables(g.W, g.H, ang, np.zeros(g.V), np.zeros(g.V), g.pdet, g.dpn)
+    mu, pdf = attenuation_table(os.path.join(DATA, "spectrum_kramers120_111.csv"), MINIDB, 6)
+    vol = phantoms.ellipsoid_phantom_torch(g.N, g.Z, g.s, g.step, seed=40, as_float=True)
+    p = Projector(g, *tabs)
+    p.set_spectrum(mu, pdf, 1000.0)
+    vol[:, 4:6] *= 1.1
+    p.load_volume_f32(vol)
+    target = p.forward().clone()
+    vol[:, 4:6] /= 1.1
+    p.load_volume_f32(vol)
+    nseg = p.count_segments()
+    out = torch.empty_like(target)
+    p.forward(out)
+    decomposition_step(vol, target, p)
+    torch.cuda.synchronize()
+    e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    e[0].record(stream)
+    p.load_volume_f32(vol)
+    p.forward(out)
+    e[1].record(stream)
+    loss, _ = decomposition_step(vol, target, p)
+    e[2].record(stream)
+    torch.cuda.synchronize()
+    fwd, step = e[0].elapsed_time(e[1]), e[1].elapsed_time(e[2])
+    r = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    r[0].record(stream)
+    decomposition_step(vol, target, p, keep_limit=0)
+    r[1].record(stream)
+    torch.cuda.synchronize()
+    step_rm = r[0].elapsed_time(r[1])
+    fg = FdkGeometry(W=800, H=800, V=720, N=512, Z=400, zstart=-20, step=0.1, scale=0.05)
+    F = Fdk(fg, ang, np.zeros(fg.V), np.zeros(fg.V))
+    filt = F.filter(out, method=FILTER_BF16X3)
+    F.backproject(filt)
+    torch.cuda.synchronize()
+    f = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    f[0].record(stream)
+    F.filter(out, filt, method=FILTER_BF16X3)
+    f[1].record(stream)
+    F.backproject(filt)
+    f[2].record(stream)
+    torch.cuda.synchronize()
+    bp = f[1].elapsed_time(f[2])
+    return {"workload": "6 x FP32 512x512x400 (0.5x0.5x1 mm), 720 views, 800x800 (0.5 mm), 111 bins",
+            "segments": nseg, "forward_ms": fwd, "forward_gseg_s": nseg / (fwd * 1e-3) / 1e9,
+            "step_ms": step, "step_over_forward": step / fwd, "loss": float(loss.item()),
+            "step_remarched_ms": step_rm, "step_remarched_over_forward": step_rm / fwd,
+            "twenty_iterations_four_phantoms_s": 80 * step * 1e-3,
+            "fdk_filter_ms": f[0].elapsed_time(f[1]), "fdk_bp_ms": bp,
+            "fdk_bp_gups": fg.N * fg.N * fg.Z * fg.V / (bp * 1e-3) / 1e9}
 
 
 def batched_section(stream, args):
@@ -681,6 +775,7 @@ def run_ours(args, rank, world, local_rank):
     ms_filter = a1.elapsed_time(a2) / args.steps
     ms_bp = a2.elapsed_time(a3) / args.steps
     gups = fg.N * fg.N * fg.Z * fg.V / (ms_bp * 1e-3) / 1e9
+    n_all, n_mask, n_eff = bp_update_counts(fg, ang, w["xs_fdk"])
     # BF16x3 work: 6 split products of a (V*H) x Kp x Np GEMM
     Kp = (fg.W + 63) // 64 * 64
     Np = (fg.W + 15) // 16 * 16
@@ -690,6 +785,7 @@ def run_ours(args, rank, world, local_rank):
     extra = {}
     if not args.no_extras:
         extra["decomposition"] = decomposition_section(stream)
+        extra["decomposition_fullscale"] = decomposition_fullscale_section(stream)
         extra["batched"] = batched_section(stream, args)
         extra["batched_small"] = batched_small_section(stream)
         extra["iterative"] = iterative_section(stream)
@@ -729,6 +825,9 @@ def run_ours(args, rank, world, local_rank):
         "fdk": {"filter_ms": ms_filter, "filter_method": "bf16x3_tcgen05", "filter_tflops": gemm_tflops,
                 "filter_ms_direct_f32": ms_filter_direct, "bf16x3_vs_direct_max_rel": filt_err,
                 "bp_ms": ms_bp, "bp_gups": gups,
+                "bp_gups_in_mask": n_mask / (ms_bp * 1e-3) / 1e9,
+                "bp_gups_effective": n_eff / (ms_bp * 1e-3) / 1e9,
+                "bp_updates": {"all": n_all, "in_mask": n_mask, "effective": n_eff},
                 "short_volume_range": [int(vi.min().item()), int(vi.max().item())]},
         "clocks": clk,
         "gather_roof": gather_roof,

@@ -2,9 +2,11 @@
 volumes 512x512x400 (0.5 x 0.5 x 1 mm) of a synthetic ellipsoid phantom, 720
 views of an 800x800 detector (0.5 mm), a 111-bin 120 kV spectrum; gradient
 steps of least-squares material decomposition against projections of the
-phantom with bone Ca and P scaled by 1.1 (per-ray path integrals do not fit
-the 4 GiB keep limit, so the backward pass recomputes them); then FDK of the
-final projections to 512x512x400 short.
+phantom with bone Ca and P scaled by 1.1 (the backward pass reads the
+per-ray path integrals kept from the forward launch, 11 GB, and recomputes
+each ray's spectral state from them; the re-marching form, for when they do
+not fit, gives the same gradient); then FDK of the final projections to
+512x512x400 short.
 
 At this size the FP64 oracle covers samples: 1024 rays of two views for the
 projection, two whole views for the ramp filter, two slices for the
@@ -69,6 +71,9 @@ def test_fullscale_decomposition_and_fdk(cuda):
     # gradient: central difference of the loss along d against <grad, d>
     loss0, grad = decomposition_step(vol, target, p)
     assert abs(float(loss0) - _loss(pred, target)) <= 1e-4 * _loss(pred, target)
+    _, grad_rm = decomposition_step(vol, target, p, keep_limit=0)   # path integrals re-marched
+    assert float((grad_rm - grad).norm()) <= 1e-5 * float(grad.norm())
+    del grad_rm
     rng = np.random.default_rng(7)
     k = 4096
     zi = torch.from_numpy(rng.integers(150, 250, k)).to(cuda)

@@ -114,13 +114,27 @@ __global__ void __launch_bounds__(256, VCBCT_BP_MIN_BLOCKS) backproject_kernel(
     float acc[ZB];
 #pragma unroll
     for (int i = 0; i < ZB; i++) acc[i] = 0.0f;
-    if (inmask) {
+    const double pitch = f.piso * f.mpn / f.W;
+    const double zz0 = f.zstart + z0 * f.step;
+    const int W = f.W, H = f.H;
+    // Slices of this block that no column of the mask sees in any view (the
+    // cone's height is exceeded: |Y| <= rm over the mask, so the detector
+    // row coordinate H/2 + z g lies between the bounds of g below) are left
+    // at zero without looping over the views; block-uniform.
+    bool seen = true;
+    {
+        const double rm = (f.N * 0.5 + 1.0) * f.scale;
+        const double gmin = 1.0 / ((1.0 + rm / f.sad) * pitch), gmax = 1.0 / ((1.0 - rm / f.sad) * pitch);
+        const double zzb = zz0 + (double)(min(ZB, f.Z - z0) - 1) * f.step;
+        const double a = zz0 * gmin, b = zz0 * gmax, c = zzb * gmin, d = zzb * gmax;
+        const double lo = (double)(H / 2) + fmin(fmin(a, b), fmin(c, d));
+        const double hi = (double)(H / 2) + fmax(fmax(a, b), fmax(c, d));
+        if (rm < f.sad && (hi < -1.0 || lo > (double)H + 1.0)) seen = false;
+    }
+    if (inmask && seen) {
         const double cp = (double)f.N / 2.0 - 0.5;
         const double xx = (x - cp) * f.scale;
         const double yy = -(y - cp) * f.scale;
-        const double pitch = f.piso * f.mpn / f.W;
-        const double zz0 = f.zstart + z0 * f.step;
-        const int W = f.W, H = f.H;
         for (int th = 0; th < f.V; th++) {
             const BpView bv = views[th];
             const double cs = bv.cs, sn = bv.sn;
@@ -134,13 +148,15 @@ __global__ void __launch_bounds__(256, VCBCT_BP_MIN_BLOCKS) backproject_kernel(
             const float wu = (float)(U - Uf);
             const double UUU = bv.ushift + U;
             const int UU = (int)floor(UUU);
+            if (UU < 0 || UU > W - 1) continue;
             const double zeta0 = (double)(H / 2) + zz0 * g;
+            // every slice of the block projects above or below the detector
+            if (zeta0 + (double)(ZB - 1) * f.step * g < -1.0 || zeta0 > (double)H + 1.0) continue;
             const double zf = floor(zeta0);
             const int Zi = (int)zf;
             const float Zf = (float)(zeta0 - zf);
             const float dz = (float)(f.step * g);
             const float w2 = (float)(1.0 / L2 / L2) * bv.dbeta * (float)f.xfactor;
-            if (UU < 0 || UU > W - 1) continue;
             const bool lastc = (UU == W - 1);
             const float cw0 = lastc ? 1.0f : 1.0f - wu;
             const float cw1 = lastc ? 0.0f : wu;
