@@ -135,13 +135,14 @@ __global__ void __launch_bounds__(256, VCBCT_BP_MIN_BLOCKS) backproject_kernel(
         const double cp = (double)f.N / 2.0 - 0.5;
         const double xx = (x - cp) * f.scale;
         const double yy = -(y - cp) * f.scale;
+        const double inv_sad = 1.0 / f.sad;
         for (int th = 0; th < f.V; th++) {
             const BpView bv = views[th];
             const double cs = bv.cs, sn = bv.sn;
             // FP64 detector coordinates of this column (:76-83)
             const double X = xx * cs + yy * sn;
             const double Y = -xx * sn + yy * cs;
-            const double L2 = 1.0 - Y / f.sad;
+            const double L2 = 1.0 - Y * inv_sad;
             const double g = 1.0 / (L2 * pitch);
             const double U = X * g;
             const double Uf = floor(U);
@@ -156,7 +157,8 @@ __global__ void __launch_bounds__(256, VCBCT_BP_MIN_BLOCKS) backproject_kernel(
             const int Zi = (int)zf;
             const float Zf = (float)(zeta0 - zf);
             const float dz = (float)(f.step * g);
-            const float w2 = (float)(1.0 / L2 / L2) * bv.dbeta * (float)f.xfactor;
+            const float iL = (float)(g * pitch);  // 1 / L2
+            const float w2 = iL * iL * bv.dbeta * (float)f.xfactor;
             const bool lastc = (UU == W - 1);
             const float cw0 = lastc ? 1.0f : 1.0f - wu;
             const float cw1 = lastc ? 0.0f : wu;
