@@ -173,6 +173,31 @@ def segments_per_view_cpu(w, views):
     return {int(v): int(r["nm"][v].sum()) for v in views}
 
 
+def rank_barrier(world):
+    """All ranks meet (a no-op for one process)."""
+    if world > 1:
+        import torch
+        torch.distributed.barrier()
+
+
+def max_over_ranks_on(x, world, device):
+    """The largest of every rank's x (each rank's timing); `device` is where
+    the process group's backend reduces (a CUDA device for NCCL, "cpu" for
+    gloo)."""
+    if world > 1:
+        import torch
+        t = torch.tensor([x], dtype=torch.float64, device=device)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return float(t.item())
+    return x
+
+
+def job_rate(units_per_rank, world, ms_max):
+    """Whole-job throughput of N replicas: every rank's units over the
+    slowest rank's time (in G units per second)."""
+    return units_per_rank * world / (ms_max * 1e-3) / 1e9
+
+
 def run_reference(args, rank, world):
     """Reference arm: the reference's CPU projector (reprojection.cpp compiled
     from its sources, driven per view and bin over all host threads) on a
@@ -689,15 +714,10 @@ def run_ours(args, rank, world, local_rank):
     stream = torch.cuda.current_stream()
 
     def barrier():
-        if world > 1:
-            torch.distributed.barrier()
+        rank_barrier(world)
 
     def max_over_ranks(x):
-        if world > 1:
-            t = torch.tensor([x], dtype=torch.float64, device=dev)
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            return float(t.item())
-        return x
+        return max_over_ranks_on(x, world, dev)
 
     # ---- device-resident step
     for _ in range(max(3, args.warmup)):
@@ -716,7 +736,7 @@ def run_ours(args, rank, world, local_rank):
     clk = clocks.stop()
     barrier()
     ms = max_over_ranks(e0.elapsed_time(e1) / args.steps)
-    value = nseg * world / (ms * 1e-3) / 1e9
+    value = job_rate(nseg, world, ms)
 
     # ---- end-to-end through the C ABI with pinned host buffers
     out_h = torch.empty((g.V, g.H, g.W), dtype=torch.float32).pin_memory()
@@ -743,7 +763,7 @@ def run_ours(args, rank, world, local_rank):
     t1.record(stream)
     torch.cuda.synchronize()
     ms_e2e = max_over_ranks(t0.elapsed_time(t1) / args.steps)
-    e2e = nseg * world / (ms_e2e * 1e-3) / 1e9
+    e2e = job_rate(nseg, world, ms_e2e)
     P.load_volume(vol_d)
 
     # ---- FDK on the projections just made (device resident)

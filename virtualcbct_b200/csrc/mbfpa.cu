@@ -519,9 +519,6 @@ struct AccumF32 : PairSums<M> {
     }
 };
 
-// Scatter of one segment's gradient into the packed float records: one
-// 16-byte vector reduction for elements 0-3 and one 8-byte (M = 6) or
-// 16-byte (M = 8) reduction for the rest.
 // Scatter of one segment's gradient into element planes: plane k holds
 // element k of every voxel at the packed record index (y*N + x)*Z + z, so
 // the 32 lanes of a warp -- adjacent detector rows, adjacent z cells of one
