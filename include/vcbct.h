@@ -121,8 +121,10 @@ int vcbct_projector_project(vcbct_projector* p, const uint16_t* volume, float* o
  * intensity I into n' / i0 with n = i0 * I and n' = n + sqrt(n) z (z standard
  * normal from a counter-based generator keyed by `seed` and the pixel's
  * index, so reproducible and independent of launch shape), clamped to
- * [0, max_counts]; kind 0 turns it off (default).  Applied in the forward
- * kernel's epilogue. */
+ * [0, max_counts]; kind 2 draws n' from Poisson(n) instead (exact counting
+ * statistics for low counts: multiplication of uniforms below n = 10, the
+ * transformed rejection method PTRS above; no reference counterpart); kind 0
+ * turns it off (default).  Applied in the forward kernel's epilogue. */
 int vcbct_projector_set_noise(vcbct_projector* p, int kind, double i0, double max_counts,
                               unsigned long long seed);
 /* The counter-based generator of the noise options: Philox-4x32-10 (Salmon

@@ -75,3 +75,37 @@ def test_reference_unit_gaussian_noise(cuda):
     e = torch.tensor([maxv, -1.0e6], dtype=torch.float32, device=cuda)
     N.check(N.lib().vcbct_gaussian_noise(C.c_void_p(e.data_ptr()), 2, maxv, 1, 1, None))
     assert e[0].item() == maxv and e[1].item() == 0.0
+
+
+@pytest.mark.parametrize("i0", [4.0, 3.0e4])
+def test_forward_poisson_counts(cuda, i0):
+    """Poisson counts in the epilogue: integer counts, reproducible, mean and
+    variance n; at low counts (the multiplication sampler) the numbers of
+    zero and one counts match sum exp(-n) and sum n exp(-n); at high counts
+    (the PTRS sampler) the skewness matches 1 / sqrt(n)."""
+    import torch
+    g, p = _projector(cuda)
+    clean = p.forward().double()
+    p.set_noise(i0, max_counts=1.0e12, seed=5, model="poisson")
+    a = p.forward().double()
+    assert torch.equal(a, p.forward().double())
+    n = (i0 * clean).flatten()
+    m = (i0 * a).flatten()
+    assert float((m - m.round()).abs().max()) <= 1e-6 * float(m.max()) + 1e-4   # whole counts
+    m = m.round()
+    keep = n > 0.05
+    n, m = n[keep], m[keep]
+    k = n.numel()
+    z = (m - n) / n.sqrt()
+    assert abs(z.mean().item()) < 5.0 / k ** 0.5 and abs(z.std().item() - 1.0) < 0.03
+    if i0 < 10:
+        for c, pc in ((0, torch.exp(-n)), (1, n * torch.exp(-n))):
+            got = float((m == c).sum())
+            want = float(pc.sum())
+            sd = float((pc * (1 - pc)).sum()) ** 0.5
+            assert abs(got - want) < 5 * sd + 1, (c, got, want, sd)
+    else:
+        skew = ((m - n) ** 3 / n ** 1.5).mean().item()          # E = 1 / sqrt(n) per pixel
+        assert abs(skew - (1.0 / n.sqrt()).mean().item()) < 6.0 * (15.0 / k) ** 0.5
+    p.set_noise(0.0)
+    assert torch.equal(p.forward().double(), clean)

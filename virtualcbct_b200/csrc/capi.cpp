@@ -353,8 +353,9 @@ extern "C" int vcbct_projector_set_noise(vcbct_projector* p, int kind, double i0
                                          unsigned long long seed)
 {
     if (!p) return fail(VCBCT_ERR_ARG, "NULL projector");
-    if (kind != 0 && kind != 1) return fail(VCBCT_ERR_ARG, "noise kind must be 0 (none) or 1 (Gaussian counts)");
-    if (kind == 1 && (!(i0 > 0.0) || !(max_counts > 0.0)))
+    if (kind < 0 || kind > 2)
+        return fail(VCBCT_ERR_ARG, "noise kind must be 0 (none), 1 (Gaussian counts) or 2 (Poisson counts)");
+    if (kind != 0 && (!(i0 > 0.0) || !(max_counts > 0.0)))
         return fail(VCBCT_ERR_ARG, "i0 and max_counts must be positive");
     p->noise_kind = kind;
     p->noise_i0 = i0;

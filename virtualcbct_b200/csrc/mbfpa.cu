@@ -942,9 +942,10 @@ __device__ __forceinline__ void forward_tile(const ForwardArgs& a, const float4*
     }
     if (a.out) {
         float I = spectral_sum<M>(s_mu, s_pdf, a.spec.NE, L) * R.leng;
-        if (a.noise_kind == 1) {
+        if (a.noise_kind != 0) {
             const uint64_t gidx = ((uint64_t)(v + a.view_offset) * P.H + (P.H - 1 - j)) * P.W + jj;
-            I = noisy_intensity(I, a.noise_i0, a.noise_max, gidx, a.noise_seed);
+            I = (a.noise_kind == 1) ? noisy_intensity(I, a.noise_i0, a.noise_max, gidx, a.noise_seed)
+                                    : poisson_intensity(I, a.noise_i0, a.noise_max, gidx, a.noise_seed);
         }
         a.out[o] = I;
     }

@@ -99,4 +99,67 @@ __device__ __forceinline__ float noisy_intensity(float I, float i0, float max_co
     return m / i0;
 }
 
+// Counter draw for the Poisson sampler: word 3 of the counter numbers the
+// draws a pixel consumes.
+__device__ __forceinline__ void philox4x32_nth(uint64_t ctr, uint32_t stream_id, uint32_t nth, uint64_t seed,
+                                               uint32_t (&out)[4])
+{
+    uint32_t c[4] = {(uint32_t)ctr, (uint32_t)(ctr >> 32), stream_id, nth};
+    philox4x32_10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
+    out[0] = c[0];
+    out[1] = c[1];
+    out[2] = c[2];
+    out[3] = c[3];
+}
+
+__device__ __forceinline__ double unit_open(uint32_t w)  // (0, 1)
+{
+    return ((double)w + 0.5) * 2.3283064365386963e-10;
+}
+
+// A Poisson(lam) count for pixel `index`.  lam < 10: multiplication of
+// uniforms until the product falls below exp(-lam) (Knuth); lam >= 10: the
+// transformed rejection method PTRS (W. Hormann, "The transformed rejection
+// method for generating Poisson random variables", Insurance: Mathematics
+// and Economics 12, 1993), two trials per counter draw.  Both loops are
+// bounded (128 uniforms; 64 trials, acceptance ~0.9 each); past the bound,
+// which no realistic draw reaches, the normal approximation is returned.
+__device__ __forceinline__ double poisson_count(double lam, uint64_t index, uint64_t seed)
+{
+    if (!(lam > 0.0)) return 0.0;
+    uint32_t w[4];
+    if (lam < 10.0) {
+        const double lim = exp(-lam);
+        double prod = 1.0;
+        for (int n = 0; n < 128; n++) {
+            if ((n & 3) == 0) philox4x32_nth(index, 2u, (uint32_t)(n >> 2), seed, w);
+            prod *= unit_open(w[n & 3]);
+            if (prod <= lim) return (double)n;
+        }
+    } else {
+        const double sl = sqrt(lam), ll = log(lam);
+        const double b = 0.931 + 2.53 * sl, a = -0.059 + 0.02483 * b;
+        const double log_inv_alpha = log(1.1239 + 1.1328 / (b - 3.4)), vr = 0.9277 - 3.6224 / (b - 2.0);
+        for (int t = 0; t < 64; t++) {
+            if ((t & 1) == 0) philox4x32_nth(index, 2u, (uint32_t)(t >> 1), seed, w);
+            const double u = unit_open(w[2 * (t & 1)]) - 0.5, v = unit_open(w[2 * (t & 1) + 1]);
+            const double us = 0.5 - fabs(u);
+            const double k = floor((2.0 * a / us + b) * u + lam + 0.43);
+            if (us >= 0.07 && v <= vr) return k;
+            if (k < 0.0 || (us < 0.013 && v > us)) continue;
+            if (log(v) + log_inv_alpha - log(a / (us * us) + b) <= -lam + k * ll - lgamma(k + 1.0)) return k;
+        }
+    }
+    return fmax(0.0, rint(lam + sqrt(lam) * (double)normal_draw(index, 3u, seed)));
+}
+
+// Poisson detector counts of an intensity: n = i0 * I expected counts, a
+// Poisson(n) draw clamped to [0, max_counts]; returns it / i0.
+__device__ __forceinline__ float poisson_intensity(float I, double i0, double max_counts, uint64_t index,
+                                                   uint64_t seed)
+{
+    const double m = fmin(poisson_count(i0 * (double)I, index, seed), max_counts);
+    return (float)(m / i0);
+}
+
 }  // namespace vcbct

@@ -204,10 +204,13 @@ class Projector:
                                                       C.c_void_p(grad.data_ptr()), _stream_ptr(stream)))
         return grad
 
-    def set_noise(self, i0: float = 0.0, max_counts: float = 65535.0, seed: int = 0):
-        """Gaussian detector noise on the projections (i0 = counts of an
-        unattenuated ray; i0 = 0 turns it off)."""
-        kind = 1 if i0 > 0 else 0
+    def set_noise(self, i0: float = 0.0, max_counts: float = 65535.0, seed: int = 0, model: str = "gaussian"):
+        """Detector noise on the projections (i0 = counts of an unattenuated
+        ray; i0 = 0 turns it off): model "gaussian" (the reference's n +
+        sqrt(n) z) or "poisson" (exact Poisson counts)."""
+        if model not in ("gaussian", "poisson"):
+            raise ValueError("model must be 'gaussian' or 'poisson'")
+        kind = 0 if i0 <= 0 else (1 if model == "gaussian" else 2)
         N.check(N.lib().vcbct_projector_set_noise(self._h, kind, float(i0), float(max_counts), int(seed)))
 
     def lengthproj(self, proj, ite: int = 0, views=None, npf=None, stream=None):
