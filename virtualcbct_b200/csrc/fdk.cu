@@ -131,6 +131,7 @@ __global__ void __launch_bounds__(256, VCBCT_BP_MIN_BLOCKS) backproject_kernel(
         const double hi = (double)(H / 2) + fmax(fmax(a, b), fmax(c, d));
         if (rm < f.sad && (hi < -1.0 || lo > (double)H + 1.0)) seen = false;
     }
+    const bool full = z0 + ZB <= f.Z;  // every slice of the block exists
     if (inmask && seen) {
         const double cp = (double)f.N / 2.0 - 0.5;
         const double xx = (x - cp) * f.scale;
@@ -164,6 +165,48 @@ __global__ void __launch_bounds__(256, VCBCT_BP_MIN_BLOCKS) backproject_kernel(
             const float cw1 = lastc ? 0.0f : wu;
             const int UU1 = lastc ? UU : UU + 1;
             const float* pv = filt + (size_t)th * H * W;
+            if (!lastc && full && zeta0 >= 0.0 && zeta0 + (double)(ZB - 1) * f.step * g < (double)H - 2.5) {
+                // every slice of the block projects between detector rows 0
+                // and H - 2: no bounds or last-row tests
+                const float* pc = pv + UU;
+#pragma unroll
+                for (int i = 0; i < ZB; i++) {
+                    const float zfrac = fmaf((float)i, dz, Zf);
+                    const float tq = __fadd_rd(zfrac, 12582912.0f);
+                    const float fl = tq - 12582912.0f;
+                    const int NZ = Zi + (__float_as_int(tq) - 0x4B400000);
+                    const float wz = zfrac - fl;
+                    const float* r0p = pc + NZ * W;
+                    const float* r1p = r0p + W;
+                    const float s0 = fmaf(cw1, __ldg(r0p + 1), cw0 * __ldg(r0p));
+                    const float s1 = fmaf(cw1, __ldg(r1p + 1), cw0 * __ldg(r1p));
+                    acc[i] = fmaf(fmaf(wz, s1, (1.0f - wz) * s0), w2, acc[i]);
+                }
+                continue;
+            }
+            if (!lastc && full) {
+                // columns UU, UU + 1 of rows NZ, NZ1: one address per row and
+                // the second column at +4 bytes; all slices of the block exist
+                const float* pc = pv + UU;
+#pragma unroll
+                for (int i = 0; i < ZB; i++) {
+                    const float zfrac = fmaf((float)i, dz, Zf);
+                    const float tq = __fadd_rd(zfrac, 12582912.0f);
+                    const float fl = tq - 12582912.0f;
+                    const int NZ = Zi + (__float_as_int(tq) - 0x4B400000);
+                    const float wz = zfrac - fl;
+                    if ((unsigned)NZ > (unsigned)(H - 1)) continue;
+                    const bool lastr = (NZ == H - 1);
+                    const float rw0 = lastr ? 1.0f : 1.0f - wz;
+                    const float rw1 = lastr ? 0.0f : wz;
+                    const float* r0p = pc + NZ * W;
+                    const float* r1p = lastr ? r0p : r0p + W;
+                    const float s0 = fmaf(cw1, __ldg(r0p + 1), cw0 * __ldg(r0p));
+                    const float s1 = fmaf(cw1, __ldg(r1p + 1), cw0 * __ldg(r1p));
+                    acc[i] = fmaf(fmaf(rw1, s1, rw0 * s0), w2, acc[i]);
+                }
+                continue;
+            }
 #pragma unroll
             for (int i = 0; i < ZB; i++) {
                 const float zfrac = fmaf((float)i, dz, Zf);
