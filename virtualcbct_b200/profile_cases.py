@@ -19,6 +19,9 @@ seconds:
   adjoint_state_c4  the same with the forward's path integrals kept
   batch_small    four uneven ellipsoid phantoms (256x256, Z 32-96, V 45-180)
                  in one persistent launch
+  adjoint_state_wide  MBFPA adjoint with kept path integrals, six float
+                 volumes 512x512x128 (0.5x0.5x1 mm), 90 views of 800x800,
+                 111 bins (the full-scale workload's per-view shape)
   lengthproj_c1  sensitivity backprojection of 36 uint16 400x400 views to
                  512x512x100 (iterative reconstruction)
   ir_update_c1   MLEM/TV update of a 512x512x100 short volume
@@ -106,6 +109,16 @@ def run(case: str, repeats: int = 2) -> str:
         g = ProjGeometry(N=256, Z=64, s=0.1, step=0.2, W=200, H=200, V=90)
         p = _projector(g, phantoms.view_angles(90), spectrum="spectrum_kramers100_91.csv")
         vol = phantoms.ellipsoid_phantom_torch(g.N, g.Z, g.s, g.step, seed=21, as_float=True)
+        p.load_volume_f32(vol)
+        _, L = p.forward_state()
+        go = torch.ones((g.V, g.H, g.W), dtype=torch.float32, device="cuda")
+        out = torch.zeros_like(vol)
+        for _ in range(repeats):
+            p.adjoint_state(L, go, out)
+    elif case == "adjoint_state_wide":
+        g = ProjGeometry(N=512, Z=128, s=0.05, step=0.1, W=800, H=800, V=90)
+        p = _projector(g, phantoms.view_angles(90), spectrum="spectrum_kramers120_111.csv")
+        vol = phantoms.ellipsoid_phantom_torch(g.N, g.Z, g.s, g.step, seed=40, as_float=True)
         p.load_volume_f32(vol)
         _, L = p.forward_state()
         go = torch.ones((g.V, g.H, g.W), dtype=torch.float32, device="cuda")
