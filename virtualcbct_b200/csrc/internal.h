@@ -113,6 +113,7 @@ struct AdjointArgs {
     float* grad_planes;      // [nmat][N*N*Z] float accumulator, z fastest
     int* err_flag;
     int cols_per_block;
+    int y0, y1;              // scatter only into volume rows iy in [y0, y1) (y1 <= y0: all)
 };
 cudaError_t launch_adjoint(const AdjointArgs& a, cudaStream_t st);
 

@@ -530,8 +530,10 @@ struct Scatter {
     size_t plane;               // N*N*Z
     int nmat;
     float g[8];
+    unsigned lo, span;          // packed indices [lo, lo + span) of the strip scattered into
     __device__ __forceinline__ void operator()(int idx, float len)
     {
+        if ((unsigned)idx - lo >= span) return;
         float* p = grad + idx;
 #pragma unroll
         for (int k = 0; k < M; k++)
@@ -869,6 +871,46 @@ __device__ __forceinline__ void warp_range(const RayPlan& R, bool valid, int& Kl
     Khi = __reduce_max_sync(0xffffffffu, hi);
 }
 
+// Iterations [klo, khi] narrowed to those whose segments can lie in volume
+// rows iy in [y0, y1): the ray's y cell cy = floor(D or O) is linear in t
+// (iy = nym - 1 - cy), two cells of margin each way; the interval march
+// computes every step's cells from t alone, so a narrowed range gives the
+// same segments as the whole ray.
+__device__ __forceinline__ void strip_iterations(const ProjParams& P, const RayPlan& R, int y0, int y1, int& klo,
+                                                 int& khi)
+{
+    const int nym = (int)(P.N * 0.5);
+    const double ca = (double)(nym - y1 - 2), cb = (double)(nym - y0 + 2);  // cy range, with margin
+    double ta, tb;
+    if (R.d) {                       // y dominant: cy = floor(D0 + pha t)
+        ta = (ca - R.D0) * R.pha;
+        tb = (cb - R.D0) * R.pha;
+    } else if (R.O1 != 0.0) {        // cy = floor(O0 + O1 t)
+        ta = (ca - R.O0) * R.invO1;
+        tb = (cb - R.O0) * R.invO1;
+    } else {                         // constant y
+        if (!(R.O0 >= ca && R.O0 <= cb)) khi = klo - 1;
+        return;
+    }
+    if (ta > tb) {
+        const double t = ta;
+        ta = tb;
+        tb = t;
+    }
+    if (!(tb >= (double)(klo - 1)) || !(ta <= (double)khi)) {
+        khi = klo - 1;
+        return;
+    }
+    klo = max(klo, (int)floor(ta));
+    khi = min(khi, (int)ceil(tb) + 1);
+}
+
+__device__ __forceinline__ void warp_range_k(int klo, int khi, bool use, int& Klo, int& Khi)
+{
+    Klo = __reduce_min_sync(0xffffffffu, use && klo <= khi ? klo : INT_MAX);
+    Khi = __reduce_max_sync(0xffffffffu, use && klo <= khi ? khi : -1);
+}
+
 // grid: (ceil(W / cols_per_block), ceil(H / 32), V); block: (32, cols_per_block).
 // Per-element path integrals of one ray (first segment + iterations
 // [Klo, Khi]).  The interval march is used unless a lane of the warp has
@@ -1141,6 +1183,20 @@ __global__ void __launch_bounds__(256, VCBCT_ADJ_MIN_BLOCKS) adjoint_kernel(Adjo
     // rays with a zero residual do not scatter
     warp_range(R, act, Klo, Khi);
     if (!__any_sync(0xffffffffu, act && R.active)) return;
+    // a warp none of whose segments can lie in the strip stops here (before
+    // recomputing or reading its path integrals)
+    const bool strip = a.y1 > a.y0;
+    const bool steep = R.active && __any_sync(0xffffffffu, fabs(R.Z1) >= 1.0);
+    int Klo2 = Klo, Khi2 = Khi;
+    if (strip && R.active && !steep) {
+        int klo = R.klo, khi = R.khi;
+        strip_iterations(P, R, a.y0, a.y1, klo, khi);
+        warp_range_k(klo, khi, act, Klo2, Khi2);
+        const unsigned NZ = (unsigned)P.N * (unsigned)P.Z;
+        const bool first_in = act && R.first_idx >= 0 &&
+                              (unsigned)R.first_idx - (unsigned)a.y0 * NZ < (unsigned)(a.y1 - a.y0) * NZ;
+        if (Klo2 > Khi2 && !__any_sync(0xffffffffu, first_in)) return;
+    }
 
     // pass 1: the per-element path integrals of this ray, recomputed by a
     // first march or read from the forward projection that made them
@@ -1177,13 +1233,14 @@ __global__ void __launch_bounds__(256, VCBCT_ADJ_MIN_BLOCKS) adjoint_kernel(Adjo
         g[6] = fmaf(w, m1.z, g[6]); g[7] = fmaf(w, m1.w, g[7]);
     }
     const float scale = -R.leng * r;
-    Scatter<M> sc{a.grad_planes, (size_t)P.N * P.N * P.Z, P.nmat, {}};
+    const unsigned NZ = (unsigned)P.N * (unsigned)P.Z;
+    Scatter<M> sc{a.grad_planes, (size_t)P.N * P.N * P.Z, P.nmat, {},
+                  strip ? (unsigned)a.y0 * NZ : 0u, strip ? (unsigned)(a.y1 - a.y0) * NZ : 0xffffffffu};
 #pragma unroll
     for (int i = 0; i < 8; i++) sc.g[i] = g[i] * scale;
     // pass 2: scatter along the same segments
     if (!R.active) return;
-    const bool steep = __any_sync(0xffffffffu, fabs(R.Z1) >= 1.0);
-    if (steep) {
+    if (steep) {  // the whole ray (its per-step state depends on where it starts), filtered
         if (act) {
             if (R.first_idx >= 0) sc(R.first_idx, R.first_len);
             if (Klo <= Khi) march(P, R, Klo, Khi, sc);
@@ -1191,8 +1248,9 @@ __global__ void __launch_bounds__(256, VCBCT_ADJ_MIN_BLOCKS) adjoint_kernel(Adjo
         return;
     }
     if (act && R.first_idx >= 0) sc(R.first_idx, R.first_len);
+    // only the iterations whose segments can lie in the strip's rows
     const XyPlan& xp = publish_plan(R, wbuf);
-    if (Klo <= Khi) march_intervals(P, R, xp, act, Klo, Khi, wbuf, sc, []() {});
+    if (Klo2 <= Khi2) march_intervals(P, R, xp, act, Klo2, Khi2, wbuf, sc, []() {});
 }
 
 // ------------------------------------------------------- layout kernels --
