@@ -97,6 +97,9 @@ __global__ void __launch_bounds__(256) filter_direct_kernel(
 #ifndef VCBCT_BP_MIN_BLOCKS
 #define VCBCT_BP_MIN_BLOCKS 5
 #endif
+#ifndef VCBCT_BP_TILE
+#define VCBCT_BP_TILE 4  // warp tile width in voxel columns (4, 8, 16 or 32)
+#endif
 #ifndef VCBCT_BP_ZB
 #define VCBCT_BP_ZB 16
 #endif
@@ -105,8 +108,14 @@ __global__ void __launch_bounds__(256, VCBCT_BP_MIN_BLOCKS) backproject_kernel(
     FdkParams f, const BpView* __restrict__ views, const float* __restrict__ filt,
     float* __restrict__ vol_f32, short* __restrict__ vol_i16)
 {
-    const int x = blockIdx.x * 32 + threadIdx.x;
-    const int y = blockIdx.y * 8 + threadIdx.y;
+    // each warp takes a TW x (32 / TW) tile of the block's 32 x 8 columns:
+    // the detector's column-edge and cone-edge lines split fewer warps than
+    // with 32 x 1 rows, and a warp's taps fall in fewer cache lines (B200,
+    // 270x270x200 from 360 half-fan views: 3.35 ms with 4 x 8 tiles, 3.44
+    // with 8 x 4, 3.59 with 16 x 2, 3.96 with 32 x 1; the volume is the same)
+    constexpr int TW = VCBCT_BP_TILE, TH = 32 / TW, WX = 32 / TW;
+    const int x = blockIdx.x * 32 + (threadIdx.y % WX) * TW + (threadIdx.x % TW);
+    const int y = blockIdx.y * 8 + (threadIdx.y / WX) * TH + (threadIdx.x / TW);
     const int z0 = blockIdx.z * ZB;
     if (x >= f.N || y >= f.N) return;
     const double R = (double)(f.N - 1) / 2.0;
