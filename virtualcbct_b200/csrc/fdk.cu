@@ -91,17 +91,20 @@ __global__ void __launch_bounds__(256) filter_direct_kernel(
 // reference's edge rules and its weight quirk (the column weight is frac(U),
 // not frac(UUU), reconstructImage.cpp:80-83).
 // Register cap (minimum resident 256-thread blocks per SM) and slices per
-// thread.  The gathers are latency-bound: 5 blocks (48 registers, 40 warps
-// per SM) with 16 slices measured 16 % faster on B200 than the compiler's
-// choice (77 registers), and faster than 8 or 32 slices at any cap.
+// thread.  The gathers are latency-bound, so occupancy pays: with 4 x 8 warp
+// tiles, 8 slices at 6 blocks (40 registers, 48 warps per SM) measured on
+// B200 as fast as 16 slices at 5 blocks on 270x270x200 from 360 half-fan
+// views (3.39 vs 3.37 ms) and 10-19 % faster where more of the volume lies in
+// the cone (512x512x400 / x100 from 720 views of 800x800: 55 vs 61 ms, 22 vs
+// 27 ms); 12, 20 slices and 16 at 4 blocks were slower.
 #ifndef VCBCT_BP_MIN_BLOCKS
-#define VCBCT_BP_MIN_BLOCKS 5
+#define VCBCT_BP_MIN_BLOCKS 6
 #endif
 #ifndef VCBCT_BP_TILE
 #define VCBCT_BP_TILE 4  // warp tile width in voxel columns (4, 8, 16 or 32)
 #endif
 #ifndef VCBCT_BP_ZB
-#define VCBCT_BP_ZB 16
+#define VCBCT_BP_ZB 8
 #endif
 template <int ZB>
 __global__ void __launch_bounds__(256, VCBCT_BP_MIN_BLOCKS) backproject_kernel(
