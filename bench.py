@@ -641,21 +641,23 @@ def deck_load_section():
         shutil.rmtree(tmp, ignore_errors=True)
 
 
-def batched_small_section(stream):
-    """Many small phantoms (64 of 128x128xZ, Z 16-64, V 18-90, 64x64
-    detector): the regime where one launch per phantom leaves the GPU idle
+def batched_small_section(stream, n=64, N=128, zr=(16, 64), vr=(18, 90), det=64, s=0.25, step=0.5, seed=77):
+    """Many small phantoms (default: 64 of 128x128xZ, Z 16-64, V 18-90, 64x64
+    detector; `bench.py` also runs 256 tiny ones: 64x64xZ, Z 8-24, V 8-24,
+    32x32): the regime where one launch per phantom leaves the GPU idle
     between launches.  Plain = one projector launch per phantom issued from
-    the host; batched = the autotuned batch replayed from its CUDA graph, and
-    the persistent single-launch strategy forced."""
+    the host (a Python loop, as a user would write it); batched = the
+    autotuned batch replayed from its CUDA graph, and the persistent and
+    flat single-launch strategies forced."""
     import torch
     from virtualcbct_b200 import Batch, Projector, ProjGeometry, attenuation_table, phantoms, trig_tables
-    rng = np.random.default_rng(77)
+    rng = np.random.default_rng(seed)
     mu, pdf = attenuation_table(os.path.join(DATA, "spectrum_kramers100_90.csv"), MINIDB, 6)
     projs, outs = [], []
-    for i in range(64):
-        Z = int(rng.integers(16, 65))
-        V = int(rng.integers(18, 91))
-        g = ProjGeometry(N=128, Z=Z, s=0.25, step=0.5, W=64, H=64, V=V)
+    for i in range(n):
+        Z = int(rng.integers(zr[0], zr[1] + 1))
+        V = int(rng.integers(vr[0], vr[1] + 1))
+        g = ProjGeometry(N=N, Z=Z, s=s, step=step, W=det, H=det, V=V)
         ang = np.deg2rad(phantoms.view_angles(V))
         tabs = trig_tables(g.W, g.H, ang, np.zeros(V), np.zeros(V), g.pdet, g.dpn)
         p = Projector(g, *tabs)
@@ -687,9 +689,9 @@ def batched_small_section(stream):
     auto = t(lambda: b_auto.forward(use_graph=True))
     pers = t(lambda: b_pers.forward(use_graph=True))
     flat = t(lambda: b_flat.forward(use_graph=True))
-    return {"workload": "64 ellipsoid phantoms 128x128xZ (Z 16-64), V 18-90, 64x64", "segments": nseg,
-            "autotuned": tuned, "plain_ms": plain, "batched_graph_ms": auto, "persistent_graph_ms": pers,
-            "flat_graph_ms": flat, "batched_over_plain_speedup": plain / auto,
+    return {"workload": f"{n} ellipsoid phantoms {N}x{N}xZ (Z {zr[0]}-{zr[1]}), V {vr[0]}-{vr[1]}, {det}x{det}",
+            "segments": nseg, "autotuned": tuned, "plain_ms": plain, "batched_graph_ms": auto,
+            "persistent_graph_ms": pers, "flat_graph_ms": flat, "batched_over_plain_speedup": plain / auto,
             "persistent_over_plain_speedup": plain / pers, "flat_over_plain_speedup": plain / flat}
 
 
@@ -808,6 +810,8 @@ def run_ours(args, rank, world, local_rank):
         extra["decomposition_fullscale"] = decomposition_fullscale_section(stream)
         extra["batched"] = batched_section(stream, args)
         extra["batched_small"] = batched_small_section(stream)
+        extra["batched_tiny"] = batched_small_section(stream, n=256, N=64, zr=(8, 24), vr=(8, 24), det=32, s=0.4,
+                                                      step=0.8, seed=78)
         extra["iterative"] = iterative_section(stream)
         extra["deck_load"] = deck_load_section()
         extra["noise"] = noise_section(stream, P, out)
