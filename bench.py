@@ -1,7 +1,7 @@
 #!/usr/bin/env python
 """Benchmark of the MBFPA hot path (plus FDK) on synthetic data.
 
-Metric (BASELINE.json): MBFPA ray-voxel throughput in Gseg/s -- one "segment"
+Metric: MBFPA ray-voxel throughput in Gseg/s -- one "segment"
 is one in-volume, in-cylinder, non-degenerate segment of the reference's
 Siddon-style march that reads one voxel's six element values -- with FDK
 backprojection GUPS, the forward+adjoint / forward ratio and the CPU baseline

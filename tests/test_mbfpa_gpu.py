@@ -10,7 +10,7 @@ from virtualcbct_b200 import Projector
 
 pytestmark = pytest.mark.gpu
 
-# north_star tolerance: 1e-5 relative per detector pixel.
+# Parity bar for projections: 1e-5 relative per detector pixel.
 RTOL = 1e-5
 
 
