@@ -43,7 +43,7 @@ enum {
     VCBCT_ERR_DEVICE = 6   /* a kernel reported a runtime fault flag */
 };
 
-/* Limits of this build. */
+/* Compile-time limits of the library. */
 #define VCBCT_MAX_MATERIALS 8   /* element planes per voxel */
 #define VCBCT_MAX_BINS 1024     /* energy bins (reference arrays are 1024) */
 
