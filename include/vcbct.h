@@ -10,7 +10,7 @@
  *
  *  1. Reference-named entry points with the reference's exact signatures, so
  *     that a main.cpp-style driver of hagaakihiro/VirtualCBCT links unchanged
- *     (see INTEGRATION.md).  Each cites the declaration it replaces.
+ *     against -lvcbct.  Each cites the declaration it replaces.
  *  2. vcbct_* entry points: explicit geometry structs, host or device
  *     buffers, a CUDA stream (passed as void*, 0 = legacy default stream) and
  *     an int status (VCBCT_OK = 0).  vcbct_last_error() gives the message of
