@@ -139,6 +139,28 @@ def bp_update_counts(fg, ang, xs):
     return N * N * Z * V, int(m.sum()) * Z * V, eff
 
 
+def fdk_cpu_baseline(fg, ang, xs, views, proj, filt):
+    """The reference's filterSinogram and reconstructImage (compiled from its
+    sources, OpenMP on all host cores) on a sample of the views, extrapolated
+    linearly in the view count to the whole stack."""
+    import oracle as O
+    try:
+        ncores = os.cpu_count() or 1
+        n = len(views)
+        _, s_filt = O.ref_filter(proj, xs[views], np.zeros(n), fg.piso, ncores)
+        _, s_bp = O.ref_backproject(fg.N, fg.Z, fg.zstart, fg.step, fg.scale, filt, fg.xfactor, ang[views], xs[views],
+                                    fg.piso, ncores)
+        k = fg.V / n
+        bp_s = s_bp * k
+        return {"filter_ms": s_filt * k * 1e3, "bp_ms": bp_s * 1e3,
+                "bp_gups": fg.N * fg.N * fg.Z * fg.V / bp_s / 1e9, "unit": "ms / GUPS", "cores": ncores,
+                "kind": "reference",
+                "sample": f"filterSinogram ({s_filt:.2f} s) and reconstructImage ({s_bp:.2f} s) on {n} of "
+                          f"{fg.V} views, extrapolated to {fg.V} views"}
+    except Exception as e:  # informative, never fatal
+        return {"value": None, "kind": "reference", "sample": f"unavailable: {e}"}
+
+
 def measured_peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -802,6 +824,10 @@ def run_ours(args, rank, world, local_rank):
     Kp = (fg.W + 63) // 64 * 64
     Np = (fg.W + 15) // 16 * 16
     gemm_tflops = 2.0 * 6 * fg.V * fg.H * Kp * Np / (ms_filter * 1e-3) / 1e12
+    # host copies of a view sample for the reference FDK's CPU timing
+    fdk_views = np.arange(0, fg.V, 10)
+    fdk_proj_h = out[torch.from_numpy(fdk_views).to(dev)].cpu().numpy()
+    fdk_filt_h = filt[torch.from_numpy(fdk_views).to(dev)].cpu().numpy()
     del F, filt_d
 
     extra = {}
@@ -882,6 +908,7 @@ def run_ours(args, rank, world, local_rank):
         except Exception as e:  # the baseline is informative, never fatal
             res["cpu_baseline"] = {"value": None, "unit": "Gseg/s", "cores": os.cpu_count(),
                                    "kind": "reference", "sample": f"unavailable: {e}"}
+        res["fdk"]["cpu_baseline"] = fdk_cpu_baseline(fg, ang, w["xs_fdk"], fdk_views, fdk_proj_h, fdk_filt_h)
     if rank == 0:
         print(json.dumps(res))
 
