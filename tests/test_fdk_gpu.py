@@ -61,6 +61,25 @@ def test_backprojection_matches_reference(cuda, xshift):
     assert np.abs(vi.astype(np.int32) - ref_i16.astype(np.int32)).max() <= 1
 
 
+def test_odd_sizes_match_reference(cuda):
+    """Odd detector and volume sizes (H / 2 and W / 2 round down as in the
+    reference; a partial slice block; warps cut by the volume's edge) and an
+    offset detector: filter against the FP64 filter, backprojection and short
+    volume against reconstructImage."""
+    if not O.have_reference():
+        pytest.skip("reference CPU objects not built")
+    g, proj, ang, xs = _case(V=7, H=41, W=47, N=33, Z=11, seed=5, xshift=1.0)
+    f = Fdk(g, ang, xs, np.zeros(g.V))
+    gpu = f.filter(proj, method=FILTER_DIRECT_F32)
+    d64 = O.filter_sinogram(proj, xs, np.zeros(g.V), O.fdk_consts(g.piso), mode=1)
+    assert np.abs(gpu - d64).max() <= 1e-5 * np.abs(d64).max()
+    filt, _ = O.ref_filter(proj, xs, np.zeros(g.V), g.piso)
+    vf, vi = f.backproject(filt)
+    ref, _ = O.ref_backproject(g.N, g.Z, g.zstart, g.step, g.scale, filt, g.xfactor, ang, xs, g.piso)
+    assert np.abs(vf - ref).max() <= 1e-5 * max(1.0, np.abs(ref).max())
+    assert np.abs(vi.astype(np.int32) - ref.astype(np.int16).astype(np.int32)).max() <= 1
+
+
 def test_fdk_chain_short_volume_within_one_lsb(cuda):
     if not O.have_reference():
         pytest.skip("reference CPU objects not built")

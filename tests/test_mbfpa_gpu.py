@@ -41,6 +41,9 @@ CASES = [
     # slice boundary (the reference's (int)(nzm - z/step) rule applies)
     ("ellipsoid", 7, dict(z_reg=0.0, V=6)),
     ("random", 8, dict(z_reg=0.0, N=32, Z=64, s=0.3, step=0.02, V=2, W=24, H=40, dpn=900.0)),
+    # one view of a 5 x 3 detector: a warp with 3 of 32 rows, a partial block
+    # of columns
+    ("ellipsoid", 11, dict(V=1, W=5, H=3)),
 ]
 
 
