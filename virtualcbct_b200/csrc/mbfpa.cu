@@ -21,6 +21,12 @@
 //    (Siddon alphas) of plane crossings.  The march itself is FP32, with
 //    voxel cells carried as integers plus a small fractional offset so that no
 //    FP32 value has to resolve a large coordinate near a plane.
+//
+// Also here: the band footprints of the host-to-host pipelined projection,
+// the batch kernels (persistent work queue, flat tile list), the adjoint
+// (per-ray spectral derivative, then the same segments scattered into one
+// z-fastest plane per element, optionally restricted to a strip of volume
+// rows), and the volume / gradient re-layout kernels.
 #include "internal.h"
 #include "noise.cuh"
 
