@@ -36,3 +36,34 @@ def test_fdk_cpu_baseline_is_never_fatal():
     r = bench.fdk_cpu_baseline(fg, np.zeros(fg.V), np.zeros(fg.V), np.arange(3), None, None)
     assert r["kind"] == "reference" and r["value"] is None
     assert r["sample"].startswith("unavailable")
+
+
+def test_effective_update_count_matches_a_direct_count():
+    """The backprojection's effective voxel-view updates (the denominator of
+    its gather-roof fraction): the per-view slice-range formula of
+    bench.bp_update_counts against a direct per-voxel test of the detector
+    column and row, on a small half-fan geometry."""
+    fg = FdkGeometry(W=16, H=12, V=12, N=21, Z=14, zstart=-10, step=1.5, scale=1.0)
+    ang = np.deg2rad(-180.0001 + np.arange(fg.V) * 30.0)
+    xs = np.full(fg.V, 4.0)  # an offset detector (x10 px)
+    n_all, n_mask, n_eff = bench.bp_update_counts(fg, ang, xs)
+    N, Z, W, H = fg.N, fg.Z, fg.W, fg.H
+    R = (N - 1) / 2.0
+    y, x = np.mgrid[0:N, 0:N].astype(np.float64)
+    m = (y - R) ** 2 + (x - R) ** 2 <= R * R
+    cp = N / 2.0 - 0.5
+    xx, yy = ((x - cp) * fg.scale)[m], (-(y - cp) * fg.scale)[m]
+    pitch = fg.piso * fg.mpn / W
+    px = fg.pdet * fg.mpn / W
+    zz = fg.zstart + np.arange(Z) * fg.step
+    eff = 0
+    for th in range(fg.V):
+        cs, sn = np.cos(ang[th]), np.sin(ang[th])
+        g = 1.0 / ((1.0 - (-xx * sn + yy * cs) / fg.sad) * pitch)
+        uu = np.floor((W // 2) + xs[th] / px - 0.5 + (xx * cs + yy * sn) * g)
+        row = np.floor((H // 2) + zz[None, :] * g[:, None])
+        ok = ((uu >= 0) & (uu <= W - 1))[:, None] & (row >= 0) & (row <= H - 1)
+        eff += int(ok.sum())
+    assert n_all == N * N * Z * fg.V and n_mask == int(m.sum()) * Z * fg.V
+    assert 0 < eff < n_mask
+    assert abs(n_eff - eff) <= 1e-3 * eff
