@@ -157,7 +157,7 @@ extern "C" int vcbct_projector_create(const vcbct_proj_geometry* g, const double
     if (e == cudaSuccess) e = p->counter.ensure(64);
     if (e == cudaSuccess) e = cudaMemset(p->counter.p, 0, 64);
     if (e != cudaSuccess) {
-        delete p;
+        vcbct_projector_destroy(p);  // frees what was allocated
         return cuda_fail(e, "vcbct_projector_create");
     }
     if (const char* c = std::getenv("VCBCT_COLS_PER_BLOCK")) {
@@ -1564,7 +1564,7 @@ extern "C" int vcbct_fdk_create(const vcbct_fdk_geometry* g, const double* angle
     ramp_kernel(W, g->det_pitch_iso_cm, g->max_pic_num, g->cutoff, g->gamma, g->alpha, f->h.data());
     int rc = upload_kernel(f);
     if (rc) {
-        delete f;
+        vcbct_fdk_destroy(f);  // frees what was allocated
         return rc;
     }
     std::vector<FilterView> fv(V);
@@ -1603,7 +1603,7 @@ extern "C" int vcbct_fdk_create(const vcbct_fdk_geometry* g, const double* angle
         f->have_wts = 1;
     }
     if (e != cudaSuccess) {
-        delete f;
+        vcbct_fdk_destroy(f);  // frees what was allocated
         return cuda_fail(e, "vcbct_fdk_create");
     }
     *out = f;
