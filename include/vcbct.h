@@ -430,6 +430,14 @@ typedef struct vcbct_fdk vcbct_fdk;
 int vcbct_fdk_create(const vcbct_fdk_geometry* g, const double* angles_rad,
                      const double* xshift, const double* yshift, vcbct_fdk** out);
 int vcbct_fdk_destroy(vcbct_fdk* f);
+/* The redundancy weights the filter applies to -log p with redundancy = 1,
+ * float [n_views][proj_width] into w (host only, no device call): for an
+ * offset (half-fan) detector, 2 sin^2(pi/4 (1 + u/u0)) across the band
+ * |u| < u0 seen from both sides of the rotation axis, 2 beyond it on the long
+ * side, 0 beyond the short edge (u: column position at the isocentre), so
+ * that a ray and its conjugate weigh 2 together.  No reference counterpart
+ * (the reference has only the offset terms of filterSinogram.cpp:86-87). */
+int vcbct_fdk_redundancy_weights(const vcbct_fdk_geometry* g, const double* xshift, float* w);
 /* Optional: replace the ramp kernel h[W][W] (prepareConstMap layout). */
 int vcbct_fdk_set_kernel(vcbct_fdk* f, const double* h);
 /* filterSinogram (R/filterSinogram.cpp:67-131): proj, filtered float [V][H][W]. */

@@ -143,6 +143,7 @@ SIGNATURES = {
     "vcbct_fdk_default_geometry": (None, [C.POINTER(FdkGeometryC)]),
     "vcbct_fdk_create": (C.c_int, [C.POINTER(FdkGeometryC), _dp, _dp, _dp, C.POINTER(_vp)]),
     "vcbct_fdk_destroy": (C.c_int, [_vp]),
+    "vcbct_fdk_redundancy_weights": (C.c_int, [C.POINTER(FdkGeometryC), _dp, _fp]),
     "vcbct_fdk_set_kernel": (C.c_int, [_vp, _dp]),
     "vcbct_fdk_filter": (C.c_int, [_vp, _vp, _vp, C.c_int, C.c_int, _vp]),
     "vcbct_fdk_backproject": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int, _vp]),

@@ -1540,6 +1540,21 @@ static void halffan_weights(const vcbct_fdk& f, std::vector<float>& w)
     }
 }
 
+extern "C" int vcbct_fdk_redundancy_weights(const vcbct_fdk_geometry* g, const double* xshift, float* w)
+{
+    if (!g || !xshift || !w) return fail(VCBCT_ERR_ARG, "NULL argument");
+    if (g->proj_width <= 1 || g->n_views <= 0 || !(g->det_pitch_iso_cm > 0) || !(g->det_pitch_cm > 0) ||
+        !(g->max_pic_num > 0))
+        return fail(VCBCT_ERR_ARG, "FDK sizes and pitches must be positive");
+    vcbct_fdk f;  // host fields only: the weights read the geometry and the shifts
+    f.g = *g;
+    f.xs.assign(xshift, xshift + g->n_views);
+    std::vector<float> wv;
+    halffan_weights(f, wv);
+    std::copy(wv.begin(), wv.end(), w);
+    return VCBCT_OK;
+}
+
 extern "C" int vcbct_fdk_create(const vcbct_fdk_geometry* g, const double* angles,
                                 const double* xshift, const double* yshift, vcbct_fdk** out)
 {

@@ -18,6 +18,19 @@ def _dp(a):
     return a.ctypes.data_as(C.POINTER(C.c_double))
 
 
+def redundancy_weights(geom: FdkGeometry, xshift=None) -> np.ndarray:
+    """The redundancy weights float [V][W] the filter applies to -log p when
+    ``geom.redundancy`` is 1 (host computation, no device call)."""
+    x = np.zeros(geom.V) if xshift is None else np.ascontiguousarray(xshift, np.float64)
+    if x.shape[0] != geom.V:
+        raise ValueError("xshift must have n_views entries")
+    w = np.empty((geom.V, geom.W), np.float32)
+    gc = geom.to_c()
+    N.check(N.lib().vcbct_fdk_redundancy_weights(C.byref(gc), _dp(x),
+                                                 w.ctypes.data_as(C.POINTER(C.c_float))))
+    return w
+
+
 class Fdk:
     def __init__(self, geom: FdkGeometry, angles_rad, xshift=None, yshift=None):
         self.geom = geom
