@@ -5,7 +5,7 @@ import numpy as np
 import pytest
 
 import oracle as O
-from virtualcbct_b200 import FILTER_DIRECT_F32, Fdk, FdkGeometry
+from virtualcbct_b200 import FILTER_BF16X3, FILTER_DIRECT_F32, Fdk, FdkGeometry, redundancy_weights
 
 pytestmark = pytest.mark.gpu
 
@@ -44,6 +44,22 @@ def test_filter_with_offset_detector(cuda):
     f = Fdk(g, ang, xs, np.zeros(g.V))
     gpu = f.filter(proj)
     d64 = O.filter_sinogram(proj, xs, np.zeros(g.V), O.fdk_consts(g.piso), mode=1)
+    assert np.abs(gpu - d64).max() <= 1e-5 * np.abs(d64).max()
+
+
+@pytest.mark.parametrize("method", [FILTER_DIRECT_F32, FILTER_BF16X3])
+def test_redundancy_weighted_filter_matches_fp64(cuda, method):
+    """With redundancy = 1 both filters weight -log p by the half-fan
+    redundancy weights before filtering: against the FP64 filter of
+    w * (-log p), given as p ** w."""
+    g, proj, ang, xs = _case(xshift=3.0)
+    g = g.with_(redundancy=1)
+    w = redundancy_weights(g, xs)
+    assert w.min() == 0.0 and w.max() == 2.0
+    f = Fdk(g, ang, xs, np.zeros(g.V))
+    gpu = f.filter(proj, method=method)
+    pw = (proj.astype(np.float64) ** w[:, None, :].astype(np.float64)).astype(np.float32)
+    d64 = O.filter_sinogram(pw, xs, np.zeros(g.V), O.fdk_consts(g.piso), mode=1)
     assert np.abs(gpu - d64).max() <= 1e-5 * np.abs(d64).max()
 
 
