@@ -46,7 +46,7 @@ METRIC = "MBFPA ray-voxel Gseg/s & FDK GUPS; batched vs plain; grad-step/fwd rat
 
 # DRAM traffic of one forward launch of this workload: ncu
 # dram__bytes_read.sum + dram__bytes_write.sum of the first launch of
-# `python -m virtualcbct_b200.profile_cases forward_c2 1` (a one-pass capture
+# `python -m measure.profile_cases forward_c2 1` (a one-pass capture
 # of the full-size launch): 3.25 GB read + 1.70 GB written.
 FORWARD_DRAM_BYTES = 4.95e9
 
@@ -845,9 +845,10 @@ def run_ours(args, rank, world, local_rank):
 
     # measured gather rooflines: the projector's and the backprojector's
     # access patterns replayed without arithmetic on this device
-    probe_fwd = vc.probe_gather(0) / 1e9
-    probe_bp_smem = vc.probe_gather(1) / 1e9
-    probe_bp_l1 = vc.probe_gather(2) / 1e9
+    from measure import probe_gather
+    probe_fwd = probe_gather(0) / 1e9
+    probe_bp_smem = probe_gather(1) / 1e9
+    probe_bp_l1 = probe_gather(2) / 1e9
     gather_roof = {
         "mbfpa": {"pattern": "ray-front 16-B record gather (11-record runs, stride Z)",
                   "peak_gseg_s": probe_fwd, "achieved_gseg_s": value, "frac": value / probe_fwd},

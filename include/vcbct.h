@@ -276,14 +276,6 @@ int vcbct_mbfpa_forward_noalloc(const vcbct_proj_geometry* g, const double* cos_
                                 const float* attenuation, const float* pdf, int n_bins,
                                 double xfactor, float* d_out, void* stream);
 
-/* Measured gather rooflines (no reference counterpart): replays of the
- * forward projector's (kind 0: lane-records of 16 B per second over a
- * 512x512x200 z-fastest volume) and the backprojector's (kind 1: bilinear
- * voxel updates per second from a shared-memory detector tile; kind 2: the
- * same from global memory through L1) access patterns with no arithmetic
- * around them.  Synchronous on `stream`; allocates and frees its buffers. */
-int vcbct_probe_gather(int kind, double* rate, void* stream);
-
 /* Host helpers of the projector's input preparation. */
 /* misc.cpp:10-37 prepareTrigonometricTable (outputs caller-allocated). */
 int vcbct_proj_trig_tables(int proj_width, int proj_height, int n_views,

@@ -1,5 +1,8 @@
 // gather_probe.cu -- measured gather rooflines of the two gather-bound kernels.
 //
+// Measurement code only: built into measure/libgather_probe.so for bench.py,
+// not part of libvcbct.so.
+//
 // The forward projector and the backprojector are bound by how fast the SMs
 // can gather small records, not by DRAM streaming (their working sets sit in
 // L2 / L1).  These probes replay each kernel's access pattern with no
@@ -19,11 +22,11 @@
 //    columns apart, successive slices 3.1 rows apart.  Rate unit: voxel
 //    updates (4 taps) per second.
 //  kind 2, the same BP pattern read from global memory through L1.
-#include "internal.h"
+#include <cuda_runtime.h>
 
 #include <cstdint>
+#include <cstdio>
 
-namespace vcbct {
 namespace {
 
 constexpr int kProbeN = 512, kProbeZ = 200, kRun = 11, kSteps = 512;
@@ -94,21 +97,40 @@ __global__ void __launch_bounds__(256) bp_tile_probe(const float* __restrict__ t
     if (acc == 1.2345e-30f) sink[0] = acc;
 }
 
-}  // namespace
-}  // namespace vcbct
+char g_msg[256];
 
-using namespace vcbct;
-
-extern "C" int vcbct_probe_gather(int kind, double* rate, void* stream)
+int cuda_err(cudaError_t e, const char* what)
 {
-    if (!rate || kind < 0 || kind > 2) return fail(VCBCT_ERR_ARG, "kind must be 0, 1 or 2");
+    std::snprintf(g_msg, sizeof g_msg, "%s: %s", what, cudaGetErrorString(e));
+    return 2;
+}
+
+}  // namespace
+
+// Message of the last failure (empty after a success).
+extern "C" const char* gather_probe_error(void) { return g_msg; }
+
+// Rate of probe `kind` (0, 1, 2; units above) on the current device, written
+// to *rate.  Returns 0, 1 for a bad argument, 2 for a CUDA failure.
+// Synchronous on `stream`; allocates and frees its own buffers.
+extern "C" int gather_probe_run(int kind, double* rate, void* stream)
+{
+    g_msg[0] = 0;
+    if (!rate || kind < 0 || kind > 2) {
+        std::snprintf(g_msg, sizeof g_msg, "kind must be 0, 1 or 2");
+        return 1;
+    }
     cudaStream_t st = (cudaStream_t)stream;
     int dev = 0, sms = 0;
-    VCBCT_CUDA_TRY(cudaGetDevice(&dev));
-    VCBCT_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return cuda_err(e, "device query");
     cudaEvent_t e0, e1;
-    VCBCT_CUDA_TRY(cudaEventCreate(&e0));
-    VCBCT_CUDA_TRY(cudaEventCreate(&e1));
+    if ((e = cudaEventCreate(&e0)) != cudaSuccess) return cuda_err(e, "event");
+    if ((e = cudaEventCreate(&e1)) != cudaSuccess) {
+        cudaEventDestroy(e0);
+        return cuda_err(e, "event");
+    }
     void* buf = nullptr;
     void* sink = nullptr;
     cudaError_t err = cudaSuccess;
@@ -150,7 +172,7 @@ extern "C" int vcbct_probe_gather(int kind, double* rate, void* stream)
     cudaEventDestroy(e1);
     if (buf) cudaFree(buf);
     if (sink) cudaFree(sink);
-    if (err != cudaSuccess) return cuda_fail(err, "gather probe");
+    if (err != cudaSuccess) return cuda_err(err, "gather probe");
     *rate = units / (ms * 1e-3);
-    return VCBCT_OK;
+    return 0;
 }

@@ -1,6 +1,6 @@
 """Small, self-contained launches of each kernel for profiler captures.
 
-    python -m virtualcbct_b200.profile_cases <case> [repeats]
+    python -m measure.profile_cases <case> [repeats]
 
 Each case builds its inputs on the device, runs the kernel ``repeats`` times
 (default 2) and prints one line.  The cases are sized to hold a few hundred MB
@@ -35,8 +35,8 @@ import sys
 
 import numpy as np
 
-from . import FILTER_BF16X3, FILTER_DIRECT_F32, Batch, Fdk, FdkGeometry, Projector, ProjGeometry
-from . import attenuation_table, phantoms, trig_tables
+from virtualcbct_b200 import FILTER_BF16X3, FILTER_DIRECT_F32, Batch, Fdk, FdkGeometry, Projector, ProjGeometry
+from virtualcbct_b200 import attenuation_table, phantoms, trig_tables
 
 DATA = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data")
 MINIDB = os.path.join(DATA, "xraydb_mini")
@@ -139,7 +139,7 @@ def run(case: str, repeats: int = 2) -> str:
         for _ in range(repeats):
             out = b.forward(use_graph=False)[0]
     elif case in ("lengthproj_c1", "ir_update_c1"):
-        from .iterative import ir_update
+        from virtualcbct_b200.iterative import ir_update
         g = ProjGeometry(N=512, Z=100, s=0.05, step=0.2, W=400, H=400, V=36)
         p = _projector(g, phantoms.view_angles(g.V))
         gen = torch.Generator(device="cuda")
@@ -159,7 +159,7 @@ def run(case: str, repeats: int = 2) -> str:
     elif case == "noise_c2":
         import ctypes as C
 
-        from . import _native as N
+        from virtualcbct_b200 import _native as N
         gen = torch.Generator(device="cuda")
         gen.manual_seed(9)
         out = 5000.0 + 55000.0 * torch.rand(360 * 400 * 400, generator=gen, device="cuda")
@@ -168,7 +168,7 @@ def run(case: str, repeats: int = 2) -> str:
     elif case == "phantom_512":
         import tempfile
 
-        from .icrp import PhantomTables, organs_to_elements
+        from virtualcbct_b200.icrp import PhantomTables, organs_to_elements
         rng = np.random.default_rng(3)
         with tempfile.TemporaryDirectory() as tmp:
             media, organs = os.path.join(tmp, "m.csv"), os.path.join(tmp, "o.csv")

@@ -20,10 +20,11 @@ ROOT = os.path.abspath(os.path.join(HERE, "..", ".."))
 sys.path.insert(0, ROOT)
 
 import oracle as O  # noqa: E402
+from oracle.refpath import reference_root  # noqa: E402
 from tests.cases import proj_case  # noqa: E402
 from tests.test_fdk_gpu import _case as fdk_case  # noqa: E402
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+REF = sys.argv[1] if len(sys.argv) > 1 else reference_root()
 P = os.path.join(REF, "Release_CBCT_Projection_CM")
 
 

@@ -113,8 +113,6 @@ def test_standalone_kernels_validate_arguments(L):
     ip, op = C.c_void_p(ids.ctypes.data), C.c_void_p(out.ctypes.data)
     assert L.vcbct_organs_to_elements(ip, 0, 1, C.byref(t), op, 0, None) == ARG
     assert L.vcbct_organs_to_elements(ip, 4, 70000, C.byref(t), op, 0, None) == LIMIT
-    r = C.c_double()
-    assert L.vcbct_probe_gather(3, C.byref(r), None) == ARG
 
 
 def test_file_readers_report_missing_files(L, tmp_path):

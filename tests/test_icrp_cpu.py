@@ -10,9 +10,10 @@ import numpy as np
 import pytest
 
 import oracle as O
+from oracle.refpath import reference_path
 from virtualcbct_b200.icrp import PhantomTables
 
-ICRP = "/root/reference/ICRPphantoms_2mmslice"
+ICRP = reference_path("ICRPphantoms_2mmslice")
 pytestmark = pytest.mark.skipif(not (O.have_icrp_convert() and os.path.isdir(ICRP)),
                                 reason="reference converter or its tables not available")
 

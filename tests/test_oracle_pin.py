@@ -10,11 +10,12 @@ import numpy as np
 import pytest
 
 import oracle as O
+from oracle.refpath import reference_path
 from tests.cases import DATA, MINIDB, proj_case
 from virtualcbct_b200 import attenuation_table
 
 GOLD = os.path.join(os.path.dirname(__file__), "golden")
-REF_P = "/root/reference/Release_CBCT_Projection_CM"
+REF_P = reference_path("Release_CBCT_Projection_CM")
 
 
 def test_attenuation_builder_matches_reference_golden():

@@ -117,7 +117,6 @@ SIGNATURES = {
     "vcbct_batch_autotune": (C.c_int, [_vp, _vp, _ip]),
     "vcbct_mbfpa_forward_noalloc": (C.c_int, [C.POINTER(ProjGeometryC), _dp, _dp, _dp, _dp, _vp, _fp,
                                               _fp, C.c_int, C.c_double, _vp, _vp]),
-    "vcbct_probe_gather": (C.c_int, [C.c_int, _dp, _vp]),
     "vcbct_projector_set_noise": (C.c_int, [_vp, C.c_int, C.c_double, C.c_double, C.c_ulonglong]),
     "vcbct_gaussian_noise": (C.c_int, [_vp, C.c_size_t, C.c_double, C.c_ulonglong, C.c_int, _vp]),
     "vcbct_philox4x32_10": (None, [_vp, _vp, _vp]),

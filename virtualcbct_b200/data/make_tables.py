@@ -68,4 +68,7 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    # the reference tree: argument, else $VCBCT_REFERENCE, else baseline/_ref
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get(
+        "VCBCT_REFERENCE", os.path.join(HERE, "..", "..", "baseline", "_ref"))
+    main(ref)
