@@ -52,21 +52,24 @@ FORWARD_DRAM_BYTES = 4.95e9
 
 
 def workload():
-    from virtualcbct_b200 import ProjGeometry, FdkGeometry, attenuation_table, phantoms
-    N, Z, s, step = 512, 200, 0.05, 0.2
-    V, W, H = 360, 400, 400
-    g = ProjGeometry(N=N, Z=Z, s=s, step=step, W=W, H=H, V=V)
-    angles_deg = phantoms.view_angles(V, -180.0001)
-    xs_proj = np.full(V, 1.6)          # projector flexmap (x100 px, misc.cpp:31)
-    xs_fdk = np.full(V, 16.0)          # FDK flexmap (x10 px, filterSinogram.cpp:86)
-    vol = phantoms.water_cylinder(N, Z, s, 12.5)
-    mu, pdf = attenuation_table(os.path.join(DATA, "spectrum_kramers100_90.csv"), MINIDB, 6)
-    fg = FdkGeometry(W=W, H=H, V=V, N=270, Z=200, zstart=-20, step=0.2, scale=0.1,
-                     redundancy=1)
-    return dict(g=g, angles_deg=angles_deg, xs_proj=xs_proj, xs_fdk=xs_fdk, vol=vol, mu=mu,
-                pdf=pdf, fg=fg, xfactor=1000.0,
-                name="25 cm water cylinder 512x512x200x6 u16 (0.5x0.5x2 mm), 360 views/1 deg, "
-                     "half-fan 160 px, 400x400 f32, 90-bin 100 kV; FDK 270x270x200")
+    """The C2 workload (measure/workloads.c2_workload) with the product
+    library's spectrum table and FDK geometry (the GPU arm)."""
+    from measure.workloads import c2_workload, native_spectrum
+    w = c2_workload()
+    w["mu"], w["pdf"] = native_spectrum(w["spectrum_csv"])
+    w["g"] = w["g"].native()
+    w["fg"] = w["fdk"].native()
+    return w
+
+
+def cpu_model() -> str:
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
 
 
 class ClockSampler:
@@ -170,27 +173,20 @@ def measured_peaks():
         return 6650.0, "fallback"
 
 
-def cpu_reference_sample(w, views, bins, nthreads):
+def cpu_reference_sample(w, tabs, views, bins, nthreads):
     """Time the reference's own CPU projector (oracle/_ref) on (views x bins)."""
     import oracle as O
-    from virtualcbct_b200 import trig_tables
-    g = w["g"]
-    ang = np.deg2rad(w["angles_deg"])
-    tabs = trig_tables(g.W, g.H, ang, w["xs_proj"], np.zeros(g.V), g.pdet, g.dpn)
-    _, secs = O.ref_mbfpa_views(g, tabs, w["vol"], w["mu"], w["pdf"], w["xfactor"], views, bins,
-                                nthreads=nthreads)
+    with O.quiet_stdout():
+        _, secs = O.ref_mbfpa_views(w["g"], tabs, w["vol"], w["mu"], w["pdf"], w["xfactor"], views, bins,
+                                    nthreads=nthreads)
     return secs
 
 
-def segments_per_view_cpu(w, views):
+def segments_per_view_cpu(w, tabs, views):
     """Segment count of the sampled views from the CPU oracle (the unit's
     definition); used by the reference arm, which must not touch the GPU."""
     import oracle as O
-    from virtualcbct_b200 import trig_tables
-    g = w["g"]
-    ang = np.deg2rad(w["angles_deg"])
-    tabs = trig_tables(g.W, g.H, ang, w["xs_proj"], np.zeros(g.V), g.pdet, g.dpn)
-    r = O.mbfpa_forward(g, tabs, w["vol"], w["mu"][:, :1], w["pdf"][:1], w["xfactor"],
+    r = O.mbfpa_forward(w["g"], tabs, w["vol"], w["mu"][:, :1], w["pdf"][:1], w["xfactor"],
                         views=views, exact=False, want=("nm",))
     return {int(v): int(r["nm"][v].sum()) for v in views}
 
@@ -221,18 +217,31 @@ def job_rate(units_per_rank, world, ms_max):
 
 
 def run_reference(args, rank, world):
-    """Reference arm: the reference's CPU projector (reprojection.cpp compiled
-    from its sources, driven per view and bin over all host threads) on a
-    bounded sample of the workload each step; Gseg/s over the full job."""
+    """Reference arm: the reference's own CPU projector (reprojection(),
+    P/reprojection.cpp, compiled from its sources into oracle/_ref) on all
+    host threads.  Its inputs are built by the reference's own code too --
+    attenuation_coefficient (P/prior_weight_production.cpp:200) on the
+    reference's x-ray DB, prepareTrigonometricTable (P/misc.cpp:10) -- and the
+    volume by measure/workloads (numpy); segments are counted by the CPU
+    oracle.  Nothing of the product library is loaded.
+
+    A step is a bounded sample of the C2 workload: one view per host thread,
+    one energy bin.  reprojection() marches every segment once per bin, so
+    the rate in the metric's unit (segments of the whole spectral
+    projection) is the sample's segments / (its seconds x the bin count);
+    ms_per_step is the measured seconds of one sample."""
     if rank != 0:
         return
     import oracle as O
-    w = workload()
+    from measure.workloads import REF_PROJ_DIR, c2_workload, reference_tables
+    w = c2_workload()
     g = w["g"]
-    if not O.have_reference():
+    if not O.have_reference() or not os.path.isdir(REF_PROJ_DIR):
         print(json.dumps({"impl": "reference", "unavailable":
                           "oracle/_ref (reference CPU code compiled from its sources) is not built"}))
         return
+    w["mu"], w["pdf"] = O.ref_attenuation(REF_PROJ_DIR, w["spectrum_csv"], 6)
+    tabs = reference_tables(w)
     ncores = os.cpu_count() or 1
     NE = int(w["pdf"].shape[0])
     nviews = max(1, min(g.V, ncores))
@@ -244,27 +253,26 @@ def run_reference(args, rank, world):
         bins = np.array([rng.integers(NE)], np.int32)
         need = [v for v in views if v not in seg_cache]
         if need:
-            seg_cache.update(segments_per_view_cpu(w, np.array(need, np.int32)))
-        t = cpu_reference_sample(w, views, bins, ncores)
+            seg_cache.update(segments_per_view_cpu(w, tabs, np.array(need, np.int32)))
+        t = cpu_reference_sample(w, tabs, views, bins, ncores)
         if it >= args.warmup:
             times.append(t)
             segs.append(sum(seg_cache[int(v)] for v in views) * len(bins))
-    # one sampled (view, bin) call re-marches the view's rays for one bin;
-    # the full job is V x NE such calls over the whole stack's segments.
-    per_seg = np.sum(times) / np.sum(segs)           # s per segment per bin
-    total_segs = np.mean([seg_cache[v] for v in seg_cache]) * g.V
-    full_time = per_seg * total_segs * NE
-    value = total_segs / full_time / 1e9
-    ms = full_time * 1e3
+    per_seg_bin = np.sum(times) / np.sum(segs)       # s per segment per bin
+    value = 1.0 / (per_seg_bin * NE) / 1e9           # Gseg/s of the spectral projection
+    total_segs = np.mean(list(seg_cache.values())) * g.V
+    sample = f"{nviews} views x 1 of {NE} bins per step ({np.mean(times):.2f} s measured per step)"
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": "Gseg/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": w["name"], "sample": f"{nviews} views x 1 bin per step",
-                   "parallelism": f"cpu{ncores}"},
-        "cpu_baseline": {"value": value, "unit": "Gseg/s", "cores": ncores, "kind": "reference",
-                         "sample": f"{nviews} views x 1 of {NE} bins per step, extrapolated to "
-                                   f"{g.V} views x {NE} bins"},
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": float(np.mean(times)) * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": w["name"], "sample": sample, "parallelism": f"cpu{ncores}"},
+        "sample_seconds": [float(t) for t in times],
+        "extrapolated_full_step_ms": per_seg_bin * total_segs * NE * 1e3,
+        "cpu_baseline": {"value": value, "unit": "Gseg/s", "cores": ncores, "cpu_model": cpu_model(),
+                         "kind": "reference",
+                         "sample": sample + f"; the full step ({g.V} views x {NE} bins) extrapolates to "
+                                           f"{per_seg_bin * total_segs * NE:.0f} s"},
         "e2e": {"value": value, "unit": "Gseg/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
 
@@ -897,11 +905,11 @@ def run_ours(args, rank, world, local_rank):
             nviews = max(1, min(g.V, ncores))
             views = np.arange(0, g.V, max(1, g.V // nviews))[:nviews].astype(np.int32)
             bins = np.array([w["pdf"].shape[0] // 2], np.int32)
-            secs = cpu_reference_sample(w, views, bins, ncores)
+            secs = cpu_reference_sample(w, tabs, views, bins, ncores)
             per_view = nseg / g.V
             full = secs * (g.V / len(views)) * w["pdf"].shape[0]
             res["cpu_baseline"] = {"value": nseg / full / 1e9, "unit": "Gseg/s", "cores": ncores,
-                                   "kind": "reference",
+                                   "cpu_model": cpu_model(), "kind": "reference",
                                    "sample": f"reprojection() on {len(views)} views x 1 of "
                                              f"{w['pdf'].shape[0]} bins ({secs:.1f} s), "
                                              f"extrapolated to {g.V} views x all bins",

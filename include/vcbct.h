@@ -191,20 +191,23 @@ int vcbct_batch_configure(vcbct_batch* b, int strategy, int cols_per_block);
 int vcbct_projector_autotune(vcbct_projector* p, float* d_out, void* stream, int* chosen);
 int vcbct_batch_autotune(vcbct_batch* b, void* stream, int* chosen);
 
-/* Reference-named entry points (Release_CBCT_Projection_CM/reprojectionOnGPU.h).
+/* C-linkage twins of the reference-named projector entry points
+ * (Release_CBCT_Projection_CM/reprojectionOnGPU.h).  The reference names
+ * themselves, with the C++ linkage of the reference headers, are declared in
+ * vcbct_reference.h and forward here; these twins serve C and ctypes callers.
  * Same argument lists and meaning, including the ignored ones (ite,
  * reprojection_float, npf_double, projVolume, anglesRad, xalpha,
- * startProjNumber).  reprojectionOnGPU writes "<outputname>.raw" as the
- * reference does.  Errors are printed to stderr and leave the state
+ * startProjNumber).  vcbct_reprojectionOnGPU writes "<outputname>.raw" as
+ * the reference does.  Errors are printed to stderr and leave the state
  * unchanged (the reference exits with status 0 instead). */
-void initializeGPU(int reconSize, double reconScale, int reconSlices, double reconStep,
+void vcbct_initializeGPU(int reconSize, double reconScale, int reconSlices, double reconStep,
                    int projImgHeight, int projImgWidth, int totalProjNumber, double* cosTable,
                    double* sinTable, double* XcenterShift, double* YcenterShift, double x_reg,
                    double y_reg, double z_reg, double DETECTOR_PITCH_CM,
                    double DETECTOR_PITCH_CM_AT_ISO_CENT, double DIST_BTWN_SRC_AND_ISOCENT_CM,
                    double DETECTOR_PIXEL_NUM, int num_material);
-void terminateGPU(void);
-void reprojectionOnGPU(int ite, int reconSize, int reconSlices, unsigned short* reconImageshort,
+void vcbct_terminateGPU(void);
+void vcbct_reprojectionOnGPU(int ite, int reconSize, int reconSlices, unsigned short* reconImageshort,
                        float* reprojection_float, float* npf_double, float* projVolume,
                        double reconScale, double reconStep, int projImgWidth,
                        int projImgHeight, int startProjNumber, int endProjNumber,
@@ -236,9 +239,10 @@ int vcbct_projector_lengthproj(vcbct_projector* p, int ite, int start_view, int 
 int vcbct_ir_update(int N, int Z, double scale, const short* before, float* out, const float* npf,
                     const float* npf_re, double wbefore, double weight_tv, double weight_prior,
                     int on_device, void* stream);
-/* Reference-named forms, host arrays, same argument lists (the unused ones
- * are ignored as in the reference). */
-void lengthproj(int ite, int reconSize, int reconSlices, short* reconImageshort,
+/* C-linkage twins of lengthproj / IR_ImageCBCT (the reference names are in
+ * vcbct_reference.h): host arrays, same argument lists (the unused ones are
+ * ignored as in the reference). */
+void vcbct_lengthproj(int ite, int reconSize, int reconSlices, short* reconImageshort,
                 unsigned short* ProjImageshort, float* npf_float, unsigned short* projVolume,
                 double reconScale, double reconStep, int projImgWidth, int projImgHeight,
                 int startProjNumber, int endProjNumber, double* ProjAngle, double* cosTable,
@@ -246,7 +250,7 @@ void lengthproj(int ite, int reconSize, int reconSlices, short* reconImageshort,
                 double* xalpha, double DETECTOR_PITCH_CM, double DETECTOR_PITCH_CM_AT_ISO_CENT,
                 double DIST_BTWN_SRC_AND_ISOCENT_CM, double DETECTOR_PIXEL_NUM, double x_reg,
                 double y_reg, double z_reg);
-void IR_ImageCBCT(const int ite, int reconSize, int reconSlices, double reconScale,
+void vcbct_IR_ImageCBCT(const int ite, int reconSize, int reconSlices, double reconScale,
                   short* reconImageshort_before, float* reconImagefloat, float* npf_float,
                   float* npf_float_re, double wbefore, double weight_tv, double weight_prior,
                   const int thinout);
@@ -259,16 +263,21 @@ void IR_ImageCBCT(const int ite, int reconSize, int reconSlices, double reconSca
  * start-up.  Same result as vcbct_projector_create + set_spectrum +
  * load_volume (device) + forward (device), in one call.
  *   d_volume  device uint16 [Z][nmat][N][N];  d_out  device float [V][H][W]
- *   tables / attenuation / pdf are host arrays as for the object API.
+ *   tables / attenuation / pdf are host arrays as for the object API; they
+ *   are copied before the call returns, so the caller may free or reuse them
+ *   at once (page-locked or not).  The device work is asynchronous on
+ *   `stream`: d_volume must stay valid, and d_out is written, when the stream
+ *   reaches the call.
  * Scratch: one file-scope device array of VCBCT_NOALLOC_SCRATCH_BYTES, held by
  * every GPU that loads the library until the process exits.  Limits:
  * recon_size^2 * recon_slices <= 4177920 voxels (16 B each), n_views <= 1024,
- * n_bins <= 1024; larger requests return VCBCT_ERR_LIMIT before any device
- * work.  The first call on a device looks up the array's device address
- * (cudaGetSymbolAddress) with that device current; make that first call
- * before any stream capture.  Calls share the array: calls that overlap on
- * the GPU (different streams or threads, not ordered) race and corrupt each
- * other.  Asynchronous on `stream`. */
+ * n_bins <= 1024; larger requests return VCBCT_ERR_LIMIT, non-finite geometry
+ * or xfactor VCBCT_ERR_ARG, before any device work.  Each call looks up the
+ * array's device address (cudaGetSymbolAddress) with the caller's device
+ * current; the first call on a device also loads the library's kernels
+ * there, so make that first call before any stream capture.  Calls share the
+ * array: calls that overlap on the GPU (different streams or threads, not
+ * ordered) race and corrupt each other. */
 #define VCBCT_NOALLOC_SCRATCH_BYTES (64u * 1024u * 1024u)
 int vcbct_mbfpa_forward_noalloc(const vcbct_proj_geometry* g, const double* cos_table,
                                 const double* sin_table, const double* xcenter_shift,
@@ -490,16 +499,19 @@ typedef struct {
 
 int vcbct_fdk_deck_read(const char* txt_path, vcbct_fdk_deck* deck);
 
-/* Reference-named FDK entry points (R/filterSinogram.h:2-6,
- * R/reconstructImage.h:2-5).  Arrays are VOLUME-ONE style pointer tables over
- * contiguous storage (mallocMD.cpp:69-109).  prepareConstMap returns a
- * pointer table the caller frees with vcbct_free_const_map. */
-double** prepareConstMap(int projWidth, double DETECTOR_PITCH_CM_AT_ISO_CENT);
+/* C-linkage twins of the reference-named FDK entry points
+ * (R/filterSinogram.h:2-6, R/reconstructImage.h:2-5; the reference names are
+ * in vcbct_reference.h).  Arrays are VOLUME-ONE style pointer tables over
+ * contiguous storage (mallocMD.cpp:69-109).  vcbct_prepareConstMap returns a
+ * pointer table laid out as new2DArray's (one calloc'd block, one malloc'd
+ * row table), which the caller frees with vcbct_free_const_map or the
+ * reference's delete2DArray. */
+double** vcbct_prepareConstMap(int projWidth, double DETECTOR_PITCH_CM_AT_ISO_CENT);
 void vcbct_free_const_map(double** constMap, int projWidth);
-void filterSinogram(int projHeight, int projWidth, int sngrmHeight, float*** projVolume,
+void vcbct_filterSinogram(int projHeight, int projWidth, int sngrmHeight, float*** projVolume,
                     float*** fltdVoxData, double** constMap, double* xshift, double* yshift,
                     double DETECTOR_PITCH_CM_AT_ISO_CENT);
-void reconstructImage(int reconSize, int reconSlices, int zstart, double reconStep,
+void vcbct_reconstructImage(int reconSize, int reconSlices, int zstart, double reconStep,
                       double reconScale, double*** reconVoxData, char** maskData,
                       int projHeight, int projWidth, int sngrmHeight, float*** sngrmVoxData,
                       int xfactor, double* anglesRad, double* cosTable, double* sinTable,

@@ -6,6 +6,7 @@ reference file and line of every step.
 """
 from __future__ import annotations
 
+import contextlib
 import ctypes as C
 import os
 import subprocess
@@ -59,6 +60,25 @@ def _load(name: str) -> C.CDLL:
         lib = C.CDLL(path, mode=C.RTLD_LOCAL)
         _LIBS[name] = lib
         return lib
+
+
+@contextlib.contextmanager
+def quiet_stdout():
+    """Send the process's C-level stdout (fd 1) to /dev/null for the
+    duration: the reference's CPU code prints progress lines there, which
+    must not mix with a caller's own output (bench.py prints one JSON line)."""
+    libc = C.CDLL(None)
+    libc.fflush(None)
+    saved = os.dup(1)
+    devnull = os.open(os.devnull, os.O_WRONLY)
+    try:
+        os.dup2(devnull, 1)
+        yield
+    finally:
+        libc.fflush(None)
+        os.dup2(saved, 1)
+        os.close(saved)
+        os.close(devnull)
 
 
 def have_reference() -> bool:
@@ -269,14 +289,51 @@ def ref_mbfpa_views(g, tables, vol, mu, pdf, xfactor, views, bins, nthreads=0):
     return out, secs
 
 
+def ref_trig_tables(W, H, angles_rad, xshift, yshift, pdet, dpn):
+    """The reference's own prepareTrigonometricTable (P/misc.cpp:10-37)."""
+    L = ref_proj()
+    L.ref_proj_trig.restype = C.c_int
+    a = np.ascontiguousarray(angles_rad, np.float64)
+    xs = np.ascontiguousarray(xshift, np.float64)
+    ys = np.ascontiguousarray(yshift, np.float64)
+    V = a.shape[0]
+    out = [np.zeros(V, np.float64) for _ in range(4)]
+    L.ref_proj_trig(C.c_int(W), C.c_int(H), C.c_int(V), _ptr(a, _dp), _ptr(xs, _dp), _ptr(ys, _dp),
+                    C.c_double(pdet), C.c_double(dpn), *[_ptr(o, _dp) for o in out])
+    return tuple(out)
+
+
+def mbfpa_sampled(g, tables, vol, mu, pdf, xfactor, views, cols, want=("d",), **kw):
+    """mbfpa_forward on a sample of rays: the given views and detector
+    columns, every row (or the detector rows `rows=(j0, j1)`).  Returns each
+    output of `want` as [len(views)][H][len(cols)] (rows in the output
+    layout: flipped unless flip=False; rows outside a given range are 0)."""
+    views = np.ascontiguousarray(views, np.int32)
+    cols = np.asarray(cols, np.int32)
+    res = {k: np.zeros((len(views), g.H, len(cols)), np.float64 if k != "f" else np.float32) for k in want}
+    pos = {int(c): i for i, c in enumerate(cols)}
+    start = 0
+    while start < len(cols):
+        end = start
+        while end + 1 < len(cols) and cols[end + 1] == cols[end] + 1:
+            end += 1
+        c0, c1 = int(cols[start]), int(cols[end]) + 1
+        r = mbfpa_forward(g, tables, vol, mu, pdf, xfactor, views=views, cols=(c0, c1), want=want, **kw)
+        for k in want:
+            res[k][:, :, pos[c0]:pos[c0] + (c1 - c0)] = r[k][views][:, :, c0:c1]
+        start = end + 1
+    return res
+
+
 def ref_attenuation(workdir, spectrum, nmat, mat_type="human"):
     """Reference attenuation_coefficient (P/prior_weight_production.cpp:200)."""
     L = ref_proj()
     L.ref_attenuation.restype = C.c_int
     mu = np.zeros(1024 * nmat, np.float32)
     pdf = np.zeros(1024, np.float32)
-    NE = L.ref_attenuation(workdir.encode(), spectrum.encode(), C.c_int(nmat),
-                           mat_type.encode(), _ptr(mu, _fp), _ptr(pdf, _fp))
+    with quiet_stdout():
+        NE = L.ref_attenuation(workdir.encode(), spectrum.encode(), C.c_int(nmat),
+                               mat_type.encode(), _ptr(mu, _fp), _ptr(pdf, _fp))
     if NE <= 0:
         raise RuntimeError("reference attenuation_coefficient failed")
     return mu[: nmat * NE].reshape(nmat, NE).copy(), pdf[:NE].copy()

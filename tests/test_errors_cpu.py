@@ -97,6 +97,14 @@ def test_noalloc_limits_before_any_device_call(L):
     g = ProjGeometry(N=8, Z=4, s=0.1, step=0.1, W=8, H=8, V=2).to_c()
     assert L.vcbct_mbfpa_forward_noalloc(C.byref(g), dp, dp, dp, dp, buf, fp, fp, 2000, 1000.0, buf, None) == ARG
     assert L.vcbct_mbfpa_forward_noalloc(C.byref(g), dp, dp, dp, dp, None, fp, fp, 1, 1000.0, buf, None) == ARG
+    # non-finite xfactor or geometry: rejected, as vcbct_projector_set_spectrum / _create do
+    for xf in (float("inf"), float("-inf"), float("nan")):
+        assert L.vcbct_mbfpa_forward_noalloc(C.byref(g), dp, dp, dp, dp, buf, fp, fp, 1, xf, buf, None) == ARG
+    for field in ("z_reg", "x_reg", "recon_scale", "sad_cm"):
+        g = ProjGeometry(N=8, Z=4, s=0.1, step=0.1, W=8, H=8, V=2).to_c()
+        setattr(g, field, float("inf") if field in ("recon_scale", "sad_cm") else float("nan"))
+        assert L.vcbct_mbfpa_forward_noalloc(C.byref(g), dp, dp, dp, dp, buf, fp, fp, 1, 1000.0, buf, None) == ARG
+        assert "finite" in _msg(L) or "positive" in _msg(L)
 
 
 def test_standalone_kernels_validate_arguments(L):

@@ -33,7 +33,7 @@ def test_lengthproj_reference_named_entry_point(cuda):
     cosT, sinT, Xc, Yc = [np.ascontiguousarray(t, np.float64) for t in tabs]
     dp = C.POINTER(C.c_double)
     L = _native.lib()
-    L.lengthproj(0, g.N, g.Z, None, None, npf.ctypes.data_as(C.POINTER(C.c_float)), C.c_void_p(proj.ctypes.data),
+    L.vcbct_lengthproj(0, g.N, g.Z, None, None, npf.ctypes.data_as(C.POINTER(C.c_float)), C.c_void_p(proj.ctypes.data),
                  g.s, g.step, g.W, g.H, 0, g.V, None, cosT.ctypes.data_as(dp), sinT.ctypes.data_as(dp),
                  Xc.ctypes.data_as(dp), Yc.ctypes.data_as(dp), 0.0, None, g.pdet, g.piso, g.sad, g.dpn,
                  g.x_reg, g.y_reg, g.z_reg)

@@ -1,6 +1,8 @@
 """CPU-side checks of the C ABI library: it loads without a GPU and exports
-every entry point include/vcbct.h declares; argument validation fails with a
-status (no CUDA call is made on these paths)."""
+every entry point include/vcbct.h declares (the reference-named C++-linkage
+entry points of include/vcbct_reference.h are checked in test_dropin_cpu.py);
+argument validation fails with a status (no CUDA call is made on these
+paths)."""
 import ctypes as C
 import os
 import re
@@ -30,7 +32,7 @@ def _declared_symbols():
 def test_library_loads_and_exports_every_declared_symbol():
     L = N.lib()
     declared = _declared_symbols()
-    assert "reprojectionOnGPU" in declared and "vcbct_projector_forward" in declared
+    assert "vcbct_reprojectionOnGPU" in declared and "vcbct_projector_forward" in declared
     missing = [n for n in declared if not hasattr(L, n)]
     assert not missing, missing
     assert set(N.SIGNATURES) == declared

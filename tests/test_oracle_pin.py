@@ -93,3 +93,46 @@ def test_oracle_gpu_and_cpu_twins_differ_only_on_tie_rays():
     b = O.mbfpa_forward(g, tabs, vol, mu, pdf, 1000.0, ties=O.TIES_CPU, want=("f",))["f"]
     cols = np.unique(np.nonzero(a != b)[2])
     assert set(cols.tolist()) <= {g.H // 2}
+
+
+GOLD_C2 = os.path.join(GOLD, "c2_reference_sample.npz")
+GOLD_DECKS = os.path.join(GOLD, "shipped_decks_reference.npz")
+
+
+def test_oracle_is_the_reference_at_c2_scale():
+    """The restated CPU twin reproduces reprojection() bitwise on the C2
+    workload (25 cm, 512x512x200, half-fan, 90 bins; the committed fixture
+    from the reference's own code) on two row bands of the sampled columns."""
+    from measure.workloads import c2_workload, native_spectrum, native_tables
+    from tests.shipped import volume_checksum
+    gold = np.load(GOLD_C2)
+    w = c2_workload()
+    g = w["g"]
+    assert int(gold["volume_checksum"]) == volume_checksum(w["vol"])
+    mu, pdf = native_spectrum(w["spectrum_csv"])
+    tabs = native_tables(w)
+    views, cols = [int(v) for v in gold["views"]], gold["cols"]
+    for rows in ((0, 12), (194, 206)):
+        r = O.mbfpa_sampled(g, tabs, w["vol"], mu, pdf, w["xfactor"], views, cols, want=("f",),
+                            ties=O.TIES_CPU, with_leng=False, flip=False, exact=True, rows=rows)["f"]
+        assert np.array_equal(r[:, rows[0]:rows[1]], gold["out"][:, rows[0]:rows[1]])
+
+
+def test_oracle_is_the_reference_on_the_shipped_decks(tmp_path):
+    """The same on the reference's shipped decks (water-phantom slices with
+    the repeat-last-slice rule, the shipped 101-bin spectrum), with the
+    inputs built by the reference's own loader, spectrum and table code."""
+    from tests import shipped
+    if not (O.have_reference() and shipped.available()):
+        pytest.skip("reference objects or staged data not built")
+    gold = np.load(GOLD_DECKS)
+    pdir, _ = shipped.layout(str(tmp_path))
+    for tag, deck in (("d36", shipped.DECK_36), ("d360", shipped.DECK_360)):
+        d = shipped.projector_inputs(pdir, deck)
+        assert int(gold[f"{tag}_volume_checksum"]) == shipped.volume_checksum(d["vol"])
+        views, cols = [int(v) for v in gold[f"{tag}_views"]], gold[f"{tag}_cols"]
+        rows = (190, 210)
+        r = O.mbfpa_sampled(d["g"], d["tabs"], d["vol"], d["mu"], d["pdf"], d["xfactor"], views, cols,
+                            want=("f",), ties=O.TIES_CPU, with_leng=False, flip=False, exact=True,
+                            rows=rows)["f"]
+        assert np.array_equal(r[:, rows[0]:rows[1]], gold[f"{tag}_out"][:, rows[0]:rows[1]])

@@ -1,0 +1,161 @@
+"""Parity at the size the headline numbers are quoted on: the 25 cm water
+cylinder, 512x512x200 x 6, 360 views with the 160-pixel half-fan offset,
+400x400 detector, 90-bin spectrum; FDK to 270x270x200
+(measure/workloads.c2_workload, the workload bench.py times).
+
+Projections come from the host-to-host C ABI call (vcbct_projector_project:
+slab uploads, row-band launches, band downloads), which exercises the paths
+only large shapes reach.  They are compared on sampled rays (every row of 32
+detector columns: both edges, the central tie column W/2 and the column
+under the isocentre) of 8 views with the FP64 oracle, and of 4 views with the
+reference's own CPU projector (reprojection(), committed fixture
+tests/golden/c2_reference_sample.npz made by make_golden_scale.py).
+
+FDK: the library's filter and backprojection of those projections against
+the reference's filterSinogram + reconstructImage (oracle/_ref) on three
+whole slices (reference behaviour: no redundancy weights), and the
+half-fan-weighted variant bench.py times against the FP64 oracle.
+
+Bars: projections 1e-5 relative per detector pixel; filtered projections and
+the volume before the cast 1e-5 of their scale; short volume +-1 LSB.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+from measure.workloads import c2_workload, detector_sample_columns, native_spectrum, native_tables
+from tests.shipped import volume_checksum
+
+pytestmark = pytest.mark.gpu
+
+RTOL = 1e-5
+GOLD = os.path.join(os.path.dirname(__file__), "golden", "c2_reference_sample.npz")
+ORACLE_VIEWS = [0, 45, 90, 135, 181, 225, 270, 315]
+SLICES = (50, 100, 150)  # z = -10, 0, +10 cm: integer zstart for reconstructImage
+
+
+@pytest.fixture(scope="module")
+def c2(cuda):
+    from virtualcbct_b200 import Projector
+    w = c2_workload()
+    g = w["g"]
+    tabs = native_tables(w)
+    mu, pdf = native_spectrum(w["spectrum_csv"])
+    p = Projector(g.native(), *tabs)
+    p.set_spectrum(mu, pdf, w["xfactor"])
+    out = p.project(w["vol"])
+    p.close()
+    return dict(w=w, tabs=tabs, mu=mu, pdf=pdf, out=out)
+
+
+def _oracle_sample(c2, views, cols, **kw):
+    w = c2["w"]
+    return O.mbfpa_sampled(w["g"], c2["tabs"], w["vol"], c2["mu"], c2["pdf"], w["xfactor"], views, cols,
+                           exact=False, **kw)
+
+
+def test_c2_projection_matches_fp64_oracle(c2):
+    g = c2["w"]["g"]
+    cols = detector_sample_columns(g.W, 160)
+    assert len(ORACLE_VIEWS) * g.H * len(cols) >= 2048
+    ref = _oracle_sample(c2, ORACLE_VIEWS, cols, want=("d",))["d"]
+    gpu = c2["out"][ORACLE_VIEWS][:, :, cols].astype(np.float64)
+    assert np.isfinite(c2["out"]).all()
+    rel = np.abs(gpu - ref) / ref
+    assert rel.max() <= RTOL, f"max rel err {rel.max():.3e} at {np.unravel_index(rel.argmax(), rel.shape)}"
+
+
+def test_c2_projection_matches_reference_cpu_projector(c2):
+    """Against reprojection() itself (the committed fixture), times the cos^3
+    factor and with rows flipped to the GPU layout; rays where the
+    reference's GPU and CPU twins break a tie differently are compared with
+    the GPU-semantics oracle instead."""
+    gold = np.load(GOLD)
+    w = c2["w"]
+    assert int(gold["volume_checksum"]) == volume_checksum(w["vol"])
+    views, cols = [int(v) for v in gold["views"]], gold["cols"]
+    og = _oracle_sample(c2, views, cols, want=("d", "f"))
+    nl = _oracle_sample(c2, views, cols, want=("d",), with_leng=False)["d"]
+    cpu_ties = _oracle_sample(c2, views, cols, want=("f",), ties=O.TIES_CPU)["f"]
+    leng = og["d"] / nl
+    ref = gold["out"][:, ::-1, :].astype(np.float64) * leng
+    gpu = c2["out"][views][:, :, cols].astype(np.float64)
+    twin = og["f"] != cpu_ties
+    rel = np.abs(gpu - ref) / ref
+    assert rel[~twin].max() <= RTOL, f"max rel err {rel[~twin].max():.3e}"
+    rel_t = np.abs(gpu - og["d"]) / og["d"]
+    assert rel_t[twin].max(initial=0.0) <= RTOL
+
+
+def _fdk(w, **kw):
+    from virtualcbct_b200 import Fdk
+    fg = w["fdk"].native(**kw)
+    ang = np.deg2rad(w["angles_deg"])
+    return fg, ang, Fdk(fg, ang, w["xs_fdk"], np.zeros(fg.V))
+
+
+@pytest.mark.parametrize("method", ["direct", "bf16x3"])
+def test_c2_fdk_slices_match_reference(c2, method):
+    """filterSinogram + reconstructImage of the reference (oracle/_ref, all
+    host threads) on three whole slices of the 270x270x200 volume."""
+    import torch
+    from virtualcbct_b200 import FILTER_BF16X3, FILTER_DIRECT_F32
+    if not O.have_reference():
+        pytest.skip("reference CPU objects not built")
+    w = c2["w"]
+    fg, ang, F = _fdk(w, redundancy=0)
+    dev = torch.from_numpy(c2["out"]).cuda()
+    filt = F.filter(dev, method=FILTER_BF16X3 if method == "bf16x3" else FILTER_DIRECT_F32)
+    vf, vi = F.backproject(filt)
+    vf, vi = vf.cpu().numpy(), vi.cpu().numpy()
+    ref_filt = _ref_filter(c2, w, fg)
+    assert np.abs(filt.cpu().numpy() - ref_filt).max() <= 1e-5 * np.abs(ref_filt).max()
+    for k in SLICES:
+        z0 = fg.zstart + k * fg.step
+        assert abs(z0 - round(z0)) < 1e-9
+        ref, _ = O.ref_backproject(fg.N, 1, int(round(z0)), fg.step, fg.scale, ref_filt, fg.xfactor, ang,
+                                   w["xs_fdk"], fg.piso)
+        assert np.abs(ref).max() > 100  # the slice lies inside the cone
+        assert np.abs(vf[k] - ref[0]).max() <= 1e-5 * np.abs(ref).max()
+        d = np.abs(vi[k].astype(np.int32) - ref[0].astype(np.int16).astype(np.int32))
+        assert d.max() <= 1, f"slice {k}: {(d > 1).sum()} voxels differ by more than 1 LSB"
+
+
+_REF_FILT = {}
+
+
+def _ref_filter(c2, w, fg):
+    if "f" not in _REF_FILT:
+        _REF_FILT["f"] = O.ref_filter(c2["out"], w["xs_fdk"], np.zeros(fg.V), fg.piso)[0]
+    return _REF_FILT["f"]
+
+
+@pytest.mark.parametrize("method", ["direct", "bf16x3"])
+def test_c2_fdk_with_half_fan_weights_matches_fp64(c2, method):
+    """The weighted variant bench.py times (no reference counterpart): the
+    filter against the FP64 filter of w * (-log p) on 8 views, the
+    backprojection of the library's filtered stack against the FP64
+    backprojection of the same stack on three slices."""
+    import torch
+    from virtualcbct_b200 import FILTER_BF16X3, FILTER_DIRECT_F32, redundancy_weights
+    w = c2["w"]
+    fg, ang, F = _fdk(w)
+    assert fg.redundancy == 1
+    dev = torch.from_numpy(c2["out"]).cuda()
+    filt = F.filter(dev, method=FILTER_BF16X3 if method == "bf16x3" else FILTER_DIRECT_F32).cpu().numpy()
+    wts = redundancy_weights(fg, w["xs_fdk"])
+    views = np.array(ORACLE_VIEWS)
+    p = c2["out"][views].astype(np.float64) ** wts[views][:, None, :].astype(np.float64)
+    d64 = O.filter_sinogram(p.astype(np.float32), w["xs_fdk"][views], np.zeros(len(views)),
+                            O.fdk_consts(fg.piso), mode=1)
+    assert np.abs(filt[views] - d64).max() <= 1e-5 * np.abs(d64).max()
+    vf, vi = F.backproject(filt)
+    c = O.fdk_consts(fg.piso)
+    for k in SLICES:
+        z0 = int(round(fg.zstart + k * fg.step))
+        ref = O.backproject(fg.N, 1, z0, fg.step, fg.scale, filt, fg.xfactor, ang, w["xs_fdk"], c)
+        assert np.abs(vf[k] - ref[0]).max() <= 1e-5 * np.abs(ref).max()
+        d = np.abs(vi[k].astype(np.int32) - ref[0].astype(np.int16).astype(np.int32))
+        assert d.max() <= 1

@@ -3,15 +3,18 @@
 It exists for callers that cannot let a library allocate device memory (hosts
 that own all memory in a fixed arena, latency-critical pipelines, deployments
 that forbid allocation after start-up).  These tests call it through the C ABI
-and check it against the object API's forward projection on two calls in a
-row, with different volumes and sizes, so that anything left in its shared
-scratch array by the first call would show in the second.  This file is
-collected last on purpose."""
+and check it on two calls in a row, with different volumes and sizes (so that
+anything left in its shared scratch array by the first call would show in the
+second), against the FP64 oracle (the independent check) and against the
+object API's forward projection.  The host tables handed to each call are
+overwritten as soon as it returns: the entry point copies them before
+returning.  This file is collected last on purpose."""
 import ctypes as C
 
 import numpy as np
 import pytest
 
+import oracle as O
 from tests.cases import proj_case, spectrum
 from virtualcbct_b200 import Projector, _native as N
 
@@ -23,15 +26,19 @@ def _dp(a):
 
 
 def _noalloc(g, tabs, vol_dev, mu, pdf, out_dev, stream):
-    tabs = [np.ascontiguousarray(t, np.float64) for t in tabs]
-    mu = np.ascontiguousarray(mu, np.float32)
-    pdf = np.ascontiguousarray(pdf, np.float32)
+    tabs = [np.array(t, np.float64) for t in tabs]
+    mu = np.array(mu, np.float32)
+    pdf = np.array(pdf, np.float32)
     gc = g.to_c()
-    return N.lib().vcbct_mbfpa_forward_noalloc(
+    rc = N.lib().vcbct_mbfpa_forward_noalloc(
         C.byref(gc), *[t.ctypes.data_as(C.POINTER(C.c_double)) for t in tabs],
         C.c_void_p(vol_dev.data_ptr()), mu.ctypes.data_as(C.POINTER(C.c_float)),
         pdf.ctypes.data_as(C.POINTER(C.c_float)), int(pdf.shape[0]), 1000.0,
         C.c_void_p(out_dev.data_ptr()), C.c_void_p(stream.cuda_stream))
+    # the call has copied its host inputs: spoil them before the GPU runs
+    for a in (*tabs, mu, pdf):
+        a.fill(np.nan)
+    return rc
 
 
 @pytest.mark.gpu
@@ -54,6 +61,8 @@ def test_noalloc_forward_matches_object_api_on_two_calls(cuda):
         a, b = out.cpu().numpy(), ref.cpu().numpy()
         assert np.isfinite(a).all()
         assert np.max(np.abs(a - b) / b) <= RTOL
+        d64 = O.mbfpa_forward(g, tabs, vol, mu, pdf, 1000.0, exact=False, want=("d",))["d"]
+        assert np.max(np.abs(a - d64) / d64) <= RTOL
 
 
 def test_noalloc_rejects_sizes_beyond_its_scratch():

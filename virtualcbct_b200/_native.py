@@ -123,10 +123,10 @@ SIGNATURES = {
     "vcbct_projector_lengthproj": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, _vp, C.c_int, _vp, C.c_int, _vp]),
     "vcbct_ir_update": (C.c_int, [C.c_int, C.c_int, C.c_double, _vp, _vp, _vp, _vp, C.c_double, C.c_double,
                                   C.c_double, C.c_int, _vp]),
-    "lengthproj": (None, [C.c_int, C.c_int, C.c_int, _vp, _vp, _fp, _vp, C.c_double, C.c_double, C.c_int,
+    "vcbct_lengthproj": (None, [C.c_int, C.c_int, C.c_int, _vp, _vp, _fp, _vp, C.c_double, C.c_double, C.c_int,
                           C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, _dp, _dp, C.c_double, _dp, C.c_double,
                           C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double]),
-    "IR_ImageCBCT": (None, [C.c_int, C.c_int, C.c_int, C.c_double, _vp, _fp, _fp, _fp, C.c_double, C.c_double,
+    "vcbct_IR_ImageCBCT": (None, [C.c_int, C.c_int, C.c_int, C.c_double, _vp, _fp, _fp, _fp, C.c_double, C.c_double,
                             C.c_double, C.c_int]),
     "vcbct_proj_trig_tables": (C.c_int, [C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, C.c_double,
                                          C.c_double, _dp, _dp, _dp, _dp]),
@@ -146,21 +146,21 @@ SIGNATURES = {
     "vcbct_fdk_set_kernel": (C.c_int, [_vp, _dp]),
     "vcbct_fdk_filter": (C.c_int, [_vp, _vp, _vp, C.c_int, C.c_int, _vp]),
     "vcbct_fdk_backproject": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int, _vp]),
-    # reference-named entry points
-    "initializeGPU": (None, [C.c_int, C.c_double, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int,
+    # C-linkage twins of the reference-named entry points
+    "vcbct_initializeGPU": (None, [C.c_int, C.c_double, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int,
                              _dp, _dp, _dp, _dp, C.c_double, C.c_double, C.c_double, C.c_double,
                              C.c_double, C.c_double, C.c_double, C.c_int]),
-    "terminateGPU": (None, []),
-    "reprojectionOnGPU": (None, [C.c_int, C.c_int, C.c_int, _vp, _fp, _fp, _fp, C.c_double,
+    "vcbct_terminateGPU": (None, []),
+    "vcbct_reprojectionOnGPU": (None, [C.c_int, C.c_int, C.c_int, _vp, _fp, _fp, _fp, C.c_double,
                                  C.c_double, C.c_int, C.c_int, C.c_int, C.c_int, _dp, _dp, _dp,
                                  _dp, _dp, C.c_double, _dp, C.c_double, C.c_double, C.c_double,
                                  C.c_double, C.c_double, C.c_double, C.c_double, _fp, _fp,
                                  C.c_int, C.c_int, C.c_char_p]),
-    "prepareConstMap": (C.POINTER(_dp), [C.c_int, C.c_double]),
+    "vcbct_prepareConstMap": (C.POINTER(_dp), [C.c_int, C.c_double]),
     "vcbct_free_const_map": (None, [C.POINTER(_dp), C.c_int]),
-    "filterSinogram": (None, [C.c_int, C.c_int, C.c_int, _vp, _vp, C.POINTER(_dp), _dp, _dp,
+    "vcbct_filterSinogram": (None, [C.c_int, C.c_int, C.c_int, _vp, _vp, C.POINTER(_dp), _dp, _dp,
                               C.c_double]),
-    "reconstructImage": (None, [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, _vp, _vp,
+    "vcbct_reconstructImage": (None, [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, _vp, _vp,
                                 C.c_int, C.c_int, C.c_int, _vp, C.c_int, _dp, _dp, _dp, _dp,
                                 C.c_double]),
 }

@@ -803,7 +803,7 @@ extern "C" int vcbct_ir_update(int N, int Z, double scale, const short* before, 
 }
 
 // Reference-named entry points of the iterative reconstruction helpers.
-extern "C" void lengthproj(int ite, int reconSize, int reconSlices, short* reconImageshort,
+extern "C" void vcbct_lengthproj(int ite, int reconSize, int reconSlices, short* reconImageshort,
                            unsigned short* ProjImageshort, float* npf_float, unsigned short* projVolume,
                            double reconScale, double reconStep, int projImgWidth, int projImgHeight,
                            int startProjNumber, int endProjNumber, double* ProjAngle, double* cosTable,
@@ -828,7 +828,7 @@ extern "C" void lengthproj(int ite, int reconSize, int reconSlices, short* recon
     if (p) vcbct_projector_destroy(p);
 }
 
-extern "C" void IR_ImageCBCT(const int ite, int reconSize, int reconSlices, double reconScale,
+extern "C" void vcbct_IR_ImageCBCT(const int ite, int reconSize, int reconSlices, double reconScale,
                              short* reconImageshort_before, float* reconImagefloat, float* npf_float,
                              float* npf_float_re, double wbefore, double weight_tv, double weight_prior,
                              const int thinout)
@@ -1336,7 +1336,7 @@ std::mutex g_ref_mu;
 vcbct_projector* g_ref_proj = nullptr;
 }  // namespace
 
-extern "C" void initializeGPU(int reconSize, double reconScale, int reconSlices, double reconStep,
+extern "C" void vcbct_initializeGPU(int reconSize, double reconScale, int reconSlices, double reconStep,
                               int projImgHeight, int projImgWidth, int totalProjNumber,
                               double* cosTable, double* sinTable, double* XcenterShift,
                               double* YcenterShift, double x_reg, double y_reg, double z_reg,
@@ -1359,14 +1359,14 @@ extern "C" void initializeGPU(int reconSize, double reconScale, int reconSlices,
     g_ref_proj = p;
 }
 
-extern "C" void terminateGPU(void)
+extern "C" void vcbct_terminateGPU(void)
 {
     std::lock_guard<std::mutex> lk(g_ref_mu);
     vcbct_projector_destroy(g_ref_proj);
     g_ref_proj = nullptr;
 }
 
-extern "C" void reprojectionOnGPU(int ite, int reconSize, int reconSlices, unsigned short* reconImageshort,
+extern "C" void vcbct_reprojectionOnGPU(int ite, int reconSize, int reconSlices, unsigned short* reconImageshort,
                                   float* reprojection_float, float* npf_double, float* projVolume,
                                   double reconScale, double reconStep, int projImgWidth,
                                   int projImgHeight, int startProjNumber, int endProjNumber,
@@ -1713,7 +1713,7 @@ extern "C" int vcbct_fdk_backproject(vcbct_fdk* f, const float* filtered, float*
 
 // ------------------------------------------------- reference-named FDK API --
 
-extern "C" double** prepareConstMap(int projWidth, double piso)
+extern "C" double** vcbct_prepareConstMap(int projWidth, double piso)
 {
     if (projWidth <= 0) {
         std::fprintf(stderr, "ERROR: invalid projWidth for prepareConstMap\n");
@@ -1743,7 +1743,7 @@ extern "C" void vcbct_free_const_map(double** m, int projWidth)
     std::free(m);
 }
 
-extern "C" void filterSinogram(int projHeight, int projWidth, int sngrmHeight, float*** projVolume,
+extern "C" void vcbct_filterSinogram(int projHeight, int projWidth, int sngrmHeight, float*** projVolume,
                                float*** fltdVoxData, double** constMap, double* xshift,
                                double* yshift, double piso)
 {
@@ -1773,7 +1773,7 @@ extern "C" void filterSinogram(int projHeight, int projWidth, int sngrmHeight, f
     vcbct_fdk_destroy(f);
 }
 
-extern "C" void reconstructImage(int reconSize, int reconSlices, int zstart, double reconStep,
+extern "C" void vcbct_reconstructImage(int reconSize, int reconSlices, int zstart, double reconStep,
                                  double reconScale, double*** reconVoxData, char** maskData,
                                  int projHeight, int projWidth, int sngrmHeight,
                                  float*** sngrmVoxData, int xfactor, double* anglesRad,

@@ -9,6 +9,8 @@
 // every input and the output; the only device memory it touches besides those
 // is the fixed array below, which every GPU that loads the library holds
 // until the process exits.
+#include <cmath>
+#include <cstring>
 #include <mutex>
 
 #include "internal.h"
@@ -29,9 +31,14 @@ constexpr size_t kOffPdf = 224 * 1024;        // [NE] floats (<= 4 KiB)
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
-std::mutex g_mu;
-constexpr int kMaxDevices = 64;
-unsigned char* g_addr[kMaxDevices] = {};
+// Host staging of the caller's tables, laid out as the device table region.
+// It is ordinary pageable memory: a cudaMemcpyAsync from pageable host memory
+// to the device has consumed its source by the time it returns (the runtime
+// stages it), so once this entry point returns the caller may free or reuse
+// its host tables, whether or not they are page-locked.  The mutex keeps two
+// host threads from filling it at once.
+std::mutex g_stage_mu;
+unsigned char g_host_stage[kTableRegion];
 
 // ViewGeom records from the four caller tables (copied raw into scratch).
 __global__ void build_views_kernel(const double* raw, int V, ViewGeom* out)
@@ -70,8 +77,13 @@ extern "C" int vcbct_mbfpa_forward_noalloc(const vcbct_proj_geometry* g, const d
     if (!(g->recon_scale > 0) || !(g->recon_step > 0) || !(g->sad_cm > 0) || !(g->det_pitch_cm > 0) ||
         !(g->det_pitch_iso_cm > 0) || !(g->det_pixel_num > 0))
         return fail(VCBCT_ERR_ARG, "vcbct_mbfpa_forward_noalloc: pitches and distances must be positive");
-    if (n_bins <= 0 || n_bins > VCBCT_MAX_BINS || !(xfactor != 0.0))
-        return fail(VCBCT_ERR_ARG, "vcbct_mbfpa_forward_noalloc: n_bins must be in [1, 1024], xfactor non-zero");
+    if (!std::isfinite(g->recon_scale) || !std::isfinite(g->recon_step) || !std::isfinite(g->sad_cm) ||
+        !std::isfinite(g->det_pitch_cm) || !std::isfinite(g->det_pitch_iso_cm) || !std::isfinite(g->det_pixel_num) ||
+        !std::isfinite(g->x_reg) || !std::isfinite(g->y_reg) || !std::isfinite(g->z_reg))
+        return fail(VCBCT_ERR_ARG, "vcbct_mbfpa_forward_noalloc: geometry values must be finite");
+    if (n_bins <= 0 || n_bins > VCBCT_MAX_BINS || !(xfactor != 0.0) || !std::isfinite(xfactor))
+        return fail(VCBCT_ERR_ARG,
+                    "vcbct_mbfpa_forward_noalloc: n_bins must be in [1, 1024], xfactor finite and non-zero");
     if ((size_t)g->n_views > kMaxViews)
         return fail(VCBCT_ERR_LIMIT, "vcbct_mbfpa_forward_noalloc: at most 1024 views");
     const double vol_bytes = (double)g->recon_size * g->recon_size * g->recon_slices * sizeof(uint4);
@@ -80,22 +92,15 @@ extern "C" int vcbct_mbfpa_forward_noalloc(const vcbct_proj_geometry* g, const d
                     "vcbct_mbfpa_forward_noalloc: volume exceeds the fixed scratch (recon_size^2 * "
                     "recon_slices must be <= 4177920 voxels; use vcbct_projector_* for larger volumes)");
 
-    int dev = 0;
-    VCBCT_CUDA_TRY(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= kMaxDevices) return fail(VCBCT_ERR_LIMIT, "device ordinal out of range");
-    unsigned char* base = nullptr;
-    {
-        // once per device, with that device current: the host-side name of
-        // g_noalloc_scratch is not a device address
-        std::lock_guard<std::mutex> lk(g_mu);
-        if (!g_addr[dev]) {
-            void* p = nullptr;
-            cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-            if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
-            g_addr[dev] = static_cast<unsigned char*>(p);
-        }
-        base = g_addr[dev];
-    }
+    // The device address of the scratch array, looked up on every call with
+    // the caller's device current (the host-side name of g_noalloc_scratch is
+    // not a device address).  The lookup is a runtime table read; doing it per
+    // call keeps the address right after a cudaDeviceReset.  The first call on
+    // a device also loads this library's kernels there, which is why that
+    // first call belongs outside any stream capture.
+    void* sym = nullptr;
+    VCBCT_CUDA_TRY(cudaGetSymbolAddress(&sym, g_noalloc_scratch));
+    unsigned char* base = static_cast<unsigned char*>(sym);
     cudaStream_t st = (cudaStream_t)stream;
     const int V = g->n_views, NE = n_bins, nmat = g->num_material;
     double* raw = reinterpret_cast<double*>(base + kOffRaw);
@@ -107,12 +112,21 @@ extern "C" int vcbct_mbfpa_forward_noalloc(const vcbct_proj_geometry* g, const d
 
     // Every region read below is fully rewritten by this call, so the
     // contents left by a previous call need no clearing.
-    VCBCT_CUDA_TRY(cudaMemcpyAsync(raw, cos_table, sizeof(double) * V, cudaMemcpyHostToDevice, st));
-    VCBCT_CUDA_TRY(cudaMemcpyAsync(raw + V, sin_table, sizeof(double) * V, cudaMemcpyHostToDevice, st));
-    VCBCT_CUDA_TRY(cudaMemcpyAsync(raw + 2 * V, xcenter_shift, sizeof(double) * V, cudaMemcpyHostToDevice, st));
-    VCBCT_CUDA_TRY(cudaMemcpyAsync(raw + 3 * V, ycenter_shift, sizeof(double) * V, cudaMemcpyHostToDevice, st));
-    VCBCT_CUDA_TRY(cudaMemcpyAsync(mu_raw, attenuation, sizeof(float) * nmat * NE, cudaMemcpyHostToDevice, st));
-    VCBCT_CUDA_TRY(cudaMemcpyAsync(dpdf, pdf, sizeof(float) * NE, cudaMemcpyHostToDevice, st));
+    {
+        std::lock_guard<std::mutex> lk(g_stage_mu);
+        double* hraw = reinterpret_cast<double*>(g_host_stage + kOffRaw);
+        std::memcpy(hraw, cos_table, sizeof(double) * V);
+        std::memcpy(hraw + V, sin_table, sizeof(double) * V);
+        std::memcpy(hraw + 2 * V, xcenter_shift, sizeof(double) * V);
+        std::memcpy(hraw + 3 * V, ycenter_shift, sizeof(double) * V);
+        std::memcpy(g_host_stage + kOffMuRaw, attenuation, sizeof(float) * nmat * NE);
+        std::memcpy(g_host_stage + kOffPdf, pdf, sizeof(float) * NE);
+        VCBCT_CUDA_TRY(cudaMemcpyAsync(raw, hraw, sizeof(double) * 4 * V, cudaMemcpyHostToDevice, st));
+        VCBCT_CUDA_TRY(cudaMemcpyAsync(mu_raw, g_host_stage + kOffMuRaw, sizeof(float) * nmat * NE,
+                                       cudaMemcpyHostToDevice, st));
+        VCBCT_CUDA_TRY(cudaMemcpyAsync(dpdf, g_host_stage + kOffPdf, sizeof(float) * NE, cudaMemcpyHostToDevice,
+                                       st));
+    }
     build_views_kernel<<<(V + 127) / 128, 128, 0, st>>>(raw, V, views);
     VCBCT_CUDA_TRY(cudaGetLastError());
     build_mu8_kernel<<<(NE * 8 + 255) / 256, 256, 0, st>>>(mu_raw, nmat, NE, xfactor, mu8);
