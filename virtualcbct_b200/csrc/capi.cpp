@@ -690,7 +690,9 @@ static int projector_adjoint(vcbct_projector* p, const float* d_L, const float* 
     if (p->NE <= 0) return fail(VCBCT_ERR_STATE, "no spectrum set");
     cudaStream_t st = (cudaStream_t)stream;
     const auto& g = p->g;
-    const size_t pk = (size_t)g.num_material * g.recon_size * g.recon_size * g.recon_slices * sizeof(float);
+    // gradient planes of element pairs (ceil(nmat / 2) x 2 floats per voxel)
+    const size_t pk = (size_t)((g.num_material + 1) / 2) * 2 * g.recon_size * g.recon_size * g.recon_slices *
+                      sizeof(float);
     VCBCT_CUDA_TRY(p->grad_pk.ensure(pk));
     VCBCT_CUDA_TRY(cudaMemsetAsync(p->grad_pk.p, 0, pk, st));
     AdjointArgs a{};
@@ -1432,7 +1434,10 @@ struct vcbct_fdk {
     DevBuf bviews;    // BpView[V]
     DevBuf wts;       // float [V][W] redundancy weights (optional)
     DevBuf in, mid, outv, outs, work;
+    DevBuf bpkeep;    // per-block view masks of the backprojection
     int have_wts = 0;
+    int b_ready = 0;          // the tensor-core filter's Toeplitz planes are split in `work`
+    void* b_at = nullptr;     // ... at this address
 };
 
 extern "C" void vcbct_fdk_default_geometry(vcbct_fdk_geometry* g)
@@ -1504,6 +1509,7 @@ static int upload_kernel(vcbct_fdk* f)
             hT[(size_t)k * W + m] = (float)(f->h[(size_t)m * W + k] + (m == k ? coeff : 0.0));
     VCBCT_CUDA_TRY(f->hT.ensure(hT.size() * sizeof(float)));
     VCBCT_CUDA_TRY(cudaMemcpy(f->hT.p, hT.data(), hT.size() * sizeof(float), cudaMemcpyHostToDevice));
+    f->b_ready = 0;  // the split Toeplitz planes follow the kernel
     return VCBCT_OK;
 }
 
@@ -1665,15 +1671,22 @@ extern "C" int vcbct_fdk_filter(vcbct_fdk* f, const float* proj, float* filtered
                                             g.proj_width, st));
     } else if (method == VCBCT_FILTER_BF16X3) {
         VCBCT_CUDA_TRY(f->work.ensure(ramp_gemm_workspace_bytes(g.n_views, g.proj_height, g.proj_width)));
+        if (f->work.p != f->b_at) {
+            f->b_ready = 0;
+            f->b_at = f->work.p;
+        }
         VCBCT_CUDA_TRY(launch_ramp_gemm_bf16x3(din, dout, f->hT.as<float>(), f->fviews.as<FilterView>(), w,
                                                pitch, (float)g.sad_cm, g.n_views, g.proj_height,
-                                               g.proj_width, f->work.p, st));
+                                               g.proj_width, f->work.p, &f->b_ready, st));
     } else {
         return fail(VCBCT_ERR_ARG, "unknown filter method");
     }
     if (!on_device) {
         VCBCT_CUDA_TRY(cudaMemcpyAsync(filtered, dout, n * sizeof(float), cudaMemcpyDeviceToHost, st));
         VCBCT_CUDA_TRY(cudaStreamSynchronize(st));
+        if (method == VCBCT_FILTER_BF16X3 &&
+            ramp_gemm_error_flag(f->work.p, g.n_views, g.proj_height, g.proj_width, st) != 0)
+            return fail(VCBCT_ERR_DEVICE, "tensor-core filter: a bounded wait ran out (output invalid)");
     }
     return VCBCT_OK;
 }
@@ -1702,7 +1715,8 @@ extern "C" int vcbct_fdk_backproject(vcbct_fdk* f, const float* filtered, float*
             di = f->outs.as<short>();
         }
     }
-    VCBCT_CUDA_TRY(launch_backproject(f->fp, f->bviews.as<BpView>(), din, df, di, st));
+    VCBCT_CUDA_TRY(f->bpkeep.ensure(backproject_workspace_bytes(f->fp)));
+    VCBCT_CUDA_TRY(launch_backproject(f->fp, f->bviews.as<BpView>(), din, df, di, f->bpkeep.as<unsigned>(), st));
     if (!on_device) {
         if (vol_f32) VCBCT_CUDA_TRY(cudaMemcpyAsync(vol_f32, df, nv * sizeof(float), cudaMemcpyDeviceToHost, st));
         if (vol_i16) VCBCT_CUDA_TRY(cudaMemcpyAsync(vol_i16, di, nv * sizeof(short), cudaMemcpyDeviceToHost, st));

@@ -6,6 +6,7 @@
 #include "internal.h"
 
 #include <climits>
+#include <cstdlib>
 
 namespace vcbct {
 namespace {
@@ -81,6 +82,45 @@ __global__ void __launch_bounds__(256) filter_direct_kernel(
     }
 }
 
+// Packed pairs of floats for Blackwell's f32x2 arithmetic: one instruction
+// for two elements, each rounded exactly as the scalar instruction would
+// round it.
+typedef unsigned long long f32x2;
+__device__ __forceinline__ f32x2 f2pack(float a, float b)
+{
+    f32x2 r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+    return r;
+}
+__device__ __forceinline__ void f2unpack(f32x2 r, float& a, float& b)
+{
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(r));
+}
+__device__ __forceinline__ f32x2 ffma2(f32x2 a, f32x2 b, f32x2 c)
+{
+    f32x2 r;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+    return r;
+}
+__device__ __forceinline__ f32x2 fmul2(f32x2 a, f32x2 b)
+{
+    f32x2 r;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ f32x2 fsub2(f32x2 a, f32x2 b)
+{
+    f32x2 r;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ f32x2 fadd2_rd(f32x2 a, f32x2 b)  // rounded toward -inf, as __fadd_rd
+{
+    f32x2 r;
+    asm("add.rm.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+
 // ----------------------------------------------------------- backprojection --
 // One thread per (x, y) voxel column and a chunk of ZB slices (register
 // accumulators).  Per (x, y, view) the detector column coordinate U, its
@@ -91,14 +131,16 @@ __global__ void __launch_bounds__(256) filter_direct_kernel(
 // reference's edge rules and its weight quirk (the column weight is frac(U),
 // not frac(UUU), reconstructImage.cpp:80-83).
 // Register cap (minimum resident 256-thread blocks per SM) and slices per
-// thread.  The gathers are latency-bound, so occupancy pays: with 4 x 8 warp
-// tiles, 8 slices at 6 blocks (40 registers, 48 warps per SM) measured on
-// B200 as fast as 16 slices at 5 blocks on 270x270x200 from 360 half-fan
-// views (3.39 vs 3.37 ms) and 10-19 % faster where more of the volume lies in
-// the cone (512x512x400 / x100 from 720 views of 800x800: 55 vs 61 ms, 22 vs
-// 27 ms); 12, 20 slices and 16 at 4 blocks were slower.
+// thread.  The gathers are latency-bound, so occupancy pays, but the packed
+// f32x2 slice loop needs register pairs: at 6 blocks (40 registers) it
+// spills in the loop (1e8 local loads on 270x270x200 from 360 half-fan
+// views), at 5 (48 registers) it does not and is faster on B200 (3.30 vs
+// 3.36 ms, the volume bitwise the same).  With the scalar loop, 8 slices at
+// 6 blocks measured as fast as 16 at 5 (3.39 vs 3.37 ms) and 10-19 % faster
+// where more of the volume lies in the cone; 12, 20 slices and 16 at 4
+// blocks were slower.
 #ifndef VCBCT_BP_MIN_BLOCKS
-#define VCBCT_BP_MIN_BLOCKS 6
+#define VCBCT_BP_MIN_BLOCKS 5
 #endif
 #ifndef VCBCT_BP_TILE
 #define VCBCT_BP_TILE 4  // warp tile width in voxel columns (4, 8, 16 or 32)
@@ -106,10 +148,71 @@ __global__ void __launch_bounds__(256) filter_direct_kernel(
 #ifndef VCBCT_BP_ZB
 #define VCBCT_BP_ZB 8
 #endif
+// Per (backprojection block, view): may any column of the block's 32 x 8
+// tile take the view in backproject_kernel?  U, g = 1 / (L2 pitch) and the
+// row coordinate H/2 + z g are linear-fractional in (x, y) with a positive
+// denominator, so over the tile's rectangle they take their extremes at its
+// four corners.  A view whose corner values put every column left of column
+// 0 or right of column W - 1 (the column test UU < 0 || UU > W - 1), or every
+// slice of the block above or below the detector (the row test), is
+// dropped; the margin is far above FP64 rounding, so a dropped view is one
+// every column of the tile would have skipped.  One warp per (block, 32
+// views): bit th & 31 of word th >> 5 of the block's mask.
 template <int ZB>
-__global__ void __launch_bounds__(256, VCBCT_BP_MIN_BLOCKS) backproject_kernel(
+__global__ void __launch_bounds__(256) bp_cull_kernel(FdkParams f, const BpView* __restrict__ views,
+                                                      int gx, int gy, int nblocks, unsigned* __restrict__ keep)
+{
+    constexpr double kMargin = 1e-3;  // detector pixels
+    const int nwords = (f.V + 31) >> 5;
+    const long wid = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (wid >= (long)nblocks * nwords) return;
+    const int lane = threadIdx.x & 31;
+    const int blk = (int)(wid / nwords), word = (int)(wid % nwords);
+    const int bx = blk % gx, by = (blk / gx) % gy, bz = blk / (gx * gy);
+    const int th = word * 32 + lane;
+    bool keep_it = false;
+    if (th < f.V) {
+        const double pitch = f.piso * f.mpn / f.W;
+        const double cp = (double)f.N / 2.0 - 0.5;
+        const double inv_sad = 1.0 / f.sad;
+        const int xa = bx * 32, xb = min(xa + 31, f.N - 1);
+        const int ya = by * 8, yb = min(ya + 7, f.N - 1);
+        const double zza = f.zstart + (double)(bz * ZB) * f.step;
+        const double zzl = zza + (double)(ZB - 1) * f.step;
+        const BpView bv = views[th];
+        double umin = 1e300, umax = -1e300, gmin = 1e300, gmax = -1e300;
+        bool ok = true;
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            const double xx = (((c & 1) ? xb : xa) - cp) * f.scale;
+            const double yy = -(((c & 2) ? yb : ya) - cp) * f.scale;
+            const double X = xx * bv.cs + yy * bv.sn;
+            const double L2 = 1.0 - (-xx * bv.sn + yy * bv.cs) * inv_sad;
+            ok = ok && L2 > 1e-3;
+            const double g = 1.0 / (L2 * pitch);
+            const double u = bv.ushift + X * g;
+            umin = fmin(umin, u);
+            umax = fmax(umax, u);
+            gmin = fmin(gmin, g);
+            gmax = fmax(gmax, g);
+        }
+        keep_it = true;
+        if (ok) {
+            const bool left = umax < -kMargin, right = umin >= (double)f.W + kMargin;
+            const double last_max = (double)(f.H / 2) + fmax(zzl * gmin, zzl * gmax);
+            const double first_min = (double)(f.H / 2) + fmin(zza * gmin, zza * gmax);
+            const bool below = last_max < -1.0 - kMargin, above = first_min > (double)f.H + 1.0 + kMargin;
+            keep_it = !(left || right || below || above);
+        }
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, keep_it);
+    if (lane == 0) keep[wid] = m;
+}
+
+template <int ZB, int MINB>
+__global__ void __launch_bounds__(256, MINB) backproject_kernel(
     FdkParams f, const BpView* __restrict__ views, const float* __restrict__ filt,
-    float* __restrict__ vol_f32, short* __restrict__ vol_i16)
+    float* __restrict__ vol_f32, short* __restrict__ vol_i16, const unsigned* __restrict__ keep)
 {
     // each warp takes a TW x (32 / TW) tile of the block's 32 x 8 columns:
     // the detector's column-edge and cone-edge lines split fewer warps than
@@ -120,9 +223,9 @@ __global__ void __launch_bounds__(256, VCBCT_BP_MIN_BLOCKS) backproject_kernel(
     const int x = blockIdx.x * 32 + (threadIdx.y % WX) * TW + (threadIdx.x % TW);
     const int y = blockIdx.y * 8 + (threadIdx.y / WX) * TH + (threadIdx.x / TW);
     const int z0 = blockIdx.z * ZB;
-    if (x >= f.N || y >= f.N) return;
+    const bool valid = x < f.N && y < f.N;
     const double R = (double)(f.N - 1) / 2.0;
-    const bool inmask = ((double)y - R) * ((double)y - R) + ((double)x - R) * ((double)x - R) <= R * R;
+    const bool inmask = valid && ((double)y - R) * ((double)y - R) + ((double)x - R) * ((double)x - R) <= R * R;
     float acc[ZB];
 #pragma unroll
     for (int i = 0; i < ZB; i++) acc[i] = 0.0f;
@@ -143,13 +246,27 @@ __global__ void __launch_bounds__(256, VCBCT_BP_MIN_BLOCKS) backproject_kernel(
         const double hi = (double)(H / 2) + fmax(fmax(a, b), fmax(c, d));
         if (rm < f.sad && (hi < -1.0 || lo > (double)H + 1.0)) seen = false;
     }
+    // Views this block's tile of columns can see (bp_cull_kernel): a view
+    // that contributes nothing to any column of the tile is dropped for the
+    // whole block.  The kept views are visited in order, so the accumulation
+    // order and the volume are those of visiting every view.
+    extern __shared__ unsigned s_views[];  // bit th set: view th is kept
+    {
+        const int nwords = (f.V + 31) >> 5;
+        const int blk = (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+        for (int i = threadIdx.y * 32 + threadIdx.x; i < nwords; i += 256)
+            s_views[i] = __ldg(keep + (size_t)blk * nwords + i);
+    }
+    const double cp = (double)f.N / 2.0 - 0.5;
+    const double inv_sad = 1.0 / f.sad;
+    __syncthreads();
+    if (!valid) return;
     const bool full = z0 + ZB <= f.Z;  // every slice of the block exists
     if (inmask && seen) {
-        const double cp = (double)f.N / 2.0 - 0.5;
         const double xx = (x - cp) * f.scale;
         const double yy = -(y - cp) * f.scale;
-        const double inv_sad = 1.0 / f.sad;
         for (int th = 0; th < f.V; th++) {
+            if (!((s_views[th >> 5] >> (th & 31)) & 1u)) continue;
             const BpView bv = views[th];
             const double cs = bv.cs, sn = bv.sn;
             // FP64 detector coordinates of this column (:76-83)
@@ -179,20 +296,31 @@ __global__ void __launch_bounds__(256, VCBCT_BP_MIN_BLOCKS) backproject_kernel(
             const float* pv = filt + (size_t)th * H * W;
             if (!lastc && full && zeta0 >= 0.0 && zeta0 + (double)(ZB - 1) * f.step * g < (double)H - 2.5) {
                 // every slice of the block projects between detector rows 0
-                // and H - 2: no bounds or last-row tests
+                // and H - 2: no bounds or last-row tests.  Two slices per
+                // step in packed f32x2 arithmetic (each element rounded as
+                // the scalar operation would round it: the same volume, half
+                // the floating-point instructions)
                 const float* pc = pv + UU;
+                const f32x2 dz2 = f2pack(dz, dz), zf2b = f2pack(Zf, Zf);
+                const f32x2 cw0_2 = f2pack(cw0, cw0), cw1_2 = f2pack(cw1, cw1), w2_2 = f2pack(w2, w2);
+                const f32x2 big2 = f2pack(12582912.0f, 12582912.0f), one2 = f2pack(1.0f, 1.0f);
 #pragma unroll
-                for (int i = 0; i < ZB; i++) {
-                    const float zfrac = fmaf((float)i, dz, Zf);
-                    const float tq = __fadd_rd(zfrac, 12582912.0f);
-                    const float fl = tq - 12582912.0f;
-                    const int NZ = Zi + (__float_as_int(tq) - 0x4B400000);
-                    const float wz = zfrac - fl;
-                    const float* r0p = pc + NZ * W;
-                    const float* r1p = r0p + W;
-                    const float s0 = fmaf(cw1, __ldg(r0p + 1), cw0 * __ldg(r0p));
-                    const float s1 = fmaf(cw1, __ldg(r1p + 1), cw0 * __ldg(r1p));
-                    acc[i] = fmaf(fmaf(wz, s1, (1.0f - wz) * s0), w2, acc[i]);
+                for (int i = 0; i < ZB; i += 2) {
+                    const f32x2 zfrac = ffma2(f2pack((float)i, (float)(i + 1)), dz2, zf2b);
+                    const f32x2 tq = fadd2_rd(zfrac, big2);
+                    const f32x2 wz = fsub2(zfrac, fsub2(tq, big2));
+                    float tqa, tqb;
+                    f2unpack(tq, tqa, tqb);
+                    const float* ra = pc + (Zi + (__float_as_int(tqa) - 0x4B400000)) * W;
+                    const float* rb = pc + (Zi + (__float_as_int(tqb) - 0x4B400000)) * W;
+                    const f32x2 s0 = ffma2(cw1_2, f2pack(__ldg(ra + 1), __ldg(rb + 1)),
+                                           fmul2(cw0_2, f2pack(__ldg(ra), __ldg(rb))));
+                    const f32x2 s1 = ffma2(cw1_2, f2pack(__ldg(ra + W + 1), __ldg(rb + W + 1)),
+                                           fmul2(cw0_2, f2pack(__ldg(ra + W), __ldg(rb + W))));
+                    const f32x2 v = ffma2(wz, s1, fmul2(fsub2(one2, wz), s0));
+                    f32x2 a2 = f2pack(acc[i], acc[i + 1]);
+                    a2 = ffma2(v, w2_2, a2);
+                    f2unpack(a2, acc[i], acc[i + 1]);
                 }
                 continue;
             }
@@ -274,13 +402,32 @@ cudaError_t launch_filter_direct(const float* proj, float* out, const float* hT,
     return cudaGetLastError();
 }
 
+size_t backproject_workspace_bytes(const FdkParams& f)
+{
+    constexpr int ZB = VCBCT_BP_ZB;
+    const size_t nblocks = (size_t)((f.N + 31) / 32) * ((f.N + 7) / 8) * ((f.Z + ZB - 1) / ZB);
+    return nblocks * (size_t)((f.V + 31) / 32) * sizeof(unsigned);
+}
+
 cudaError_t launch_backproject(const FdkParams& f, const BpView* d_views, const float* filt,
-                               float* vol_f32, short* vol_i16, cudaStream_t st)
+                               float* vol_f32, short* vol_i16, unsigned* keep, cudaStream_t st)
 {
     constexpr int ZB = VCBCT_BP_ZB;
     dim3 block(32, 8);
     dim3 grid((f.N + 31) / 32, (f.N + 7) / 8, (f.Z + ZB - 1) / ZB);
-    backproject_kernel<ZB><<<grid, block, 0, st>>>(f, d_views, filt, vol_f32, vol_i16);
+    const int nblocks = (int)(grid.x * grid.y * grid.z);
+    const long nwarps = (long)nblocks * ((f.V + 31) / 32);
+    bp_cull_kernel<ZB><<<(unsigned)((nwarps * 32 + 255) / 256), 256, 0, st>>>(f, d_views, (int)grid.x, (int)grid.y,
+                                                                               nblocks, keep);
+    const size_t smem = (size_t)((f.V + 31) / 32) * sizeof(unsigned);
+    // resident blocks per SM (the register cap): VCBCT_BP_MIN_BLOCKS by
+    // default, 5 or 6 through the environment variable of the same name
+    int minb = VCBCT_BP_MIN_BLOCKS;
+    if (const char* e = std::getenv("VCBCT_BP_MIN_BLOCKS")) minb = std::atoi(e) == 6 ? 6 : 5;
+    if (minb == 5)
+        backproject_kernel<ZB, 5><<<grid, block, smem, st>>>(f, d_views, filt, vol_f32, vol_i16, keep);
+    else
+        backproject_kernel<ZB, 6><<<grid, block, smem, st>>>(f, d_views, filt, vol_f32, vol_i16, keep);
     return cudaGetLastError();
 }
 

@@ -110,7 +110,7 @@ struct AdjointArgs {
     const float* grad_out;   // [V][H][W] d loss / d intensity
     const float* L_in;       // [V][H][W][nmat] path integrals of the forward, or
                              // nullptr: recompute them (first march)
-    float* grad_planes;      // [nmat][N*N*Z] float accumulator, z fastest
+    float* grad_planes;      // [ceil(nmat/2)][N*N*Z][2] float accumulator, element pairs, z fastest
     int* err_flag;
     int cols_per_block;
     int y0, y1;              // scatter only into volume rows iy in [y0, y1) (y1 <= y0: all)
@@ -153,14 +153,23 @@ struct BpView {
     float dbeta;     // half the neighbouring angular gap (:45-71)
     float pad;
 };
+// keep: backproject_workspace_bytes(f) of device scratch (the per-block view
+// masks, rewritten by every launch).
+size_t backproject_workspace_bytes(const FdkParams& f);
 cudaError_t launch_backproject(const FdkParams& f, const BpView* d_views, const float* filt,
-                               float* vol_f32, short* vol_i16, cudaStream_t st);
+                               float* vol_f32, short* vol_i16, unsigned* keep, cudaStream_t st);
 
-// BF16 3-term split tensor-core ramp filter (tcgen05).
+// BF16 3-term split tensor-core ramp filter (tcgen05).  The workspace holds
+// the split Toeplitz planes: with *b_ready set they are taken as already
+// split from hT into this workspace and are not redone; the launch sets it
+// once it has queued the split (b_ready may be null: split every call).
 size_t ramp_gemm_workspace_bytes(int V, int H, int W);
 cudaError_t launch_ramp_gemm_bf16x3(const float* proj, float* out, const float* hT,
                                     const FilterView* views, const float* wts, float pitch,
                                     float sad, int V, int H, int W, void* workspace,
-                                    cudaStream_t st);
+                                    int* b_ready, cudaStream_t st);
+// The kernel's fault flag (1 after a bounded wait ran out; its output is then
+// invalid), read synchronously on `st`; -1 if it cannot be read.
+int ramp_gemm_error_flag(void* workspace, int V, int H, int W, cudaStream_t st);
 
 }  // namespace vcbct

@@ -532,18 +532,22 @@ struct AccumF32 : PairSums<M> {
 // reduction per element and lane; the L2 applies them per sector).
 template <int M>
 struct Scatter {
-    float* __restrict__ grad;   // [nmat][N*N*Z]
+    float* __restrict__ grad;   // [ceil(nmat/2)][N*N*Z][2]: element pairs (2q, 2q+1) interleaved
     size_t plane;               // N*N*Z
     int nmat;
-    float g[8];
+    float g[8];                 // zero beyond nmat
     unsigned lo, span;          // packed indices [lo, lo + span) of the strip scattered into
     __device__ __forceinline__ void operator()(int idx, float len)
     {
         if ((unsigned)idx - lo >= span) return;
-        float* p = grad + idx;
+        // one 8-byte vector reduction per element pair: half the reduction
+        // instructions of per-element planes, and a warp's 32 lanes (about 11
+        // consecutive z cells) touch 3-4 sectors per pair plane
 #pragma unroll
-        for (int k = 0; k < M; k++)
-            if (k < nmat) atomicAdd(p + k * plane, g[k] * len);
+        for (int q = 0; q < M / 2; q++)
+            if (2 * q < nmat)
+                atomicAdd(reinterpret_cast<float2*>(grad) + (size_t)q * plane + idx,
+                          make_float2(g[2 * q] * len, g[2 * q + 1] * len));
     }
     __device__ __forceinline__ void lanes(bool p, int idx, float len)
     {
@@ -1332,10 +1336,11 @@ __global__ void unpack_grad_kernel(const float* __restrict__ src, int N, int Z, 
     const int m = blockIdx.z / zt;
     const int x0 = blockIdx.x * 32, y = blockIdx.y, z0 = (blockIdx.z % zt) * 32;
     const size_t NN = (size_t)N * N;
-    const float* plane = src + (size_t)m * NN * Z;
+    // element m is slot m % 2 of pair plane m / 2 (see Scatter)
+    const float* plane = src + (size_t)(m / 2) * NN * Z * 2 + (m % 2);
     for (int xx = threadIdx.y; xx < 32; xx += 8) {
         const int x = x0 + xx, z = z0 + threadIdx.x;
-        tile[threadIdx.x][xx] = (x < N && z < Z) ? plane[((size_t)y * N + x) * Z + z] : 0.0f;
+        tile[threadIdx.x][xx] = (x < N && z < Z) ? plane[(((size_t)y * N + x) * Z + z) * 2] : 0.0f;
     }
     __syncthreads();
     for (int zz = threadIdx.y; zz < 32; zz += 8) {

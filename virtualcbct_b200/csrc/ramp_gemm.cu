@@ -9,13 +9,19 @@
 // with i + j <= 2 (G0B0 G0B1 G1B0 G0B2 G1B1 G2B0) are accumulated in FP32 in
 // tensor memory, which keeps about 24 significant bits.
 //
-// One CTA computes a 128-row x NT-column output tile (NT <= 512; wider
-// detectors take several column tiles): warp 0 issues
-// TMA loads into a 3-stage shared-memory ring (128B swizzle, K-major), warp 1
-// issues tcgen05.mma from a single thread into a 128 x NT FP32 accumulator in
-// tensor memory, warps 2-5 read the accumulator back (tcgen05.ld), apply the
-// cosine factor and store.  No cluster multicast is used.  Every mbarrier
-// wait is bounded; on timeout the kernel raises a device flag and returns.
+// One CTA computes a 128-row x NT-column output tile (NT <= 512, a multiple
+// of 32; wider detectors take several column tiles), K tile by K tile.
+// split_a_kernel first writes the three A planes of -logf(p) to global
+// memory; the split Toeplitz planes (B) are made once per kernel.  In the
+// GEMM, warp 0 streams by TMA, per K tile, the tile's three A planes (a
+// 2-stage ring) and then B planes 2, 1, 0, each as two column halves (a
+// 4-stage ring), so each B plane of a K tile is loaded once and multiplied by
+// every A plane it pairs with; warp 1 issues tcgen05.mma from a single thread
+// into two 128 x NT/2 FP32 accumulators in tensor memory (columns 0 and 256);
+// warps 2-9 read them back (tcgen05.ld), apply the cosine factor and store.
+// No cluster multicast is used.  Every mbarrier wait is bounded; on timeout
+// the kernel raises a device flag, stops issuing, waits (bounded) for its
+// loads in flight and returns; its output is then invalid.
 #include <cuda.h>
 #include <cuda_bf16.h>
 
@@ -26,11 +32,8 @@ namespace {
 
 constexpr int BM = 128;           // rows per CTA tile (UMMA M)
 constexpr int BK = 64;            // K per stage: 64 bf16 = one 128-byte swizzle row
-constexpr int kThreads = 192;     // 6 warps
+constexpr int kThreads = 320;     // 10 warps
 constexpr long long kWaitCycles = 4000000000LL;  // ~2 s at 1.9 GHz
-
-// (a-plane, b-plane) of the six split products, smallest terms first
-__constant__ int c_terms[6][2] = {{2, 0}, {1, 1}, {0, 2}, {1, 0}, {0, 1}, {0, 0}};
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p)
 {
@@ -121,30 +124,95 @@ __device__ __forceinline__ void umma_commit(uint64_t* bar)
                  : "memory");
 }
 
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v)
+// x = x0 + x1 + x2 in bfloat16 (round to nearest even at each step).
+__device__ __forceinline__ void split3(float x, __nv_bfloat16& a, __nv_bfloat16& b, __nv_bfloat16& c)
 {
-    uint32_t r[32];
+    a = __float2bfloat16_rn(x);
+    const float r1 = x - __bfloat162float(a);
+    b = __float2bfloat16_rn(r1);
+    const float r2 = r1 - __bfloat162float(b);
+    c = __float2bfloat16_rn(r2);
+}
+
+// The same split of two values at once, each plane packed as bf16x2 (low
+// half = first value): one cvt.rn.bf16x2.f32 per plane and a packed f32x2
+// subtraction per residual, each element rounded exactly as split3 rounds it.
+__device__ __forceinline__ uint32_t bf16x2_rn(float lo, float hi)
+{
+    uint32_t r;
+    asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(hi), "f"(lo));
+    return r;
+}
+__device__ __forceinline__ unsigned long long bf16x2_widen(uint32_t v)  // -> {lo, hi} as f32x2
+{
+    unsigned long long r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "r"(v << 16), "r"(v & 0xffff0000u));
+    return r;
+}
+__device__ __forceinline__ unsigned long long fsub2(unsigned long long a, unsigned long long b)
+{
+    unsigned long long r;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ void split3x2(float x, float y, uint32_t& p0, uint32_t& p1, uint32_t& p2)
+{
+    unsigned long long v;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(v) : "f"(x), "f"(y));
+    p0 = bf16x2_rn(x, y);
+    const unsigned long long r1 = fsub2(v, bf16x2_widen(p0));
+    float r1x, r1y;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(r1x), "=f"(r1y) : "l"(r1));
+    p1 = bf16x2_rn(r1x, r1y);
+    const unsigned long long r2 = fsub2(r1, bf16x2_widen(p1));
+    float r2x, r2y;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(r2x), "=f"(r2y) : "l"(r2));
+    p2 = bf16x2_rn(r2x, r2y);
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v)
+{
+    uint32_t r[16];
     asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
-          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
-          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
         : "r"(taddr));
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-    for (int i = 0; i < 32; i++) v[i] = __uint_as_float(r[i]);
+    for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
 }
 
 struct GemmArgs {
     float* out;
     const FilterView* views;
     float pitch, sad;
-    int M, H, W, NT, Kp, ktiles, stages;  // NT: output columns per CTA (blockIdx.y selects the column tile)
-    int vec;                              // rows of `out` 16-byte aligned (W % 4 == 0, aligned base)
+    int M, H, W, NT, Kp, ktiles;  // NT: output columns per CTA (blockIdx.y selects the column tile)
+    int vec;                      // rows of `out` 16-byte aligned (W % 4 == 0, aligned base)
     int* err;
 };
+
+constexpr int kEpiWarps = 8;                    // warps 2-9: the epilogue, two per TMEM lane quarter
+static_assert(kThreads == 64 + 32 * kEpiWarps, "warp 0 TMA, warp 1 MMA, the rest epilogue");
+constexpr uint32_t kHalfCol = 256;              // TMEM column of the second column half
+constexpr int kAStages = 2;                     // A ring: the three planes of one K tile each
+constexpr int kBStages = 4;                     // B ring: one column half of one plane of one K tile each
+constexpr uint32_t kAPlaneBytes = BM * BK * 2;  // one 128 x 64 bf16 plane, 16 KiB
+constexpr uint32_t kAStageBytes = 3 * kAPlaneBytes;
+
+// Shared-memory footprint of a CTA with NT output columns (before 1 KiB
+// alignment slack): A ring, B ring of NT/2-row halves, mbarriers, TMEM slot.
+__host__ __device__ constexpr size_t gemm_smem_bytes(int NT)
+{
+    return (size_t)kAStages * kAStageBytes + (size_t)kBStages * (NT / 2) * BK * 2 +
+           8 * (2 * kAStages + 2 * kBStages + 1) + 16;
+}
+
+// Warp-uniform bounded wait (tcgen05.ld needs converged warps).
+__device__ __forceinline__ bool warp_wait(uint64_t* bar, uint32_t phase, int* err)
+{
+    return __all_sync(0xffffffffu, mbar_wait(bar, phase, err));
+}
 
 __global__ void __launch_bounds__(kThreads, 1)
 ramp_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, GemmArgs g)
@@ -152,27 +220,30 @@ ramp_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant_
     extern __shared__ uint8_t smem_raw[];
     // 1024-byte alignment for the 128-byte swizzle atoms
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-    const int S = g.stages;
-    const uint32_t a_bytes = BM * BK * 2;
-    const uint32_t b_bytes = (uint32_t)g.NT * BK * 2;
-    uint8_t* stage_base = smem;
-    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + (size_t)S * (a_bytes + b_bytes));
-    uint64_t* full = bars;
-    uint64_t* empty = bars + S;
-    uint64_t* accum = bars + 2 * S;
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * S + 1);
+    const int NH = g.NT / 2;                      // columns of one B half (a multiple of 16)
+    const uint32_t bh_bytes = (uint32_t)NH * BK * 2;
+    uint8_t* abuf = smem;                         // kAStages x 3 planes
+    uint8_t* bbuf = smem + kAStages * kAStageBytes;  // kBStages x one B half
+    uint64_t* bars = reinterpret_cast<uint64_t*>(bbuf + (size_t)kBStages * bh_bytes);
+    uint64_t* a_full = bars;
+    uint64_t* a_empty = bars + kAStages;
+    uint64_t* b_full = bars + 2 * kAStages;
+    uint64_t* b_empty = bars + 2 * kAStages + kBStages;
+    uint64_t* accum = bars + 2 * kAStages + 2 * kBStages;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(accum + 1);
 
     const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
     const int m0 = blockIdx.x * BM;
     const int n0 = blockIdx.y * g.NT;
-    const int N1 = g.NT < 256 ? g.NT : 256;
-    const int N2 = g.NT - N1;
-    const int nk = 6 * g.ktiles;
 
     if (threadIdx.x == 0) {
-        for (int s = 0; s < S; s++) {
-            mbar_init(&full[s], 1);
-            mbar_init(&empty[s], 1);
+        for (int s = 0; s < kAStages; s++) {
+            mbar_init(&a_full[s], 1);
+            mbar_init(&a_empty[s], 1);
+        }
+        for (int s = 0; s < kBStages; s++) {
+            mbar_init(&b_full[s], 1);
+            mbar_init(&b_empty[s], 1);
         }
         mbar_init(accum, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -188,47 +259,72 @@ ramp_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant_
     const uint32_t taddr = *tmem_slot;
 
     if (warp == 0 && lane == 0) {
-        // TMA producer
-        for (int kb = 0; kb < nk; kb++) {
-            const int s = kb % S;
-            if (kb >= S && !mbar_wait(&empty[s], ((kb / S) - 1) & 1, g.err)) break;
-            const int term = kb / g.ktiles, kt = kb % g.ktiles;
-            uint8_t* sa = stage_base + (size_t)s * (a_bytes + b_bytes);
-            uint8_t* sb = sa + a_bytes;
-            mbar_expect_tx(&full[s], a_bytes + b_bytes);
-            tma_load_3d(sa, &tmA, &full[s], kt * BK, m0, c_terms[term][0]);
-            tma_load_3d(sb, &tmB, &full[s], kt * BK, n0, c_terms[term][1]);
-            tma_load_3d(sb + (size_t)(g.NT / 2) * BK * 2, &tmB, &full[s], kt * BK, n0 + g.NT / 2, c_terms[term][1]);
-        }
-    } else if (warp == 1 && lane == 0) {
-        // MMA issuer
-        const uint32_t id1 = idesc_bf16(BM, N1);
-        const uint32_t id2 = idesc_bf16(BM, N2 > 0 ? N2 : 16);
+        // TMA producer.  Per K tile: the three A planes (one A stage), then
+        // the B planes 2, 1, 0, each as two column halves (six B stages) --
+        // the order the MMA thread consumes them in.
+        int na = 0, nb = 0;  // stages issued
         bool ok = true;
-        for (int kb = 0; kb < nk && ok; kb++) {
-            const int s = kb % S;
-            ok = mbar_wait(&full[s], (kb / S) & 1, g.err);
-            if (!ok) break;
-            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const uint32_t sa = smem_u32(stage_base + (size_t)s * (a_bytes + b_bytes));
-            const uint32_t sb = sa + a_bytes;
-#pragma unroll
-            for (int kk = 0; kk < BK / 16; kk++) {
-                const uint64_t ad = sw128_desc(sa + kk * 32);
-                const uint32_t acc = (kb > 0 || kk > 0) ? 1u : 0u;
-                umma_bf16(taddr, ad, sw128_desc(sb + kk * 32), id1, acc);
-                if (N2 > 0) umma_bf16(taddr + (uint32_t)N1, ad, sw128_desc(sb + N1 * 128 + kk * 32), id2, acc);
+        for (int kt = 0; kt < g.ktiles && ok; kt++) {
+            const int sa = kt % kAStages;
+            if (kt >= kAStages && !(ok = mbar_wait(&a_empty[sa], ((kt / kAStages) - 1) & 1, g.err))) break;
+            uint8_t* da = abuf + (size_t)sa * kAStageBytes;
+            mbar_expect_tx(&a_full[sa], kAStageBytes);
+            for (int i = 0; i < 3; i++) tma_load_3d(da + i * kAPlaneBytes, &tmA, &a_full[sa], kt * BK, m0, i);
+            na = kt + 1;
+            for (int q = 0; q < 6; q++) {
+                const int kb = kt * 6 + q, s = kb % kBStages;
+                if (kb >= kBStages && !(ok = mbar_wait(&b_empty[s], ((kb / kBStages) - 1) & 1, g.err))) break;
+                const int plane = 2 - q / 2, h = q % 2;
+                mbar_expect_tx(&b_full[s], bh_bytes);
+                tma_load_3d(bbuf + (size_t)s * bh_bytes, &tmB, &b_full[s], kt * BK, n0 + h * NH, plane);
+                nb = kb + 1;
             }
-            umma_commit(&empty[s]);
+        }
+        // no load may still be in flight into this CTA's shared memory when it
+        // exits: wait (bounded) for the last stages issued
+        for (int k = na - kAStages; k < na; k++)
+            if (k >= 0) mbar_wait(&a_full[k % kAStages], (k / kAStages) & 1, g.err);
+        for (int k = nb - kBStages; k < nb; k++)
+            if (k >= 0) mbar_wait(&b_full[k % kBStages], (k / kBStages) & 1, g.err);
+    } else if (warp == 1 && lane == 0) {
+        // MMA issuer: per K tile and B plane j, each column half against A
+        // planes 2 - j .. 0, so the products (2,0) (1,1) (0,2) (1,0) (0,1)
+        // (0,0) are all formed, smaller terms of a tile before larger ones.
+        const uint32_t idesc = idesc_bf16(BM, NH);
+        bool ok = true, fresh[2] = {true, true};
+        for (int kt = 0; kt < g.ktiles && ok; kt++) {
+            const int sa = kt % kAStages;
+            if (!(ok = mbar_wait(&a_full[sa], (kt / kAStages) & 1, g.err))) break;
+            const uint32_t abase = smem_u32(abuf + (size_t)sa * kAStageBytes);
+            for (int q = 0; q < 6 && ok; q++) {
+                const int kb = kt * 6 + q, s = kb % kBStages;
+                if (!(ok = mbar_wait(&b_full[s], (kb / kBStages) & 1, g.err))) break;
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const int j = 2 - q / 2, h = q % 2;
+                const uint32_t sb = smem_u32(bbuf + (size_t)s * bh_bytes);
+                const uint32_t dcol = taddr + (uint32_t)h * kHalfCol;
+                for (int i = 2 - j; i >= 0; i--) {
+                    const uint32_t sai = abase + (uint32_t)i * kAPlaneBytes;
+#pragma unroll
+                    for (int kk = 0; kk < BK / 16; kk++) {
+                        umma_bf16(dcol, sw128_desc(sai + kk * 32), sw128_desc(sb + kk * 32), idesc, fresh[h] ? 0u : 1u);
+                        fresh[h] = false;
+                    }
+                }
+                umma_commit(&b_empty[s]);
+            }
+            umma_commit(&a_empty[sa]);
         }
         umma_commit(accum);
     } else if (warp >= 2) {
-        // epilogue: TMEM -> registers -> cosine factor -> global
-        const int q = warp % 4;  // TMEM lane quarter this warp may access
+        // epilogue: TMEM -> registers -> cosine factor -> global; two warps
+        // per TMEM lane quarter (a warp may access lanes 32 (warp % 4) ..),
+        // each taking every other 16-column chunk; logical column c lies at
+        // TMEM column c (first half) or kHalfCol + c - NT/2 (second half)
+        const int q = warp % 4;
+        const int half = (warp - 2) / 4;
         const int row = m0 + 32 * q + lane;
-        // warp-uniform outcome: tcgen05.ld needs the whole warp converged
-        const bool ready = __all_sync(0xffffffffu, mbar_wait(accum, 0, g.err));
-        if (ready) {
+        if (warp_wait(accum, 0, g.err)) {
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             float pos2 = 0.0f, xcs = 0.0f;
             if (row < g.M) {
@@ -240,28 +336,28 @@ ramp_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant_
             // cosine factor sad / sqrt(sad^2 + pos1^2 + pos2^2) from the
             // reciprocal square root (2 ulp), stored 16 bytes at a time
             const float sad = g.sad, base2 = fmaf(pos2, pos2, sad * sad);
-            for (int c = 0; c < g.NT; c += 32) {
-                float v32[32];
-                tmem_ld32(taddr + ((uint32_t)(32 * q) << 16) + (uint32_t)c, v32);
+            for (int c = 16 * half; c < g.NT; c += 32) {
+                float v16[16];
+                const uint32_t col = c < NH ? (uint32_t)c : kHalfCol + (uint32_t)(c - NH);
+                tmem_ld16(taddr + ((uint32_t)(32 * q) << 16) + col, v16);
                 const int mb = n0 + c;
                 if (row < g.M && mb < g.W) {
                     float* o = g.out + (size_t)row * g.W + mb;
 #pragma unroll
-                    for (int i = 0; i < 32; i++) {
+                    for (int i = 0; i < 16; i++) {
                         const float pos1 = fabsf(xcs + (float)(mb + i)) * g.pitch;
-                        v32[i] *= sad * rsqrtf(fmaf(pos1, pos1, base2));
+                        v16[i] *= sad * rsqrtf(fmaf(pos1, pos1, base2));
                     }
-                    // columns of this tile only (the last 32-column chunk may
-                    // run past NT into unwritten accumulator columns)
+                    // columns of this tile and of the detector only
                     const int lim = min(g.W - mb, g.NT - c);
-                    if (g.vec && lim >= 32) {
+                    if (g.vec && lim >= 16) {
 #pragma unroll
-                        for (int i = 0; i < 32; i += 4)
-                            *reinterpret_cast<float4*>(o + i) = make_float4(v32[i], v32[i + 1], v32[i + 2], v32[i + 3]);
+                        for (int i = 0; i < 16; i += 4)
+                            *reinterpret_cast<float4*>(o + i) = make_float4(v16[i], v16[i + 1], v16[i + 2], v16[i + 3]);
                     } else {
 #pragma unroll
-                        for (int i = 0; i < 32; i++)
-                            if (i < lim) o[i] = v32[i];
+                        for (int i = 0; i < 16; i++)
+                            if (i < lim) o[i] = v16[i];
                     }
                 }
             }
@@ -270,47 +366,52 @@ ramp_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant_
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     if (warp == 1) {
+        // every MMA this CTA issued has completed before its accumulator is
+        // released (the commit above arrives on `accum` once they have)
+        warp_wait(accum, 0, g.err);
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(512));
     }
 }
 
-// x = x0 + x1 + x2 in bfloat16 (round to nearest even at each step).
-__device__ __forceinline__ void split3(float x, __nv_bfloat16& a, __nv_bfloat16& b, __nv_bfloat16& c)
-{
-    a = __float2bfloat16_rn(x);
-    const float r1 = x - __bfloat162float(a);
-    b = __float2bfloat16_rn(r1);
-    const float r2 = r1 - __bfloat162float(b);
-    c = __float2bfloat16_rn(r2);
-}
-
 // A planes [3][M][Kp]: split of g = -logf(p) (times the redundancy weight).
-// grid (M, ceil(Kp / 512)), block 128: one detector row per block, four
-// consecutive columns per thread, written as 8-byte groups (Kp is a multiple
-// of 64, so every group is aligned).
-__global__ void split_a_kernel(const float* __restrict__ proj, const float* __restrict__ wts, int M, int H, int W,
-                               int Kp, __nv_bfloat16* __restrict__ planes)
+// grid (M, ceil(Kp / 1024)), block 128: one detector row per block, eight
+// consecutive columns per thread (two 16-byte loads where the row allows),
+// each plane written as one 16-byte group (Kp is a multiple of 64).
+__global__ void __launch_bounds__(128) split_a_kernel(const float* __restrict__ proj, const float* __restrict__ wts,
+                                                      int M, int H, int W, int Kp, int vec,
+                                                      __nv_bfloat16* __restrict__ planes)
 {
     const int r = blockIdx.x;
-    const int k0 = 4 * (blockIdx.y * blockDim.x + threadIdx.x);
+    const int k0 = 8 * (blockIdx.y * blockDim.x + threadIdx.x);
     if (k0 >= Kp) return;
     const float* pr = proj + (size_t)r * W;
     const float* wr = wts ? wts + (size_t)(r / H) * W : nullptr;
-    __align__(8) __nv_bfloat16 a[4], b[4], c[4];
+    float x[8];
+    if (vec && k0 + 8 <= W) {
+        const float4 a = __ldg(reinterpret_cast<const float4*>(pr + k0));
+        const float4 b = __ldg(reinterpret_cast<const float4*>(pr + k0 + 4));
+        x[0] = a.x; x[1] = a.y; x[2] = a.z; x[3] = a.w;
+        x[4] = b.x; x[5] = b.y; x[6] = b.z; x[7] = b.w;
 #pragma unroll
-    for (int q = 0; q < 4; q++) {
-        const int k = k0 + q;
-        float g = 0.0f;
-        if (k < W) {
-            g = -logf(__ldg(pr + k));
-            if (wr) g *= __ldg(wr + k);
-        }
-        split3(g, a[q], b[q], c[q]);
+        for (int q = 0; q < 8; q++) x[q] = -logf(x[q]);
+    } else {
+#pragma unroll
+        for (int q = 0; q < 8; q++) x[q] = (k0 + q < W) ? -logf(__ldg(pr + k0 + q)) : 0.0f;
     }
+    if (wr) {
+#pragma unroll
+        for (int q = 0; q < 8; q++)
+            if (k0 + q < W) x[q] *= __ldg(wr + k0 + q);
+    }
+    uint4 p0, p1, p2;
+    split3x2(x[0], x[1], p0.x, p1.x, p2.x);
+    split3x2(x[2], x[3], p0.y, p1.y, p2.y);
+    split3x2(x[4], x[5], p0.z, p1.z, p2.z);
+    split3x2(x[6], x[7], p0.w, p1.w, p2.w);
     const size_t plane = (size_t)M * Kp, o = (size_t)r * Kp + k0;
-    *reinterpret_cast<uint2*>(planes + o) = *reinterpret_cast<const uint2*>(a);
-    *reinterpret_cast<uint2*>(planes + plane + o) = *reinterpret_cast<const uint2*>(b);
-    *reinterpret_cast<uint2*>(planes + 2 * plane + o) = *reinterpret_cast<const uint2*>(c);
+    *reinterpret_cast<uint4*>(planes + o) = p0;
+    *reinterpret_cast<uint4*>(planes + plane + o) = p1;
+    *reinterpret_cast<uint4*>(planes + 2 * plane + o) = p2;
 }
 
 // B planes [3][Np][Kp]: B[m][k] = hT[k][m] (ramp kernel + diagonal coefficient).
@@ -360,10 +461,13 @@ bool make_map(CUtensorMap* map, void* base, int rows, int Kp, int box_rows)
 }
 
 // Output columns are split into ntiles tiles of NT <= 512 columns (one
-// tensor-memory accumulator of 128 x NT FP32 each); B is padded to
-// Np = ntiles * NT rows.
+// tensor-memory accumulator of 128 x NT FP32 each; NT a multiple of 32, so a
+// column half is a legal MMA width); B is padded to Np = ntiles * NT rows.
+// The workspace holds the split A planes, the split Toeplitz planes (a
+// function of the kernel and W only, split once per kernel) and the error
+// flag.
 struct Layout {
-    int M, Np, NT, ntiles, Kp, stages;
+    int M, Np, NT, ntiles, Kp;
     size_t a_off, b_off, err_off, total, smem;
 };
 
@@ -373,16 +477,13 @@ Layout layout_for(int V, int H, int W)
     L.M = V * H;
     const int n16 = (W + 15) / 16 * 16;
     L.ntiles = (n16 + 511) / 512;
-    L.NT = ((n16 + L.ntiles - 1) / L.ntiles + 15) / 16 * 16;
+    L.NT = ((n16 + L.ntiles - 1) / L.ntiles + 31) / 32 * 32;
     L.Np = L.ntiles * L.NT;
     L.Kp = (W + BK - 1) / BK * BK;
-    const size_t stage = (size_t)BM * BK * 2 + (size_t)L.NT * BK * 2;
-    L.stages = (int)((225 * 1024 - 1024 - 128) / stage);
-    if (L.stages > 3) L.stages = 3;
-    L.smem = 1024 + (size_t)L.stages * stage + 8 * (2 * L.stages + 1) + 16;
-    L.a_off = 0;
-    L.b_off = (3 * (size_t)L.M * L.Kp * 2 + 1023) / 1024 * 1024;
-    L.err_off = L.b_off + (3 * (size_t)L.Np * L.Kp * 2 + 1023) / 1024 * 1024;
+    L.smem = 1024 + gemm_smem_bytes(L.NT);
+    L.b_off = 0;
+    L.a_off = (3 * (size_t)L.Np * L.Kp * 2 + 1023) / 1024 * 1024;
+    L.err_off = L.a_off + (3 * (size_t)L.M * L.Kp * 2 + 1023) / 1024 * 1024;
     L.total = L.err_off + 256;
     return L;
 }
@@ -393,29 +494,33 @@ size_t ramp_gemm_workspace_bytes(int V, int H, int W) { return layout_for(V, H, 
 
 cudaError_t launch_ramp_gemm_bf16x3(const float* proj, float* out, const float* hT, const FilterView* views,
                                     const float* wts, float pitch, float sad, int V, int H, int W, void* workspace,
-                                    cudaStream_t st)
+                                    int* b_ready, cudaStream_t st)
 {
     if (W < 16 || W > 4096) return cudaErrorInvalidValue;
     const Layout L = layout_for(V, H, W);
-    if (L.stages < 2) return cudaErrorInvalidValue;
+    if (L.smem > 227 * 1024) return cudaErrorInvalidValue;
     uint8_t* ws = static_cast<uint8_t*>(workspace);
     __nv_bfloat16* ap = reinterpret_cast<__nv_bfloat16*>(ws + L.a_off);
     __nv_bfloat16* bp = reinterpret_cast<__nv_bfloat16*>(ws + L.b_off);
     int* err = reinterpret_cast<int*>(ws + L.err_off);
     cudaError_t e = cudaMemsetAsync(err, 0, sizeof(int), st);
     if (e != cudaSuccess) return e;
-    {
-        split_a_kernel<<<dim3((unsigned)L.M, (unsigned)((L.Kp + 511) / 512)), 128, 0, st>>>(proj, wts, L.M, H, W,
-                                                                                         L.Kp, ap);
+    if (!b_ready || !*b_ready) {
+        // the Toeplitz planes change only with the kernel: split once
         const size_t nb = (size_t)L.Np * L.Kp;
         split_b_kernel<<<(unsigned)((nb + 255) / 256), 256, 0, st>>>(hT, W, L.Np, L.Kp, bp);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        if (b_ready) *b_ready = 1;
     }
+    const int avec = (W % 4 == 0 && (reinterpret_cast<uintptr_t>(proj) & 15) == 0) ? 1 : 0;
+    split_a_kernel<<<dim3((unsigned)L.M, (unsigned)((L.Kp + 1023) / 1024)), 128, 0, st>>>(proj, wts, L.M, H, W, L.Kp,
+                                                                                      avec, ap);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
     CUtensorMap tmA, tmB;
     if (!make_map(&tmA, ap, L.M, L.Kp, BM) || !make_map(&tmB, bp, L.Np, L.Kp, L.NT / 2))
         return cudaErrorInvalidValue;
     const int vec = (W % 4 == 0 && (reinterpret_cast<uintptr_t>(out) & 15) == 0) ? 1 : 0;
-    GemmArgs g{out, views, pitch, sad, L.M, H, W, L.NT, L.Kp, L.Kp / BK, L.stages, vec, err};
+    GemmArgs g{out, views, pitch, sad, L.M, H, W, L.NT, L.Kp, L.Kp / BK, vec, err};
     e = cudaFuncSetAttribute(ramp_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem);
     if (e != cudaSuccess) return e;
     ramp_gemm_kernel<<<dim3((L.M + BM - 1) / BM, L.ntiles), kThreads, L.smem, st>>>(tmA, tmB, g);
