@@ -38,7 +38,7 @@ import numpy as np
 from virtualcbct_b200 import FILTER_BF16X3, FILTER_DIRECT_F32, Batch, Fdk, FdkGeometry, Projector, ProjGeometry
 from virtualcbct_b200 import attenuation_table, phantoms, trig_tables
 
-DATA = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data")
+DATA = os.path.join(os.path.dirname(os.path.abspath(__file__)), "..", "virtualcbct_b200", "data")
 MINIDB = os.path.join(DATA, "xraydb_mini")
 
 

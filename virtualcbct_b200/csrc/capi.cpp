@@ -846,7 +846,8 @@ extern "C" void vcbct_IR_ImageCBCT(const int ite, int reconSize, int reconSlices
 //
 // A batch is a list of (projector, device output) items.  Three launch
 // strategies, picked by vcbct_batch_autotune:
-//  - persistent: one launch of batch_forward_kernel over every item's tiles
+//  - persistent: one launch of persistent_batch_kernel per kFlatItems items,
+//    a GPU-filling grid whose blocks take every item's tiles from a counter
 //    (counter reset + kernel);
 //  - per-item: each item's own forward_kernel launch, spread over two
 //    branches that fork from and join to the caller's stream, so one item's
@@ -862,13 +863,12 @@ static_assert(sizeof(FlatBatch) <= 32000, "the flat batch parameter block exceed
 struct vcbct_batch {
     std::vector<vcbct_projector*> proj;
     std::vector<float*> outs;
-    DevBuf items;       // BatchItem[]
     DevBuf counter;
     long long total = 0;
     int NEmax = 0, nmat_max = 0;
     int cols_per_block = 4, blocks = 0;
     int strategy = 0;   // 0: persistent launch, 1: per-item launches, 2: single flat launch
-    std::vector<FlatBatch> flat;  // strategy 2: the launches' parameter blocks
+    std::vector<FlatBatch> flat;  // strategies 0 and 2: the launches' parameter blocks
     bool dirty = true;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -896,7 +896,6 @@ extern "C" int vcbct_batch_destroy(vcbct_batch* b)
 {
     if (!b) return VCBCT_OK;
     batch_drop_graph(b);
-    b->items.release();
     b->counter.release();
     for (int k = 0; k < kBatchBranches; k++) {
         if (b->branch[k]) cudaStreamDestroy(b->branch[k]);
@@ -933,45 +932,35 @@ extern "C" int vcbct_batch_configure(vcbct_batch* b, int strategy, int cols_per_
 static int batch_build(vcbct_batch* b)
 {
     if (b->proj.empty()) return fail(VCBCT_ERR_STATE, "empty batch");
-    std::vector<BatchItem> it(b->proj.size());
-    long long u = 0;
     b->NEmax = 0;
     b->nmat_max = 0;
+    b->total = 0;
     const int cpb = b->cols_per_block;
-    for (size_t i = 0; i < b->proj.size(); i++) {
-        vcbct_projector* p = b->proj[i];
-        ForwardArgs a;
-        int rc = make_fwd_args(p, a);
-        if (rc) return rc;
-        a.out = b->outs[i];
-        a.cols_per_block = cpb;
-        it[i].fa = a;
-        it[i].unit_begin = u;
-        it[i].ncolb = (p->g.proj_width + cpb - 1) / cpb;
-        it[i].pad = 0;
-        u += (long long)it[i].ncolb * p->g.n_views * ((p->g.proj_height + 31) / 32);
-        b->NEmax = std::max(b->NEmax, p->NE);
-        b->nmat_max = std::max(b->nmat_max, p->g.num_material);
-    }
-    b->total = u;
-    // parameter blocks of the flat strategy, kFlatItems items each
+    // parameter blocks of the single-launch strategies, kFlatItems items each
     b->flat.clear();
-    for (size_t i0 = 0; i0 < it.size(); i0 += kFlatItems) {
+    for (size_t i0 = 0; i0 < b->proj.size(); i0 += kFlatItems) {
         FlatBatch fb{};
-        const size_t n = std::min<size_t>(kFlatItems, it.size() - i0);
+        const size_t n = std::min<size_t>(kFlatItems, b->proj.size() - i0);
         fb.nitems = (int)n;
         long long t = 0;
         for (size_t i = 0; i < n; i++) {
-            fb.fa[i] = it[i0 + i].fa;
-            fb.ncolb[i] = it[i0 + i].ncolb;
+            vcbct_projector* p = b->proj[i0 + i];
+            ForwardArgs a;
+            int rc = make_fwd_args(p, a);
+            if (rc) return rc;
+            a.out = b->outs[i0 + i];
+            a.cols_per_block = cpb;
+            fb.fa[i] = a;
+            fb.ncolb[i] = (p->g.proj_width + cpb - 1) / cpb;
             fb.begin[i] = t;
-            t += (long long)it[i0 + i].ncolb * it[i0 + i].fa.p.V * ((it[i0 + i].fa.p.H + 31) / 32);
+            t += (long long)fb.ncolb[i] * p->g.n_views * ((p->g.proj_height + 31) / 32);
+            b->NEmax = std::max(b->NEmax, p->NE);
+            b->nmat_max = std::max(b->nmat_max, p->g.num_material);
         }
         fb.begin[n] = t;
+        b->total += t;
         b->flat.push_back(fb);
     }
-    VCBCT_CUDA_TRY(b->items.ensure(sizeof(BatchItem) * it.size()));
-    VCBCT_CUDA_TRY(cudaMemcpy(b->items.p, it.data(), sizeof(BatchItem) * it.size(), cudaMemcpyHostToDevice));
     VCBCT_CUDA_TRY(b->counter.ensure(64));
     int dev = 0, sms = 0;
     VCBCT_CUDA_TRY(cudaGetDevice(&dev));
@@ -991,9 +980,9 @@ static int batch_launch(vcbct_batch* b, cudaStream_t st)
         return VCBCT_OK;
     }
     if (b->strategy == 0) {
-        VCBCT_CUDA_TRY(launch_batch_forward(b->items.as<BatchItem>(), (int)b->proj.size(), b->total, b->NEmax,
-                                            b->nmat_max, b->cols_per_block, b->blocks,
-                                            b->counter.as<unsigned long long>(), st));
+        for (const FlatBatch& fb : b->flat)
+            VCBCT_CUDA_TRY(launch_persistent_batch(fb, b->NEmax, b->nmat_max, b->cols_per_block, b->blocks,
+                                                   b->counter.as<unsigned long long>(), st));
         return VCBCT_OK;
     }
     if (!b->fork) {

@@ -90,16 +90,10 @@ struct FlatBatch {
 };
 cudaError_t launch_flat_batch(const FlatBatch& b, int NEmax, int nmat_max, int cols_per_block, cudaStream_t st);
 
-// One phantom of a batched forward projection (u16 volume, no counter).
-struct BatchItem {
-    ForwardArgs fa;
-    long long unit_begin;  // index of its first work tile
-    int ncolb;             // column blocks per view and row band
-    int pad;
-};
-cudaError_t launch_batch_forward(const BatchItem* d_items, int nitems, long long total_units, int NEmax,
-                                 int nmat_max, int cols_per_block, int blocks, unsigned long long* counter,
-                                 cudaStream_t st);
+// The same items in one persistent launch of `blocks` blocks that take work
+// tiles from `counter` (zeroed by the launch).
+cudaError_t launch_persistent_batch(const FlatBatch& b, int NEmax, int nmat_max, int cols_per_block, int blocks,
+                                   unsigned long long* counter, cudaStream_t st);
 int batch_blocks_per_sm(int nmat_max, int cols_per_block, int NEmax);
 
 struct AdjointArgs {

@@ -1107,55 +1107,49 @@ __global__ void VCBCT_FWD_BOUNDS flat_batch_kernel(const __grid_constant__ FlatB
     forward_tile<M, false, false>(fa, s_mu, s_pdf, iv_buffer(smem, fa.spec.NE), v, rowt, colb);
 }
 
-// Persistent batched forward projection: every block repeatedly takes the
-// next work tile from a global counter.  Tiles are numbered item by item,
-// and within an item by row band, then view, then column block (the order of
-// forward_kernel's grid), so the items' uneven view and slice counts
-// load-balance across the whole GPU in one launch.
-// The current item's arguments are staged in shared memory, so the march
-// reads them like forward_kernel reads its parameters (no global loads or
-// registers held for them); the bounds cap registers as forward_kernel's.
+// Persistent batched forward projection: a grid of as many blocks as fit on
+// the GPU at once, every block repeatedly taking the next work tile from a
+// global counter.  Tiles are numbered item by item, and within an item by
+// row band, then view, then column block (the order of forward_kernel's
+// grid), so the items' uneven view and slice counts load-balance across the
+// whole GPU in one launch.  The items' arguments sit in the launch's
+// parameter block as for flat_batch_kernel: the march reads them from the
+// parameter bank (a block-uniform index found by a binary search), so they
+// hold no registers; a block reloads the spectrum table only when its next
+// tile belongs to another item.
 template <int M>
-__global__ void __launch_bounds__(256) batch_forward_kernel(const BatchItem* __restrict__ items, int nitems,
-                                                               long long total, int NEmax,
-                                                               unsigned long long* counter)
+__global__ void VCBCT_FWD_BOUNDS persistent_batch_kernel(const __grid_constant__ FlatBatch b,
+                                                         unsigned long long* counter, int NEmax)
 {
     extern __shared__ float4 smem[];
     __shared__ long long s_unit;
-    __shared__ ForwardArgs s_fa;
-    __shared__ long long s_begin;
-    __shared__ int s_ncolb;
     float4* s_mu = smem;
     float* s_pdf = reinterpret_cast<float*>(smem + 2 * NEmax);
     IvRec* s_iv = iv_buffer(smem, NEmax);
+    const long long total = b.begin[b.nitems];
     int cur = -1;
     for (;;) {
         if (threadIdx.x == 0 && threadIdx.y == 0) s_unit = (long long)atomicAdd(counter, 1ull);
         __syncthreads();
         const long long u = s_unit;
-        if (u >= total) break;
-        int lo = 0, hi = nitems - 1;  // last item with begin <= u
+        if (u >= total) break;  // block-uniform
+        int lo = 0, hi = b.nitems - 1;  // last item with begin <= u
         while (lo < hi) {
-            const int mid = (lo + hi + 1) / 2;
-            if (items[mid].unit_begin <= u) lo = mid;
+            const int mid = (lo + hi + 1) >> 1;
+            if (b.begin[mid] <= u) lo = mid;
             else hi = mid - 1;
         }
         if (lo != cur) {  // block-uniform
-            if (threadIdx.x == 0 && threadIdx.y == 0) {
-                s_fa = items[lo].fa;
-                s_begin = items[lo].unit_begin;
-                s_ncolb = items[lo].ncolb;
-            }
-            load_spectrum(items[lo].fa.spec, s_mu, s_pdf);
+            load_spectrum(b.fa[lo].spec, s_mu, s_pdf);
             cur = lo;
         }
         __syncthreads();
-        const long long w = u - s_begin;
-        const int colb = (int)(w % s_ncolb);
-        const long long rest = w / s_ncolb;
-        const int v = (int)(rest % s_fa.p.V);
-        const int rowt = (int)(rest / s_fa.p.V);
-        forward_tile<M, false, false>(s_fa, s_mu, s_pdf, s_iv, v, rowt, colb);
+        const long long w = u - b.begin[lo];
+        const int colb = (int)(w % b.ncolb[lo]);
+        const long long rest = w / b.ncolb[lo];
+        const int v = (int)(rest % b.fa[lo].p.V);
+        const int rowt = (int)(rest / b.fa[lo].p.V);
+        forward_tile<M, false, false>(b.fa[lo], s_mu, s_pdf, s_iv, v, rowt, colb);
         __syncthreads();
     }
 }
@@ -1398,10 +1392,10 @@ static cudaError_t launch_fwd_t(const ForwardArgs& a, cudaStream_t st)
     return cudaGetLastError();
 }
 
-cudaError_t launch_batch_forward(const BatchItem* d_items, int nitems, long long total_units, int NEmax,
-                                 int nmat_max, int cols_per_block, int blocks, unsigned long long* counter,
-                                 cudaStream_t st)
+cudaError_t launch_persistent_batch(const FlatBatch& b, int NEmax, int nmat_max, int cols_per_block, int blocks,
+                                   unsigned long long* counter, cudaStream_t st)
 {
+    if (b.begin[b.nitems] <= 0) return cudaSuccess;
     dim3 block(32, cols_per_block);
     size_t shm = ((size_t)2 * NEmax + (NEmax + 3) / 4) * sizeof(float4) +
                  (size_t)cols_per_block * kIvSlots * sizeof(IvRec);
@@ -1409,8 +1403,8 @@ cudaError_t launch_batch_forward(const BatchItem* d_items, int nitems, long long
     // stream capture)
     cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st);
     if (e != cudaSuccess) return e;
-    if (nmat_max <= 6) batch_forward_kernel<6><<<blocks, block, shm, st>>>(d_items, nitems, total_units, NEmax, counter);
-    else batch_forward_kernel<8><<<blocks, block, shm, st>>>(d_items, nitems, total_units, NEmax, counter);
+    auto k = (nmat_max <= 6) ? persistent_batch_kernel<6> : persistent_batch_kernel<8>;
+    k<<<blocks, block, shm, st>>>(b, counter, NEmax);
     return cudaGetLastError();
 }
 
@@ -1434,7 +1428,7 @@ int batch_blocks_per_sm(int nmat_max, int cols_per_block, int NEmax)
     size_t shm = ((size_t)2 * NEmax + (NEmax + 3) / 4) * sizeof(float4) +
                  (size_t)cols_per_block * kIvSlots * sizeof(IvRec);
     int n = 0;
-    auto k = (nmat_max <= 6) ? batch_forward_kernel<6> : batch_forward_kernel<8>;
+    auto k = (nmat_max <= 6) ? persistent_batch_kernel<6> : persistent_batch_kernel<8>;
     if (shm > 48 * 1024 && cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm) != cudaSuccess)
         return 0;
     auto kf = (nmat_max <= 6) ? flat_batch_kernel<6> : flat_batch_kernel<8>;
