@@ -68,3 +68,20 @@ def volume_checksum(vol: np.ndarray) -> int:
     v = vol.reshape(-1).astype(np.uint64)
     idx = np.arange(v.size, dtype=np.uint64) % np.uint64(1000003)
     return int((v * (idx + np.uint64(1))).sum() % np.uint64(2 ** 61 - 1))
+
+
+def report(key: str, value) -> None:
+    """Record a measured error under `key` in the JSON file named by the
+    environment variable VCBCT_PARITY_REPORT (no-op when it is unset), so a
+    run of the parity tests leaves the numbers behind, not only pass/fail."""
+    import json
+    path = os.environ.get("VCBCT_PARITY_REPORT")
+    if not path:
+        return
+    data = {}
+    if os.path.exists(path):
+        with open(path) as f:
+            data = json.load(f)
+    data[key] = value
+    with open(path, "w") as f:
+        json.dump(data, f, indent=1, sort_keys=True)

@@ -89,6 +89,8 @@ def test_reference_programs_run_on_libvcbct(cuda, tmp_path, tag, pdeck, fdeck):
                          want=("d",), exact=False)["d"]
     gpu = out[views][:, :, cols].astype(np.float64)
     rel = np.abs(gpu - og) / og
+    shipped.report(f"{tag} drop-in projection vs FP64 oracle (rel/pixel, {len(views)} views x 24 columns)",
+                   float(rel.max()))
     assert rel.max() <= RTOL, f"max rel err vs FP64 oracle {rel.max():.3e}"
 
     # the fixture's views against the reference's own reprojection()
@@ -104,6 +106,8 @@ def test_reference_programs_run_on_libvcbct(cuda, tmp_path, tag, pdeck, fdeck):
     gpu = out[gv][:, :, gc].astype(np.float64)
     twin = od["f"] != cpu_ties
     rel = np.abs(gpu - ref) / ref
+    shipped.report(f"{tag} drop-in projection vs reprojection() (rel/pixel, 4 views x all 101 bins; tie rays)",
+                   [float(rel[~twin].max()), int(twin.sum())])
     assert rel[~twin].max() <= RTOL, f"max rel err vs reprojection() {rel[~twin].max():.3e}"
     assert (np.abs(gpu - od["d"]) / od["d"])[twin].max(initial=0.0) <= RTOL
 
@@ -127,6 +131,8 @@ def test_reference_programs_run_on_libvcbct(cuda, tmp_path, tag, pdeck, fdeck):
     ref_vol = np.fromfile(os.path.join(ref_r, fd["recon_file"]), np.int16)
     assert ref_vol.size == n and np.abs(ref_vol).max() > 100
     d = np.abs(vol.astype(np.int32) - ref_vol.astype(np.int32))
+    shipped.report(f"{tag} drop-in cbct2 short volume vs the reference cbct2 (LSB, whole volume; voxels off by 1)",
+                   [int(d.max()), int((d > 0).sum())])
     assert d.max() <= 1, f"{(d > 1).sum()} voxels differ from the reference cbct2 by more than 1 LSB"
 
     # the library's own FDK program on the same deck, reading vcbct_proj's file
