@@ -130,3 +130,34 @@ def test_bf16x3_tensor_core_filter_matches_fp64(cuda, V, H, W, xshift):
     direct = f.filter(proj, method=FILTER_DIRECT_F32)
     assert np.abs(direct - d64).max() <= 1e-5 * np.abs(d64).max()
     assert np.abs(gpu - direct).max() <= tol * np.abs(d64).max()
+
+
+@pytest.mark.parametrize("redundancy", [0, 1])
+def test_bf16x3_fused_and_split_a_operand_agree(cuda, redundancy):
+    """Device projections with 16-byte-aligned rows take the fused form (the
+    GEMM makes the A planes of -ln p in shared memory); the same values at a
+    4-byte offset take the split pass through global memory.  Both against
+    the FP64 filter at 1e-5 of the scale, with and without redundancy
+    weights."""
+    import torch
+    g, proj, ang, xs = _case(V=3, H=70, W=400, seed=11, xshift=2.0)
+    g = g.with_(redundancy=redundancy)
+    f = Fdk(g, ang, xs, np.zeros(g.V))
+    if redundancy:
+        w = redundancy_weights(g, xs)
+        pw = (proj.astype(np.float64) ** w[:, None, :].astype(np.float64)).astype(np.float32)
+    else:
+        pw = proj
+    d64 = O.filter_sinogram(pw, xs, np.zeros(g.V), O.fdk_consts(g.piso), mode=1)
+    n = proj.size
+    aligned = torch.from_numpy(proj).cuda()
+    store = torch.empty(n + 1, dtype=torch.float32, device="cuda")
+    offset = store[1:].view(proj.shape)
+    offset.copy_(aligned)
+    assert aligned.data_ptr() % 16 == 0 and offset.data_ptr() % 16 == 4
+    fused = f.filter(aligned, method=FILTER_BF16X3).cpu().numpy()
+    split = f.filter(offset, method=FILTER_BF16X3).cpu().numpy()
+    scale = np.abs(d64).max()
+    assert np.abs(fused - d64).max() <= 1e-5 * scale
+    assert np.abs(split - d64).max() <= 1e-5 * scale
+    assert np.abs(fused - split).max() <= 1e-5 * scale

@@ -1659,7 +1659,8 @@ extern "C" int vcbct_fdk_filter(vcbct_fdk* f, const float* proj, float* filtered
                                             pitch, (float)g.sad_cm, g.n_views, g.proj_height,
                                             g.proj_width, st));
     } else if (method == VCBCT_FILTER_BF16X3) {
-        VCBCT_CUDA_TRY(f->work.ensure(ramp_gemm_workspace_bytes(g.n_views, g.proj_height, g.proj_width)));
+        VCBCT_CUDA_TRY(f->work.ensure(ramp_gemm_workspace_bytes(g.n_views, g.proj_height, g.proj_width,
+                                                                 ramp_gemm_fused(din, g.proj_width))));
         if (f->work.p != f->b_at) {
             f->b_ready = 0;
             f->b_at = f->work.p;

@@ -157,7 +157,11 @@ cudaError_t launch_backproject(const FdkParams& f, const BpView* d_views, const 
 // the split Toeplitz planes: with *b_ready set they are taken as already
 // split from hT into this workspace and are not redone; the launch sets it
 // once it has queued the split (b_ready may be null: split every call).
-size_t ramp_gemm_workspace_bytes(int V, int H, int W);
+// The fused form (rows of `proj` 16-byte aligned: W % 4 == 0 and an aligned
+// base, ramp_gemm_fused) splits -ln p inside the GEMM; the other needs room
+// for the split A planes as well: size the workspace with the same flag.
+bool ramp_gemm_fused(const float* proj, int W);
+size_t ramp_gemm_workspace_bytes(int V, int H, int W, bool fused);
 cudaError_t launch_ramp_gemm_bf16x3(const float* proj, float* out, const float* hT,
                                     const FilterView* views, const float* wts, float pitch,
                                     float sad, int V, int H, int W, void* workspace,

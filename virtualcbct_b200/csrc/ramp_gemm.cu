@@ -10,15 +10,22 @@
 // tensor memory, which keeps about 24 significant bits.
 //
 // One CTA computes a 128-row x NT-column output tile (NT <= 512, a multiple
-// of 32; wider detectors take several column tiles), K tile by K tile.
-// split_a_kernel first writes the three A planes of -logf(p) to global
-// memory; the split Toeplitz planes (B) are made once per kernel.  In the
-// GEMM, warp 0 streams by TMA, per K tile, the tile's three A planes (a
-// 2-stage ring) and then B planes 2, 1, 0, each as two column halves (a
-// 4-stage ring), so each B plane of a K tile is loaded once and multiplied by
-// every A plane it pairs with; warp 1 issues tcgen05.mma from a single thread
-// into two 128 x NT/2 FP32 accumulators in tensor memory (columns 0 and 256);
-// warps 2-9 read them back (tcgen05.ld), apply the cosine factor and store.
+// of 32; wider detectors take several column tiles), K tile by K tile.  The
+// split Toeplitz planes (B) are made once per kernel.  In the GEMM, warp 0
+// streams by TMA, per K tile, the A operand and then B planes 2, 1, 0, each
+// as two column halves (a ring of 3 or 4 stages), so each B plane of a K tile
+// is loaded once and multiplied by every A plane it pairs with; warp 1 issues
+// tcgen05.mma from a single thread into two 128 x NT/2 FP32 accumulators in
+// tensor memory (columns 0 and 256); warps 2-9 read them back (tcgen05.ld),
+// apply the cosine factor and store.
+//
+// The A operand, fused form (rows of p 16-byte aligned): warp 0 stages the
+// 128 x 64 FP32 tile of p in shared memory and warps 2-9, idle until the
+// epilogue, turn it into the three swizzled bf16 planes of -ln p in a
+// 2-stage ring -- p is read from HBM once and no split copy is written.
+// Unfused form (other widths): split_a_kernel first writes the three A planes
+// to global memory and warp 0 loads them by TMA.
+//
 // No cluster multicast is used.  Every mbarrier wait is bounded; on timeout
 // the kernel raises a device flag, stops issuing, waits (bounded) for its
 // loads in flight and returns; its output is then invalid.
@@ -186,26 +193,107 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v)
 struct GemmArgs {
     float* out;
     const FilterView* views;
+    const float* wts;             // fused form: optional redundancy weights [V][W] (multiply -ln p)
     float pitch, sad;
     int M, H, W, NT, Kp, ktiles;  // NT: output columns per CTA (blockIdx.y selects the column tile)
     int vec;                      // rows of `out` 16-byte aligned (W % 4 == 0, aligned base)
     int* err;
 };
 
-constexpr int kEpiWarps = 8;                    // warps 2-9: the epilogue, two per TMEM lane quarter
-static_assert(kThreads == 64 + 32 * kEpiWarps, "warp 0 TMA, warp 1 MMA, the rest epilogue");
+constexpr int kEpiWarps = 8;                    // warps 2-9: A planes (fused form), then the epilogue
+static_assert(kThreads == 64 + 32 * kEpiWarps, "warp 0 TMA, warp 1 MMA, the rest A planes / epilogue");
 constexpr uint32_t kHalfCol = 256;              // TMEM column of the second column half
 constexpr int kAStages = 2;                     // A ring: the three planes of one K tile each
-constexpr int kBStages = 4;                     // B ring: one column half of one plane of one K tile each
 constexpr uint32_t kAPlaneBytes = BM * BK * 2;  // one 128 x 64 bf16 plane, 16 KiB
 constexpr uint32_t kAStageBytes = 3 * kAPlaneBytes;
+constexpr uint32_t kPTileBytes = BM * BK * 4;   // fused form: one 128 x 64 FP32 tile of p, 32 KiB
+
+// B ring stages (one column half of one plane of one K tile each): the fused
+// form gives up one to hold the FP32 tile of p.
+__host__ __device__ constexpr int b_stages(bool fused) { return fused ? 3 : 4; }
 
 // Shared-memory footprint of a CTA with NT output columns (before 1 KiB
-// alignment slack): A ring, B ring of NT/2-row halves, mbarriers, TMEM slot.
-__host__ __device__ constexpr size_t gemm_smem_bytes(int NT)
+// alignment slack): [p tile], A ring, B ring of NT/2-row halves, mbarriers,
+// TMEM slot.
+__host__ __device__ constexpr size_t gemm_smem_bytes(int NT, bool fused)
 {
-    return (size_t)kAStages * kAStageBytes + (size_t)kBStages * (NT / 2) * BK * 2 +
-           8 * (2 * kAStages + 2 * kBStages + 1) + 16;
+    return (fused ? (size_t)kPTileBytes : 0) + (size_t)kAStages * kAStageBytes +
+           (size_t)b_stages(fused) * (NT / 2) * BK * 2 + 8 * (2 + 2 * kAStages + 2 * b_stages(fused) + 1) + 16;
+}
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int c0, int c1)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%3, %4}], [%2];" ::"r"(smem_u32(dst)),
+        "l"(map), "r"(smem_u32(bar)), "r"(c0), "r"(c1)
+        : "memory");
+}
+
+__device__ __forceinline__ void st_shared_u32(uint32_t addr, uint32_t v)
+{
+    asm volatile("st.shared.b32 [%0], %1;" ::"r"(addr), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ float2 ld_shared_f2(uint32_t addr)
+{
+    float2 v;
+    asm volatile("ld.shared.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "r"(addr) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// Fused form: one K tile of the A operand made in shared memory from the
+// FP32 tile of p the TMA thread has staged (row r at r * 256 bytes; rows
+// beyond M and columns beyond W read as 0 and are skipped): g = -ln(p)
+// (times the redundancy weight), split into three bf16 planes, each stored as
+// the 128-byte-swizzled K-major tile a TMA load with
+// CU_TENSOR_MAP_SWIZZLE_128B would write (row r at r * 128 bytes, the 16-byte
+// chunk index XOR r % 8; buffers 1024-byte aligned).  Producer warp w makes
+// rows 16 w .. 16 w + 15, lane l the columns kt * 64 + 2 l, + 1 of each: one
+// 8-byte shared load and one 4-byte store per plane, conflict-free.
+// Redundancy weights: with wfast (H >= 16) the warp's rows hold at most two
+// views, whose weights the caller has loaded (wa before CTA row rsplit, wb
+// from it on); otherwise each row loads its own.
+__device__ __forceinline__ void convert_a_tile(const GemmArgs& g, int m0, int kt, int pw, int lane,
+                                               uint32_t ptile, uint32_t abuf, bool wfast, int rsplit, float2 wa,
+                                               float2 wb)
+{
+    const int k = kt * BK + 2 * lane;
+    const bool in0 = k < g.W, in1 = k + 1 < g.W;
+#pragma unroll 4
+    for (int rr = 0; rr < BM / kEpiWarps; rr++) {
+        const int r = pw * (BM / kEpiWarps) + rr;
+        const int row = m0 + r;
+        const float2 pv = ld_shared_f2(ptile + (uint32_t)r * (BK * 4) + (uint32_t)lane * 8u);
+        float x = 0.0f, y = 0.0f;
+        if (row < g.M) {
+            // -ln p from the hardware base-2 logarithm (relative error ~2^-22;
+            // the split keeps ~24 bits, the filter's bar is 1e-5 of its scale)
+            if (in0) x = __log2f(pv.x) * -0.693147180559945309f;
+            if (in1) y = __log2f(pv.y) * -0.693147180559945309f;
+            if (g.wts && in0) {
+                float2 w = r < rsplit ? wa : wb;
+                if (!wfast) {
+                    const float* wr = g.wts + (size_t)(row / g.H) * g.W + k;
+                    w = make_float2(__ldg(wr), in1 ? __ldg(wr + 1) : 1.0f);
+                }
+                x *= w.x;
+                y *= w.y;
+            }
+        }
+        uint32_t q0, q1, q2;
+        split3x2(x, y, q0, q1, q2);
+        const uint32_t off = (uint32_t)r * 128u + (uint32_t)lane * 4u;
+        const uint32_t sw = off ^ (((off >> 7) & 7u) << 4);
+        st_shared_u32(abuf + sw, q0);
+        st_shared_u32(abuf + kAPlaneBytes + sw, q1);
+        st_shared_u32(abuf + 2 * kAPlaneBytes + sw, q2);
+    }
 }
 
 // Warp-uniform bounded wait (tcgen05.ld needs converged warps).
@@ -214,22 +302,27 @@ __device__ __forceinline__ bool warp_wait(uint64_t* bar, uint32_t phase, int* er
     return __all_sync(0xffffffffu, mbar_wait(bar, phase, err));
 }
 
+template <bool FUSED>
 __global__ void __launch_bounds__(kThreads, 1)
 ramp_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, GemmArgs g)
 {
+    constexpr int SB = b_stages(FUSED);
     extern __shared__ uint8_t smem_raw[];
     // 1024-byte alignment for the 128-byte swizzle atoms
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     const int NH = g.NT / 2;                      // columns of one B half (a multiple of 16)
     const uint32_t bh_bytes = (uint32_t)NH * BK * 2;
-    uint8_t* abuf = smem;                         // kAStages x 3 planes
-    uint8_t* bbuf = smem + kAStages * kAStageBytes;  // kBStages x one B half
-    uint64_t* bars = reinterpret_cast<uint64_t*>(bbuf + (size_t)kBStages * bh_bytes);
-    uint64_t* a_full = bars;
-    uint64_t* a_empty = bars + kAStages;
-    uint64_t* b_full = bars + 2 * kAStages;
-    uint64_t* b_empty = bars + 2 * kAStages + kBStages;
-    uint64_t* accum = bars + 2 * kAStages + 2 * kBStages;
+    uint8_t* ptile = smem;                        // fused form: the FP32 tile of p
+    uint8_t* abuf = smem + (FUSED ? kPTileBytes : 0);   // kAStages x 3 planes
+    uint8_t* bbuf = abuf + kAStages * kAStageBytes;    // SB x one B half
+    uint64_t* bars = reinterpret_cast<uint64_t*>(bbuf + (size_t)SB * bh_bytes);
+    uint64_t* p_full = bars;                      // fused form: TMA bytes of the p tile
+    uint64_t* p_empty = bars + 1;                 // fused form: the converter warps are done reading it
+    uint64_t* a_full = bars + 2;
+    uint64_t* a_empty = bars + 2 + kAStages;
+    uint64_t* b_full = bars + 2 + 2 * kAStages;
+    uint64_t* b_empty = bars + 2 + 2 * kAStages + SB;
+    uint64_t* accum = bars + 2 + 2 * kAStages + 2 * SB;
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(accum + 1);
 
     const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
@@ -237,11 +330,13 @@ ramp_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant_
     const int n0 = blockIdx.y * g.NT;
 
     if (threadIdx.x == 0) {
+        mbar_init(p_full, 1);
+        mbar_init(p_empty, kEpiWarps);
         for (int s = 0; s < kAStages; s++) {
-            mbar_init(&a_full[s], 1);
+            mbar_init(&a_full[s], FUSED ? kEpiWarps : 1);
             mbar_init(&a_empty[s], 1);
         }
-        for (int s = 0; s < kBStages; s++) {
+        for (int s = 0; s < SB; s++) {
             mbar_init(&b_full[s], 1);
             mbar_init(&b_empty[s], 1);
         }
@@ -259,21 +354,36 @@ ramp_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant_
     const uint32_t taddr = *tmem_slot;
 
     if (warp == 0 && lane == 0) {
-        // TMA producer.  Per K tile: the three A planes (one A stage), then
-        // the B planes 2, 1, 0, each as two column halves (six B stages) --
-        // the order the MMA thread consumes them in.
+        // TMA producer.  Per K tile: the A operand (fused form: the FP32 tile
+        // of p; otherwise the three split A planes, one A stage), then the B
+        // planes 2, 1, 0, each as two column halves (six B stages) -- the
+        // order the consumers take them in.
         int na = 0, nb = 0;  // stages issued
         bool ok = true;
+        if (FUSED) {  // the first p tile; tile kt + 1 follows B half 3 of tile kt
+            mbar_expect_tx(p_full, kPTileBytes);
+            tma_load_2d(ptile, &tmA, p_full, 0, m0);
+            na = 1;
+        }
         for (int kt = 0; kt < g.ktiles && ok; kt++) {
-            const int sa = kt % kAStages;
-            if (kt >= kAStages && !(ok = mbar_wait(&a_empty[sa], ((kt / kAStages) - 1) & 1, g.err))) break;
-            uint8_t* da = abuf + (size_t)sa * kAStageBytes;
-            mbar_expect_tx(&a_full[sa], kAStageBytes);
-            for (int i = 0; i < 3; i++) tma_load_3d(da + i * kAPlaneBytes, &tmA, &a_full[sa], kt * BK, m0, i);
-            na = kt + 1;
+            if (!FUSED) {
+                const int sa = kt % kAStages;
+                if (kt >= kAStages && !(ok = mbar_wait(&a_empty[sa], ((kt / kAStages) - 1) & 1, g.err))) break;
+                uint8_t* da = abuf + (size_t)sa * kAStageBytes;
+                mbar_expect_tx(&a_full[sa], kAStageBytes);
+                for (int i = 0; i < 3; i++) tma_load_3d(da + i * kAPlaneBytes, &tmA, &a_full[sa], kt * BK, m0, i);
+                na = kt + 1;
+            }
             for (int q = 0; q < 6; q++) {
-                const int kb = kt * 6 + q, s = kb % kBStages;
-                if (kb >= kBStages && !(ok = mbar_wait(&b_empty[s], ((kb / kBStages) - 1) & 1, g.err))) break;
+                if (FUSED && q == 3 && kt + 1 < g.ktiles) {
+                    // the staged tile is free once the converters have read it
+                    if (!(ok = mbar_wait(p_empty, kt & 1, g.err))) break;
+                    mbar_expect_tx(p_full, kPTileBytes);
+                    tma_load_2d(ptile, &tmA, p_full, (kt + 1) * BK, m0);
+                    na = kt + 2;
+                }
+                const int kb = kt * 6 + q, s = kb % SB;
+                if (kb >= SB && !(ok = mbar_wait(&b_empty[s], ((kb / SB) - 1) & 1, g.err))) break;
                 const int plane = 2 - q / 2, h = q % 2;
                 mbar_expect_tx(&b_full[s], bh_bytes);
                 tma_load_3d(bbuf + (size_t)s * bh_bytes, &tmB, &b_full[s], kt * BK, n0 + h * NH, plane);
@@ -282,10 +392,14 @@ ramp_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant_
         }
         // no load may still be in flight into this CTA's shared memory when it
         // exits: wait (bounded) for the last stages issued
-        for (int k = na - kAStages; k < na; k++)
-            if (k >= 0) mbar_wait(&a_full[k % kAStages], (k / kAStages) & 1, g.err);
-        for (int k = nb - kBStages; k < nb; k++)
-            if (k >= 0) mbar_wait(&b_full[k % kBStages], (k / kBStages) & 1, g.err);
+        if (FUSED) {
+            if (na > 0) mbar_wait(p_full, (na - 1) & 1, g.err);
+        } else {
+            for (int k = na - kAStages; k < na; k++)
+                if (k >= 0) mbar_wait(&a_full[k % kAStages], (k / kAStages) & 1, g.err);
+        }
+        for (int k = nb - SB; k < nb; k++)
+            if (k >= 0) mbar_wait(&b_full[k % SB], (k / SB) & 1, g.err);
     } else if (warp == 1 && lane == 0) {
         // MMA issuer: per K tile and B plane j, each column half against A
         // planes 2 - j .. 0, so the products (2,0) (1,1) (0,2) (1,0) (0,1)
@@ -297,8 +411,8 @@ ramp_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant_
             if (!(ok = mbar_wait(&a_full[sa], (kt / kAStages) & 1, g.err))) break;
             const uint32_t abase = smem_u32(abuf + (size_t)sa * kAStageBytes);
             for (int q = 0; q < 6 && ok; q++) {
-                const int kb = kt * 6 + q, s = kb % kBStages;
-                if (!(ok = mbar_wait(&b_full[s], (kb / kBStages) & 1, g.err))) break;
+                const int kb = kt * 6 + q, s = kb % SB;
+                if (!(ok = mbar_wait(&b_full[s], (kb / SB) & 1, g.err))) break;
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                 const int j = 2 - q / 2, h = q % 2;
                 const uint32_t sb = smem_u32(bbuf + (size_t)s * bh_bytes);
@@ -317,6 +431,49 @@ ramp_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant_
         }
         umma_commit(accum);
     } else if (warp >= 2) {
+        bool ok = true;
+        if (FUSED) {
+            // the A planes of every K tile from the staged p tile,
+            // double-buffered against the MMAs
+            const int pw = warp - 2;
+            // the warp's rows m0 + 16 pw .. + 15 lie in views va and (from CTA
+            // row rsplit on) va + 1 when H >= 16
+            const int rw = m0 + pw * (BM / kEpiWarps);
+            const bool wfast = g.wts != nullptr && g.H >= BM / kEpiWarps;
+            const int va = rw / g.H;
+            const int rsplit = (va + 1) * g.H - m0;
+            const bool has_a = rw < g.M;
+            const bool has_b = rsplit < pw * (BM / kEpiWarps) + BM / kEpiWarps && m0 + rsplit < g.M;
+            for (int kt = 0; kt < g.ktiles; kt++) {
+                const int sa = kt % kAStages;
+                // this tile's weights, loaded before the waits so that their
+                // latency passes while the p tile arrives
+                float2 wa = make_float2(1.0f, 1.0f), wb = wa;
+                const int k = kt * BK + 2 * lane;
+                if (wfast && k < g.W) {
+                    const bool in1 = k + 1 < g.W;
+                    if (has_a) {
+                        const float* wr = g.wts + (size_t)va * g.W + k;
+                        wa = make_float2(__ldg(wr), in1 ? __ldg(wr + 1) : 1.0f);
+                    }
+                    if (has_b) {
+                        const float* wr = g.wts + (size_t)(va + 1) * g.W + k;
+                        wb = make_float2(__ldg(wr), in1 ? __ldg(wr + 1) : 1.0f);
+                    }
+                }
+                if (!(ok = warp_wait(p_full, kt & 1, g.err))) break;
+                if (kt >= kAStages && !(ok = warp_wait(&a_empty[sa], ((kt / kAStages) - 1) & 1, g.err))) break;
+                convert_a_tile(g, m0, kt, pw, lane, smem_u32(ptile), smem_u32(abuf + (size_t)sa * kAStageBytes),
+                               wfast, rsplit, wa, wb);
+                // generic-proxy stores -> visible to the tensor core (async proxy)
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                __syncwarp();
+                if (lane == 0) {
+                    mbar_arrive(p_empty);
+                    mbar_arrive(&a_full[sa]);
+                }
+            }
+        }
         // epilogue: TMEM -> registers -> cosine factor -> global; two warps
         // per TMEM lane quarter (a warp may access lanes 32 (warp % 4) ..),
         // each taking every other 16-column chunk; logical column c lies at
@@ -324,7 +481,7 @@ ramp_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant_
         const int q = warp % 4;
         const int half = (warp - 2) / 4;
         const int row = m0 + 32 * q + lane;
-        if (warp_wait(accum, 0, g.err)) {
+        if (ok && warp_wait(accum, 0, g.err)) {
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             float pos2 = 0.0f, xcs = 0.0f;
             if (row < g.M) {
@@ -373,13 +530,12 @@ ramp_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant_
     }
 }
 
-// A planes [3][M][Kp]: split of g = -logf(p) (times the redundancy weight).
-// grid (M, ceil(Kp / 1024)), block 128: one detector row per block, eight
-// consecutive columns per thread (two 16-byte loads where the row allows),
-// each plane written as one 16-byte group (Kp is a multiple of 64).
+// Unfused form, rows of p not 16-byte aligned: A planes [3][M][Kp], the
+// split of g = -logf(p) (times the redundancy weight).  grid (M, ceil(Kp /
+// 1024)), block 128: one detector row per block, eight consecutive columns
+// per thread, each plane written as one 16-byte group (Kp is a multiple of 64).
 __global__ void __launch_bounds__(128) split_a_kernel(const float* __restrict__ proj, const float* __restrict__ wts,
-                                                      int M, int H, int W, int Kp, int vec,
-                                                      __nv_bfloat16* __restrict__ planes)
+                                                      int M, int H, int W, int Kp, __nv_bfloat16* __restrict__ planes)
 {
     const int r = blockIdx.x;
     const int k0 = 8 * (blockIdx.y * blockDim.x + threadIdx.x);
@@ -387,21 +543,13 @@ __global__ void __launch_bounds__(128) split_a_kernel(const float* __restrict__ 
     const float* pr = proj + (size_t)r * W;
     const float* wr = wts ? wts + (size_t)(r / H) * W : nullptr;
     float x[8];
-    if (vec && k0 + 8 <= W) {
-        const float4 a = __ldg(reinterpret_cast<const float4*>(pr + k0));
-        const float4 b = __ldg(reinterpret_cast<const float4*>(pr + k0 + 4));
-        x[0] = a.x; x[1] = a.y; x[2] = a.z; x[3] = a.w;
-        x[4] = b.x; x[5] = b.y; x[6] = b.z; x[7] = b.w;
 #pragma unroll
-        for (int q = 0; q < 8; q++) x[q] = -logf(x[q]);
-    } else {
-#pragma unroll
-        for (int q = 0; q < 8; q++) x[q] = (k0 + q < W) ? -logf(__ldg(pr + k0 + q)) : 0.0f;
-    }
-    if (wr) {
-#pragma unroll
-        for (int q = 0; q < 8; q++)
-            if (k0 + q < W) x[q] *= __ldg(wr + k0 + q);
+    for (int q = 0; q < 8; q++) {
+        x[q] = 0.0f;
+        if (k0 + q < W) {
+            x[q] = -logf(__ldg(pr + k0 + q));
+            if (wr) x[q] *= __ldg(wr + k0 + q);
+        }
     }
     uint4 p0, p1, p2;
     split3x2(x[0], x[1], p0.x, p1.x, p2.x);
@@ -460,18 +608,33 @@ bool make_map(CUtensorMap* map, void* base, int rows, int Kp, int box_rows)
               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// 2D FP32 tensor [M][W] (the projections) with box {64, 128}, no swizzle;
+// columns beyond W and rows beyond M read as zero.
+bool make_p_map(CUtensorMap* map, const float* proj, int M, int W)
+{
+    EncodeTiledFn fn = encode_fn();
+    if (!fn) return false;
+    cuuint64_t dims[2] = {(cuuint64_t)W, (cuuint64_t)M};
+    cuuint64_t strides[1] = {(cuuint64_t)W * 4};
+    cuuint32_t box[2] = {(cuuint32_t)BK, (cuuint32_t)BM};
+    cuuint32_t estr[2] = {1, 1};
+    return fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(proj), dims, strides, box, estr,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 // Output columns are split into ntiles tiles of NT <= 512 columns (one
 // tensor-memory accumulator of 128 x NT FP32 each; NT a multiple of 32, so a
 // column half is a legal MMA width); B is padded to Np = ntiles * NT rows.
-// The workspace holds the split A planes, the split Toeplitz planes (a
-// function of the kernel and W only, split once per kernel) and the error
-// flag.
+// The workspace holds the split Toeplitz planes (a function of the kernel
+// and W only, split once per kernel), the error flag and, for the unfused
+// form only, the split A planes.
 struct Layout {
     int M, Np, NT, ntiles, Kp;
     size_t a_off, b_off, err_off, total, smem;
 };
 
-Layout layout_for(int V, int H, int W)
+Layout layout_for(int V, int H, int W, bool fused)
 {
     Layout L{};
     L.M = V * H;
@@ -480,27 +643,32 @@ Layout layout_for(int V, int H, int W)
     L.NT = ((n16 + L.ntiles - 1) / L.ntiles + 31) / 32 * 32;
     L.Np = L.ntiles * L.NT;
     L.Kp = (W + BK - 1) / BK * BK;
-    L.smem = 1024 + gemm_smem_bytes(L.NT);
+    L.smem = 1024 + gemm_smem_bytes(L.NT, fused);
     L.b_off = 0;
-    L.a_off = (3 * (size_t)L.Np * L.Kp * 2 + 1023) / 1024 * 1024;
-    L.err_off = L.a_off + (3 * (size_t)L.M * L.Kp * 2 + 1023) / 1024 * 1024;
-    L.total = L.err_off + 256;
+    L.err_off = (3 * (size_t)L.Np * L.Kp * 2 + 1023) / 1024 * 1024;
+    L.a_off = L.err_off + 1024;
+    L.total = L.a_off + (fused ? 0 : (3 * (size_t)L.M * L.Kp * 2 + 1023) / 1024 * 1024);
     return L;
 }
 
 }  // namespace
 
-size_t ramp_gemm_workspace_bytes(int V, int H, int W) { return layout_for(V, H, W).total; }
+bool ramp_gemm_fused(const float* proj, int W)
+{
+    return W % 4 == 0 && (reinterpret_cast<uintptr_t>(proj) & 15) == 0;
+}
+
+size_t ramp_gemm_workspace_bytes(int V, int H, int W, bool fused) { return layout_for(V, H, W, fused).total; }
 
 cudaError_t launch_ramp_gemm_bf16x3(const float* proj, float* out, const float* hT, const FilterView* views,
                                     const float* wts, float pitch, float sad, int V, int H, int W, void* workspace,
                                     int* b_ready, cudaStream_t st)
 {
     if (W < 16 || W > 4096) return cudaErrorInvalidValue;
-    const Layout L = layout_for(V, H, W);
+    const bool fused = ramp_gemm_fused(proj, W);
+    const Layout L = layout_for(V, H, W, fused);
     if (L.smem > 227 * 1024) return cudaErrorInvalidValue;
     uint8_t* ws = static_cast<uint8_t*>(workspace);
-    __nv_bfloat16* ap = reinterpret_cast<__nv_bfloat16*>(ws + L.a_off);
     __nv_bfloat16* bp = reinterpret_cast<__nv_bfloat16*>(ws + L.b_off);
     int* err = reinterpret_cast<int*>(ws + L.err_off);
     cudaError_t e = cudaMemsetAsync(err, 0, sizeof(int), st);
@@ -512,24 +680,36 @@ cudaError_t launch_ramp_gemm_bf16x3(const float* proj, float* out, const float* 
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
         if (b_ready) *b_ready = 1;
     }
-    const int avec = (W % 4 == 0 && (reinterpret_cast<uintptr_t>(proj) & 15) == 0) ? 1 : 0;
-    split_a_kernel<<<dim3((unsigned)L.M, (unsigned)((L.Kp + 1023) / 1024)), 128, 0, st>>>(proj, wts, L.M, H, W, L.Kp,
-                                                                                      avec, ap);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
     CUtensorMap tmA, tmB;
-    if (!make_map(&tmA, ap, L.M, L.Kp, BM) || !make_map(&tmB, bp, L.Np, L.Kp, L.NT / 2))
-        return cudaErrorInvalidValue;
+    if (!make_map(&tmB, bp, L.Np, L.Kp, L.NT / 2)) return cudaErrorInvalidValue;
+    if (fused) {
+        if (!make_p_map(&tmA, proj, L.M, W)) return cudaErrorInvalidValue;
+    } else {
+        // rows not 16-byte aligned: split A into the workspace first
+        __nv_bfloat16* ap = reinterpret_cast<__nv_bfloat16*>(ws + L.a_off);
+        split_a_kernel<<<dim3((unsigned)L.M, (unsigned)((L.Kp + 1023) / 1024)), 128, 0, st>>>(proj, wts, L.M, H, W,
+                                                                                          L.Kp, ap);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        if (!make_map(&tmA, ap, L.M, L.Kp, BM)) return cudaErrorInvalidValue;
+    }
     const int vec = (W % 4 == 0 && (reinterpret_cast<uintptr_t>(out) & 15) == 0) ? 1 : 0;
-    GemmArgs g{out, views, pitch, sad, L.M, H, W, L.NT, L.Kp, L.Kp / BK, vec, err};
-    e = cudaFuncSetAttribute(ramp_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem);
-    if (e != cudaSuccess) return e;
-    ramp_gemm_kernel<<<dim3((L.M + BM - 1) / BM, L.ntiles), kThreads, L.smem, st>>>(tmA, tmB, g);
+    GemmArgs g{out, views, fused ? wts : nullptr, pitch, sad, L.M, H, W, L.NT, L.Kp, L.Kp / BK, vec, err};
+    const dim3 grid((L.M + BM - 1) / BM, L.ntiles);
+    if (fused) {
+        e = cudaFuncSetAttribute(ramp_gemm_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem);
+        if (e != cudaSuccess) return e;
+        ramp_gemm_kernel<true><<<grid, kThreads, L.smem, st>>>(tmA, tmB, g);
+    } else {
+        e = cudaFuncSetAttribute(ramp_gemm_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem);
+        if (e != cudaSuccess) return e;
+        ramp_gemm_kernel<false><<<grid, kThreads, L.smem, st>>>(tmA, tmB, g);
+    }
     return cudaGetLastError();
 }
 
 int ramp_gemm_error_flag(void* workspace, int V, int H, int W, cudaStream_t st)
 {
-    const Layout L = layout_for(V, H, W);
+    const Layout L = layout_for(V, H, W, true);  // the flag's place is the same in both layouts
     int h = 0;
     if (cudaMemcpyAsync(&h, static_cast<uint8_t*>(workspace) + L.err_off, sizeof(int), cudaMemcpyDeviceToHost, st) !=
             cudaSuccess ||
