@@ -209,9 +209,23 @@ __global__ void __launch_bounds__(256) bp_cull_kernel(FdkParams f, const BpView*
     if (lane == 0) keep[wid] = m;
 }
 
-template <int ZB, int MINB>
+// Launch constants of the backprojection, formed on the host in the same
+// IEEE double operations as the device would (kernel parameters, so they
+// are read from the constant bank instead of occupying registers).
+struct BpConst {
+    double pitch;    // piso * mpn / W: detector pitch at the isocentre
+    double inv_sad;  // 1 / sad
+    double cp;       // N / 2 - 0.5: the volume centre in voxels
+};
+
+static_assert(sizeof(BpView) == 32, "BpView is staged as four 8-byte words");
+
+// SV: the view table is copied to shared memory at block start (the
+// per-view loads at the head of each set-up chain then come from shared
+// memory instead of through L1).
+template <int ZB, int MINB, bool SV>
 __global__ void __launch_bounds__(256, MINB) backproject_kernel(
-    FdkParams f, const BpView* __restrict__ views, const float* __restrict__ filt,
+    FdkParams f, BpConst k, const BpView* __restrict__ views, const float* __restrict__ filt,
     float* __restrict__ vol_f32, short* __restrict__ vol_i16, const unsigned* __restrict__ keep)
 {
     // each warp takes a TW x (32 / TW) tile of the block's 32 x 8 columns:
@@ -229,7 +243,7 @@ __global__ void __launch_bounds__(256, MINB) backproject_kernel(
     float acc[ZB];
 #pragma unroll
     for (int i = 0; i < ZB; i++) acc[i] = 0.0f;
-    const double pitch = f.piso * f.mpn / f.W;
+    const double pitch = k.pitch;
     const double zz0 = f.zstart + z0 * f.step;
     const int W = f.W, H = f.H;
     // Slices of this block that no column of the mask sees in any view (the
@@ -250,15 +264,22 @@ __global__ void __launch_bounds__(256, MINB) backproject_kernel(
     // that contributes nothing to any column of the tile is dropped for the
     // whole block.  The kept views are visited in order, so the accumulation
     // order and the volume are those of visiting every view.
-    extern __shared__ unsigned s_views[];  // bit th set: view th is kept
+    extern __shared__ __align__(16) unsigned char s_raw[];
+    const BpView* s_bv = reinterpret_cast<const BpView*>(s_raw);  // SV: [V]
+    unsigned* s_views = reinterpret_cast<unsigned*>(s_raw + (SV ? (size_t)f.V * sizeof(BpView) : 0));
     {
+        const int tid = threadIdx.y * 32 + threadIdx.x;
         const int nwords = (f.V + 31) >> 5;
         const int blk = (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
-        for (int i = threadIdx.y * 32 + threadIdx.x; i < nwords; i += 256)
-            s_views[i] = __ldg(keep + (size_t)blk * nwords + i);
+        for (int i = tid; i < nwords; i += 256) s_views[i] = __ldg(keep + (size_t)blk * nwords + i);
+        if (SV) {
+            const unsigned long long* src = reinterpret_cast<const unsigned long long*>(views);
+            unsigned long long* dst = reinterpret_cast<unsigned long long*>(s_raw);
+            for (int i = tid; i < f.V * 4; i += 256) dst[i] = __ldg(src + i);
+        }
     }
-    const double cp = (double)f.N / 2.0 - 0.5;
-    const double inv_sad = 1.0 / f.sad;
+    const double cp = k.cp;
+    const double inv_sad = k.inv_sad;
     __syncthreads();
     if (!valid) return;
     const bool full = z0 + ZB <= f.Z;  // every slice of the block exists
@@ -267,7 +288,7 @@ __global__ void __launch_bounds__(256, MINB) backproject_kernel(
         const double yy = -(y - cp) * f.scale;
         for (int th = 0; th < f.V; th++) {
             if (!((s_views[th >> 5] >> (th & 31)) & 1u)) continue;
-            const BpView bv = views[th];
+            const BpView bv = SV ? s_bv[th] : views[th];
             const double cs = bv.cs, sn = bv.sn;
             // FP64 detector coordinates of this column (:76-83)
             const double X = xx * cs + yy * sn;
@@ -415,19 +436,32 @@ cudaError_t launch_backproject(const FdkParams& f, const BpView* d_views, const 
     constexpr int ZB = VCBCT_BP_ZB;
     dim3 block(32, 8);
     dim3 grid((f.N + 31) / 32, (f.N + 7) / 8, (f.Z + ZB - 1) / ZB);
+    BpConst k;
+    k.pitch = f.piso * f.mpn / f.W;
+    k.inv_sad = 1.0 / f.sad;
+    k.cp = (double)f.N / 2.0 - 0.5;
     const int nblocks = (int)(grid.x * grid.y * grid.z);
     const long nwarps = (long)nblocks * ((f.V + 31) / 32);
     bp_cull_kernel<ZB><<<(unsigned)((nwarps * 32 + 255) / 256), 256, 0, st>>>(f, d_views, (int)grid.x, (int)grid.y,
                                                                                nblocks, keep);
-    const size_t smem = (size_t)((f.V + 31) / 32) * sizeof(unsigned);
+    // the view table goes to shared memory where it fits the default 48 KB
+    // with the view mask
+    const size_t mask_bytes = (size_t)((f.V + 31) / 32) * sizeof(unsigned);
+    const size_t table_bytes = (size_t)f.V * sizeof(BpView);
+    const bool sv = table_bytes + mask_bytes <= 48 * 1024;
+    const size_t smem = mask_bytes + (sv ? table_bytes : 0);
     // resident blocks per SM (the register cap): VCBCT_BP_MIN_BLOCKS by
     // default, 5 or 6 through the environment variable of the same name
     int minb = VCBCT_BP_MIN_BLOCKS;
     if (const char* e = std::getenv("VCBCT_BP_MIN_BLOCKS")) minb = std::atoi(e) == 6 ? 6 : 5;
-    if (minb == 5)
-        backproject_kernel<ZB, 5><<<grid, block, smem, st>>>(f, d_views, filt, vol_f32, vol_i16, keep);
+    if (minb == 5 && sv)
+        backproject_kernel<ZB, 5, true><<<grid, block, smem, st>>>(f, k, d_views, filt, vol_f32, vol_i16, keep);
+    else if (minb == 5)
+        backproject_kernel<ZB, 5, false><<<grid, block, smem, st>>>(f, k, d_views, filt, vol_f32, vol_i16, keep);
+    else if (sv)
+        backproject_kernel<ZB, 6, true><<<grid, block, smem, st>>>(f, k, d_views, filt, vol_f32, vol_i16, keep);
     else
-        backproject_kernel<ZB, 6><<<grid, block, smem, st>>>(f, d_views, filt, vol_f32, vol_i16, keep);
+        backproject_kernel<ZB, 6, false><<<grid, block, smem, st>>>(f, k, d_views, filt, vol_f32, vol_i16, keep);
     return cudaGetLastError();
 }
 

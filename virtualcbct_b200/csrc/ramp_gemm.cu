@@ -32,67 +32,17 @@
 #include <cuda.h>
 #include <cuda_bf16.h>
 
+#include "async_copy.cuh"
 #include "internal.h"
 
 namespace vcbct {
 namespace {
 
+using namespace async_copy;
+
 constexpr int BM = 128;           // rows per CTA tile (UMMA M)
 constexpr int BK = 64;            // K per stage: 64 bf16 = one 128-byte swizzle row
 constexpr int kThreads = 320;     // 10 warps
-constexpr long long kWaitCycles = 4000000000LL;  // ~2 s at 1.9 GHz
-
-__device__ __forceinline__ uint32_t smem_u32(const void* p)
-{
-    return (uint32_t)__cvta_generic_to_shared(p);
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count)
-{
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes)
-{
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
-                 : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t phase)
-{
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(phase)
-        : "memory");
-    return ok != 0;
-}
-
-// Bounded wait on an mbarrier phase; false (and the error flag) on timeout.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase, int* err)
-{
-    const long long t0 = clock64();
-    while (!mbar_try_wait(bar, phase)) {
-        if (clock64() - t0 > kWaitCycles) {
-            atomicExch(err, 1);
-            return false;
-        }
-    }
-    return true;
-}
-
-__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, uint64_t* bar, int c0,
-                                            int c1, int c2)
-{
-    asm volatile(
-        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
-        " [%0], [%1, {%3, %4, %5}], [%2];" ::"r"(smem_u32(dst)),
-        "l"(map), "r"(smem_u32(bar)), "r"(c0), "r"(c1), "r"(c2)
-        : "memory");
-}
 
 // Shared-memory matrix descriptor of a K-major tile with 128-byte swizzle:
 // rows of 128 B, 8-row atoms 1024 B apart (stride byte offset), start address
@@ -221,15 +171,6 @@ __host__ __device__ constexpr size_t gemm_smem_bytes(int NT, bool fused)
            (size_t)b_stages(fused) * (NT / 2) * BK * 2 + 8 * (2 + 2 * kAStages + 2 * b_stages(fused) + 1) + 16;
 }
 
-__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int c0, int c1)
-{
-    asm volatile(
-        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
-        " [%0], [%1, {%3, %4}], [%2];" ::"r"(smem_u32(dst)),
-        "l"(map), "r"(smem_u32(bar)), "r"(c0), "r"(c1)
-        : "memory");
-}
-
 __device__ __forceinline__ void st_shared_u32(uint32_t addr, uint32_t v)
 {
     asm volatile("st.shared.b32 [%0], %1;" ::"r"(addr), "r"(v) : "memory");
@@ -240,11 +181,6 @@ __device__ __forceinline__ float2 ld_shared_f2(uint32_t addr)
     float2 v;
     asm volatile("ld.shared.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "r"(addr) : "memory");
     return v;
-}
-
-__device__ __forceinline__ void mbar_arrive(uint64_t* bar)
-{
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
 // Fused form: one K tile of the A operand made in shared memory from the
@@ -466,7 +402,7 @@ ramp_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant_
                 convert_a_tile(g, m0, kt, pw, lane, smem_u32(ptile), smem_u32(abuf + (size_t)sa * kAStageBytes),
                                wfast, rsplit, wa, wb);
                 // generic-proxy stores -> visible to the tensor core (async proxy)
-                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                fence_proxy_async();
                 __syncwarp();
                 if (lane == 0) {
                     mbar_arrive(p_empty);
@@ -575,23 +511,6 @@ __global__ void split_b_kernel(const float* __restrict__ hT, int W, int Np, int 
     planes[i] = a;
     planes[plane + i] = b;
     planes[2 * plane + i] = c;
-}
-
-typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
-                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
-                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-
-EncodeTiledFn encode_fn()
-{
-    static EncodeTiledFn fn = nullptr;
-    if (!fn) {
-        void* p = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
-            q == cudaDriverEntryPointSuccess)
-            fn = reinterpret_cast<EncodeTiledFn>(p);
-    }
-    return fn;
 }
 
 // 3D bf16 tensor [planes][rows][Kp] with box {64, box_rows, 1}, 128-byte swizzle.
