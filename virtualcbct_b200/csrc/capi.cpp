@@ -1424,6 +1424,8 @@ struct vcbct_fdk {
     DevBuf wts;       // float [V][W] redundancy weights (optional)
     DevBuf in, mid, outv, outs, work;
     DevBuf bpkeep;    // per-block view masks of the backprojection
+    int bp_keep_ready = 0;    // the masks in `bpkeep` are made (they follow the geometry only) ...
+    void* bp_keep_at = nullptr;  // ... at this address
     int have_wts = 0;
     int b_ready = 0;          // the tensor-core filter's Toeplitz planes are split in `work`
     void* b_at = nullptr;     // ... at this address
@@ -1660,7 +1662,7 @@ extern "C" int vcbct_fdk_filter(vcbct_fdk* f, const float* proj, float* filtered
                                             g.proj_width, st));
     } else if (method == VCBCT_FILTER_BF16X3) {
         VCBCT_CUDA_TRY(f->work.ensure(ramp_gemm_workspace_bytes(g.n_views, g.proj_height, g.proj_width,
-                                                                 ramp_gemm_fused(din, g.proj_width))));
+                                                                 ramp_gemm_fused(din, dout, g.proj_width))));
         if (f->work.p != f->b_at) {
             f->b_ready = 0;
             f->b_at = f->work.p;
@@ -1706,7 +1708,12 @@ extern "C" int vcbct_fdk_backproject(vcbct_fdk* f, const float* filtered, float*
         }
     }
     VCBCT_CUDA_TRY(f->bpkeep.ensure(backproject_workspace_bytes(f->fp)));
-    VCBCT_CUDA_TRY(launch_backproject(f->fp, f->bviews.as<BpView>(), din, df, di, f->bpkeep.as<unsigned>(), st));
+    if (f->bpkeep.p != f->bp_keep_at) {
+        f->bp_keep_ready = 0;
+        f->bp_keep_at = f->bpkeep.p;
+    }
+    VCBCT_CUDA_TRY(launch_backproject(f->fp, f->bviews.as<BpView>(), din, df, di, f->bpkeep.as<unsigned>(),
+                                      &f->bp_keep_ready, st));
     if (!on_device) {
         if (vol_f32) VCBCT_CUDA_TRY(cudaMemcpyAsync(vol_f32, df, nv * sizeof(float), cudaMemcpyDeviceToHost, st));
         if (vol_i16) VCBCT_CUDA_TRY(cudaMemcpyAsync(vol_i16, di, nv * sizeof(short), cudaMemcpyDeviceToHost, st));

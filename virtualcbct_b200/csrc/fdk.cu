@@ -286,8 +286,13 @@ __global__ void __launch_bounds__(256, MINB) backproject_kernel(
     if (inmask && seen) {
         const double xx = (x - cp) * f.scale;
         const double yy = -(y - cp) * f.scale;
-        for (int th = 0; th < f.V; th++) {
-            if (!((s_views[th >> 5] >> (th & 31)) & 1u)) continue;
+        // the kept views in order, one mask word at a time (the culled ones
+        // cost nothing)
+        const int nwords = (f.V + 31) >> 5;
+        for (int wi = 0; wi < nwords; wi++)
+        for (unsigned wd = s_views[wi]; wd != 0u;) {
+            const int th = wi * 32 + __ffs(wd) - 1;
+            wd &= wd - 1u;
             const BpView bv = SV ? s_bv[th] : views[th];
             const double cs = bv.cs, sn = bv.sn;
             // FP64 detector coordinates of this column (:76-83)
@@ -431,7 +436,8 @@ size_t backproject_workspace_bytes(const FdkParams& f)
 }
 
 cudaError_t launch_backproject(const FdkParams& f, const BpView* d_views, const float* filt,
-                               float* vol_f32, short* vol_i16, unsigned* keep, cudaStream_t st)
+                               float* vol_f32, short* vol_i16, unsigned* keep, int* keep_ready,
+                               cudaStream_t st)
 {
     constexpr int ZB = VCBCT_BP_ZB;
     dim3 block(32, 8);
@@ -442,8 +448,14 @@ cudaError_t launch_backproject(const FdkParams& f, const BpView* d_views, const 
     k.cp = (double)f.N / 2.0 - 0.5;
     const int nblocks = (int)(grid.x * grid.y * grid.z);
     const long nwarps = (long)nblocks * ((f.V + 31) / 32);
-    bp_cull_kernel<ZB><<<(unsigned)((nwarps * 32 + 255) / 256), 256, 0, st>>>(f, d_views, (int)grid.x, (int)grid.y,
-                                                                               nblocks, keep);
+    if (!keep_ready || !*keep_ready) {
+        // the view masks follow the geometry and the views only: made once
+        bp_cull_kernel<ZB><<<(unsigned)((nwarps * 32 + 255) / 256), 256, 0, st>>>(f, d_views, (int)grid.x,
+                                                                                   (int)grid.y, nblocks, keep);
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        if (keep_ready) *keep_ready = 1;
+    }
     // the view table goes to shared memory where it fits the default 48 KB
     // with the view mask
     const size_t mask_bytes = (size_t)((f.V + 31) / 32) * sizeof(unsigned);

@@ -147,20 +147,24 @@ struct BpView {
     float dbeta;     // half the neighbouring angular gap (:45-71)
     float pad;
 };
-// keep: backproject_workspace_bytes(f) of device scratch (the per-block view
-// masks, rewritten by every launch).
+// keep: backproject_workspace_bytes(f) of device scratch holding the
+// per-block view masks, a function of the geometry and the views only: with
+// *keep_ready set they are taken as made and not redone; the launch sets it
+// once it has queued them (keep_ready may be null: made every call).
 size_t backproject_workspace_bytes(const FdkParams& f);
 cudaError_t launch_backproject(const FdkParams& f, const BpView* d_views, const float* filt,
-                               float* vol_f32, short* vol_i16, unsigned* keep, cudaStream_t st);
+                               float* vol_f32, short* vol_i16, unsigned* keep, int* keep_ready,
+                               cudaStream_t st);
 
 // BF16 3-term split tensor-core ramp filter (tcgen05).  The workspace holds
 // the split Toeplitz planes: with *b_ready set they are taken as already
 // split from hT into this workspace and are not redone; the launch sets it
 // once it has queued the split (b_ready may be null: split every call).
-// The fused form (rows of `proj` 16-byte aligned: W % 4 == 0 and an aligned
-// base, ramp_gemm_fused) splits -ln p inside the GEMM; the other needs room
-// for the split A planes as well: size the workspace with the same flag.
-bool ramp_gemm_fused(const float* proj, int W);
+// The fused form (rows of `proj` and `out` 16-byte aligned: W % 4 == 0 and
+// aligned bases, ramp_gemm_fused) splits -ln p inside the GEMM and stores
+// through TMA; the other needs room for the split A planes as well: size the
+// workspace with the same flag.
+bool ramp_gemm_fused(const float* proj, const float* out, int W);
 size_t ramp_gemm_workspace_bytes(int V, int H, int W, bool fused);
 cudaError_t launch_ramp_gemm_bf16x3(const float* proj, float* out, const float* hT,
                                     const FilterView* views, const float* wts, float pitch,

@@ -42,7 +42,7 @@ using namespace async_copy;
 
 constexpr int BM = 128;           // rows per CTA tile (UMMA M)
 constexpr int BK = 64;            // K per stage: 64 bf16 = one 128-byte swizzle row
-constexpr int kThreads = 320;     // 10 warps
+constexpr int kThreads = 576;     // 18 warps
 
 // Shared-memory matrix descriptor of a K-major tile with 128-byte swizzle:
 // rows of 128 B, 8-row atoms 1024 B apart (stride byte offset), start address
@@ -140,6 +140,27 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v)
     for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
 }
 
+// The same load without its wait, and the wait as a use of the registers it
+// fills (so that no read of them is scheduled before it): the next chunk's
+// load overlaps the current chunk's arithmetic.
+__device__ __forceinline__ void tmem_ld16_async(uint32_t taddr, uint32_t (&r)[16])
+{
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_wait_ld(uint32_t (&r)[16])
+{
+    asm volatile("tcgen05.wait::ld.sync.aligned;"
+                 : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]),
+                   "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]), "+r"(r[12]), "+r"(r[13]), "+r"(r[14]),
+                   "+r"(r[15])
+                 :
+                 : "memory");
+}
+
 struct GemmArgs {
     float* out;
     const FilterView* views;
@@ -150,7 +171,7 @@ struct GemmArgs {
     int* err;
 };
 
-constexpr int kEpiWarps = 8;                    // warps 2-9: A planes (fused form), then the epilogue
+constexpr int kEpiWarps = 16;                   // warps 2-17: A planes (fused form), then the epilogue
 static_assert(kThreads == 64 + 32 * kEpiWarps, "warp 0 TMA, warp 1 MMA, the rest A planes / epilogue");
 constexpr uint32_t kHalfCol = 256;              // TMEM column of the second column half
 constexpr int kAStages = 2;                     // A ring: the three planes of one K tile each
@@ -169,6 +190,28 @@ __host__ __device__ constexpr size_t gemm_smem_bytes(int NT, bool fused)
 {
     return (fused ? (size_t)kPTileBytes : 0) + (size_t)kAStages * kAStageBytes +
            (size_t)b_stages(fused) * (NT / 2) * BK * 2 + 8 * (2 + 2 * kAStages + 2 * b_stages(fused) + 1) + 16;
+}
+
+// Shared -> global tensor store of one box (clipped at the tensor's edges),
+// tracked as a bulk group of the issuing thread.
+__device__ __forceinline__ void tma_store_2d(const CUtensorMap* map, const void* src, int c0, int c1)
+{
+    asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%2, %3}], [%1];" ::"l"(map),
+                 "r"(smem_u32(src)), "r"(c0), "r"(c1)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+// this thread's bulk groups but the newest one have finished reading shared memory
+__device__ __forceinline__ void bulk_wait_read_all_but_one()
+{
+    asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
+}
+// all of this thread's bulk groups are complete
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+
+__device__ __forceinline__ void st_shared_v4(uint32_t addr, float a, float b, float c, float d)
+{
+    asm volatile("st.shared.v4.f32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "f"(a), "f"(b), "f"(c), "f"(d) : "memory");
 }
 
 __device__ __forceinline__ void st_shared_u32(uint32_t addr, uint32_t v)
@@ -240,7 +283,8 @@ __device__ __forceinline__ bool warp_wait(uint64_t* bar, uint32_t phase, int* er
 
 template <bool FUSED>
 __global__ void __launch_bounds__(kThreads, 1)
-ramp_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, GemmArgs g)
+ramp_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                 const __grid_constant__ CUtensorMap tmO, GemmArgs g)
 {
     constexpr int SB = b_stages(FUSED);
     extern __shared__ uint8_t smem_raw[];
@@ -293,14 +337,17 @@ ramp_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant_
         // TMA producer.  Per K tile: the A operand (fused form: the FP32 tile
         // of p; otherwise the three split A planes, one A stage), then the B
         // planes 2, 1, 0, each as two column halves (six B stages) -- the
-        // order the consumers take them in.
-        int na = 0, nb = 0;  // stages issued
+        // order the consumers take them in.  Fused form: p tile n + 1 is
+        // requested as soon as the converters have released tile n, polled
+        // while the thread waits for B ring stages.
+        int na = 0, nb = 0;  // stages (fused form: p tiles) issued
         bool ok = true;
-        if (FUSED) {  // the first p tile; tile kt + 1 follows B half 3 of tile kt
+        auto issue_p = [&]() {
             mbar_expect_tx(p_full, kPTileBytes);
-            tma_load_2d(ptile, &tmA, p_full, 0, m0);
-            na = 1;
-        }
+            tma_load_2d(ptile, &tmA, p_full, na * BK, m0);
+            na++;
+        };
+        if (FUSED) issue_p();
         for (int kt = 0; kt < g.ktiles && ok; kt++) {
             if (!FUSED) {
                 const int sa = kt % kAStages;
@@ -310,21 +357,33 @@ ramp_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant_
                 for (int i = 0; i < 3; i++) tma_load_3d(da + i * kAPlaneBytes, &tmA, &a_full[sa], kt * BK, m0, i);
                 na = kt + 1;
             }
-            for (int q = 0; q < 6; q++) {
-                if (FUSED && q == 3 && kt + 1 < g.ktiles) {
-                    // the staged tile is free once the converters have read it
-                    if (!(ok = mbar_wait(p_empty, kt & 1, g.err))) break;
-                    mbar_expect_tx(p_full, kPTileBytes);
-                    tma_load_2d(ptile, &tmA, p_full, (kt + 1) * BK, m0);
-                    na = kt + 2;
-                }
+            for (int q = 0; q < 6 && ok; q++) {
                 const int kb = kt * 6 + q, s = kb % SB;
-                if (kb >= SB && !(ok = mbar_wait(&b_empty[s], ((kb / SB) - 1) & 1, g.err))) break;
+                if (kb >= SB) {
+                    // bounded wait for the stage, serving the p tiles meanwhile
+                    const uint32_t ph = ((kb / SB) - 1) & 1;
+                    const long long t0 = clock64();
+                    while (!mbar_try_wait(&b_empty[s], ph)) {
+                        if (FUSED && na < g.ktiles && mbar_try_wait(p_empty, (na - 1) & 1)) issue_p();
+                        if (clock64() - t0 > kWaitCycles) {
+                            atomicExch(g.err, 1);
+                            ok = false;
+                            break;
+                        }
+                    }
+                    if (!ok) break;
+                }
+                if (FUSED && na < g.ktiles && mbar_try_wait(p_empty, (na - 1) & 1)) issue_p();
                 const int plane = 2 - q / 2, h = q % 2;
                 mbar_expect_tx(&b_full[s], bh_bytes);
                 tma_load_3d(bbuf + (size_t)s * bh_bytes, &tmB, &b_full[s], kt * BK, n0 + h * NH, plane);
                 nb = kb + 1;
             }
+        }
+        // p tiles not yet requested when the last B stage went out
+        while (FUSED && ok && na < g.ktiles) {
+            if (!(ok = mbar_wait(p_empty, (na - 1) & 1, g.err))) break;
+            issue_p();
         }
         // no load may still be in flight into this CTA's shared memory when it
         // exits: wait (bounded) for the last stages issued
@@ -410,12 +469,14 @@ ramp_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant_
                 }
             }
         }
-        // epilogue: TMEM -> registers -> cosine factor -> global; two warps
+        // epilogue: TMEM -> registers -> cosine factor -> global; four warps
         // per TMEM lane quarter (a warp may access lanes 32 (warp % 4) ..),
-        // each taking every other 16-column chunk; logical column c lies at
+        // grp = (warp - 2) / 4 choosing the column half (grp / 2) and every
+        // other 16-column chunk of it (grp % 2); logical column c lies at
         // TMEM column c (first half) or kHalfCol + c - NT/2 (second half)
         const int q = warp % 4;
-        const int half = (warp - 2) / 4;
+        const int grp = (warp - 2) / 4;
+        const int half = grp >> 1, part = grp & 1;
         const int row = m0 + 32 * q + lane;
         if (ok && warp_wait(accum, 0, g.err)) {
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -427,30 +488,95 @@ ramp_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant_
                 xcs = fv.xcs;
             }
             // cosine factor sad / sqrt(sad^2 + pos1^2 + pos2^2) from the
-            // reciprocal square root (2 ulp), stored 16 bytes at a time
+            // reciprocal square root (2 ulp)
             const float sad = g.sad, base2 = fmaf(pos2, pos2, sad * sad);
-            for (int c = 16 * half; c < g.NT; c += 32) {
-                float v16[16];
-                const uint32_t col = c < NH ? (uint32_t)c : kHalfCol + (uint32_t)(c - NH);
-                tmem_ld16(taddr + ((uint32_t)(32 * q) << 16) + col, v16);
-                const int mb = n0 + c;
-                if (row < g.M && mb < g.W) {
-                    float* o = g.out + (size_t)row * g.W + mb;
+            if (FUSED) {
+                // Warp (q, half, part) drains TMEM lane quarter q of column
+                // half `half` (the logical columns half NH .. half NH + NH - 1),
+                // the 16-column chunks part, part + 2, ..., the next chunk's
+                // load in flight while this one is scaled and stored.  Each 32-row x 16-column chunk goes
+                // through a 2 KB staging buffer (two per warp, in the A ring,
+                // free once the last MMA has completed) in the layout of a
+                // CU_TENSOR_MAP_SWIZZLE_64B box (row r at 64 r bytes, 16-byte
+                // chunk j at j ^ ((r >> 1) & 3): conflict-free vector stores),
+                // and one TMA store writes it whole: full sectors, rows and
+                // columns past the detector clipped, instead of 32 rows
+                // touched by every warp store.
+                uint8_t* stage = abuf + (size_t)(warp - 2) * 4096;
+                const int r0 = m0 + 32 * q;
+                const uint32_t tq = taddr + ((uint32_t)(32 * q) << 16) + (uint32_t)half * kHalfCol;
+                const int nch = NH / 16;
+                int nst = 0;
+                uint32_t cur[16], nxt[16];
+                if (part < nch) {
+                    tmem_ld16_async(tq + 16u * (uint32_t)part, cur);
+                    tmem_wait_ld(cur);
+                }
+                for (int i = part; i < nch; i += 2) {
+                    if (i + 2 < nch) tmem_ld16_async(tq + 16u * (uint32_t)(i + 2), nxt);
+                    const int mb = n0 + half * NH + 16 * i;
+                    if (mb < g.W && r0 < g.M) {  // else the whole box lies past the detector
+                        float v16[16];
+                        const float fmb = (float)mb;  // + j exactly: column indices are far below 2^24
 #pragma unroll
-                    for (int i = 0; i < 16; i++) {
-                        const float pos1 = fabsf(xcs + (float)(mb + i)) * g.pitch;
-                        v16[i] *= sad * rsqrtf(fmaf(pos1, pos1, base2));
+                        for (int j = 0; j < 16; j++) {
+                            const float pos1 = fabsf(xcs + (fmb + (float)j)) * g.pitch;
+                            v16[j] = __uint_as_float(cur[j]) * (sad * rsqrtf(fmaf(pos1, pos1, base2)));
+                        }
+                        uint8_t* buf = stage + (nst & 1) * 2048;
+                        if (nst >= 2) {
+                            // the store issued from this buffer two chunks ago has read it
+                            if (lane == 0) bulk_wait_read_all_but_one();
+                            __syncwarp();
+                        }
+                        const uint32_t rb = smem_u32(buf) + (uint32_t)lane * 64u;
+                        const uint32_t sw = ((uint32_t)lane >> 1) & 3u;
+#pragma unroll
+                        for (int j = 0; j < 4; j++)
+                            st_shared_v4(rb + ((j ^ sw) << 4), v16[4 * j], v16[4 * j + 1], v16[4 * j + 2],
+                                         v16[4 * j + 3]);
+                        fence_proxy_async();
+                        __syncwarp();
+                        if (lane == 0) {
+                            tma_store_2d(&tmO, buf, mb, r0);
+                            bulk_commit();
+                        }
+                        nst++;
                     }
-                    // columns of this tile and of the detector only
-                    const int lim = min(g.W - mb, g.NT - c);
-                    if (g.vec && lim >= 16) {
+                    if (i + 2 < nch) {
+                        tmem_wait_ld(nxt);
 #pragma unroll
-                        for (int i = 0; i < 16; i += 4)
-                            *reinterpret_cast<float4*>(o + i) = make_float4(v16[i], v16[i + 1], v16[i + 2], v16[i + 3]);
-                    } else {
+                        for (int j = 0; j < 16; j++) cur[j] = nxt[j];
+                    }
+                }
+                // the stores are complete (and their buffers read) before exit
+                if (lane == 0) bulk_wait_all();
+            } else {
+                // stored 16 bytes at a time
+                for (int c = 16 * grp; c < g.NT; c += 64) {
+                    float v16[16];
+                    const uint32_t col = c < NH ? (uint32_t)c : kHalfCol + (uint32_t)(c - NH);
+                    tmem_ld16(taddr + ((uint32_t)(32 * q) << 16) + col, v16);
+                    const int mb = n0 + c;
+                    if (row < g.M && mb < g.W) {
+                        float* o = g.out + (size_t)row * g.W + mb;
 #pragma unroll
-                        for (int i = 0; i < 16; i++)
-                            if (i < lim) o[i] = v16[i];
+                        for (int i = 0; i < 16; i++) {
+                            const float pos1 = fabsf(xcs + (float)(mb + i)) * g.pitch;
+                            v16[i] *= sad * rsqrtf(fmaf(pos1, pos1, base2));
+                        }
+                        // columns of this tile and of the detector only
+                        const int lim = min(g.W - mb, g.NT - c);
+                        if (g.vec && lim >= 16) {
+#pragma unroll
+                            for (int i = 0; i < 16; i += 4)
+                                *reinterpret_cast<float4*>(o + i) =
+                                    make_float4(v16[i], v16[i + 1], v16[i + 2], v16[i + 3]);
+                        } else {
+#pragma unroll
+                            for (int i = 0; i < 16; i++)
+                                if (i < lim) o[i] = v16[i];
+                        }
                     }
                 }
             }
@@ -542,6 +668,21 @@ bool make_p_map(CUtensorMap* map, const float* proj, int M, int W)
               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// 2D FP32 tensor [M][W] (the filtered output) with box {16, 32} in the
+// 64-byte swizzle layout; stores are clipped at W and M.
+bool make_out_map(CUtensorMap* map, float* out, int M, int W)
+{
+    EncodeTiledFn fn = encode_fn();
+    if (!fn) return false;
+    cuuint64_t dims[2] = {(cuuint64_t)W, (cuuint64_t)M};
+    cuuint64_t strides[1] = {(cuuint64_t)W * 4};
+    cuuint32_t box[2] = {16, 32};
+    cuuint32_t estr[2] = {1, 1};
+    return fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, out, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+              CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 // Output columns are split into ntiles tiles of NT <= 512 columns (one
 // tensor-memory accumulator of 128 x NT FP32 each; NT a multiple of 32, so a
 // column half is a legal MMA width); B is padded to Np = ntiles * NT rows.
@@ -572,9 +713,9 @@ Layout layout_for(int V, int H, int W, bool fused)
 
 }  // namespace
 
-bool ramp_gemm_fused(const float* proj, int W)
+bool ramp_gemm_fused(const float* proj, const float* out, int W)
 {
-    return W % 4 == 0 && (reinterpret_cast<uintptr_t>(proj) & 15) == 0;
+    return W % 4 == 0 && (reinterpret_cast<uintptr_t>(proj) & 15) == 0 && (reinterpret_cast<uintptr_t>(out) & 15) == 0;
 }
 
 size_t ramp_gemm_workspace_bytes(int V, int H, int W, bool fused) { return layout_for(V, H, W, fused).total; }
@@ -584,7 +725,7 @@ cudaError_t launch_ramp_gemm_bf16x3(const float* proj, float* out, const float* 
                                     int* b_ready, cudaStream_t st)
 {
     if (W < 16 || W > 4096) return cudaErrorInvalidValue;
-    const bool fused = ramp_gemm_fused(proj, W);
+    const bool fused = ramp_gemm_fused(proj, out, W);
     const Layout L = layout_for(V, H, W, fused);
     if (L.smem > 227 * 1024) return cudaErrorInvalidValue;
     uint8_t* ws = static_cast<uint8_t*>(workspace);
@@ -599,10 +740,11 @@ cudaError_t launch_ramp_gemm_bf16x3(const float* proj, float* out, const float* 
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
         if (b_ready) *b_ready = 1;
     }
-    CUtensorMap tmA, tmB;
+    CUtensorMap tmA, tmB, tmO;
     if (!make_map(&tmB, bp, L.Np, L.Kp, L.NT / 2)) return cudaErrorInvalidValue;
+    tmO = tmB;  // the unfused form stores without TMA
     if (fused) {
-        if (!make_p_map(&tmA, proj, L.M, W)) return cudaErrorInvalidValue;
+        if (!make_p_map(&tmA, proj, L.M, W) || !make_out_map(&tmO, out, L.M, W)) return cudaErrorInvalidValue;
     } else {
         // rows not 16-byte aligned: split A into the workspace first
         __nv_bfloat16* ap = reinterpret_cast<__nv_bfloat16*>(ws + L.a_off);
@@ -617,11 +759,11 @@ cudaError_t launch_ramp_gemm_bf16x3(const float* proj, float* out, const float* 
     if (fused) {
         e = cudaFuncSetAttribute(ramp_gemm_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem);
         if (e != cudaSuccess) return e;
-        ramp_gemm_kernel<true><<<grid, kThreads, L.smem, st>>>(tmA, tmB, g);
+        ramp_gemm_kernel<true><<<grid, kThreads, L.smem, st>>>(tmA, tmB, tmO, g);
     } else {
         e = cudaFuncSetAttribute(ramp_gemm_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem);
         if (e != cudaSuccess) return e;
-        ramp_gemm_kernel<false><<<grid, kThreads, L.smem, st>>>(tmA, tmB, g);
+        ramp_gemm_kernel<false><<<grid, kThreads, L.smem, st>>>(tmA, tmB, tmO, g);
     }
     return cudaGetLastError();
 }
