@@ -299,12 +299,15 @@ __global__ void __launch_bounds__(256, MINB) backproject_kernel(
             const double X = xx * cs + yy * sn;
             const double Y = -xx * sn + yy * cs;
             const double L2 = 1.0 - Y * inv_sad;
-            const double g = 1.0 / (L2 * pitch);
+            // the correctly rounded reciprocal: 1.0 / (L2 pitch) to the bit
+            const double g = __drcp_rn(L2 * pitch);
             const double U = X * g;
             const double Uf = floor(U);
             const float wu = (float)(U - Uf);
             const double UUU = bv.ushift + U;
-            const int UU = (int)floor(UUU);
+            // floor and conversion in one (round-down conversion; out of
+            // range or NaN gives INT_MIN or INT_MAX, both rejected below)
+            const int UU = __double2int_rd(UUU);
             if (UU < 0 || UU > W - 1) continue;
             const double zeta0 = (double)(H / 2) + zz0 * g;
             // every slice of the block projects above or below the detector
