@@ -220,6 +220,16 @@ struct BpConst {
 
 static_assert(sizeof(BpView) == 32, "BpView is staged as four 8-byte words");
 
+// Slice block of launch index i of n, from the middle of the volume out
+// (c, c + 1, c - 1, c + 2, ... with c = (n - 1) / 2): the blocks near the
+// slab's centre, seen by every view, are the longest and start first, the
+// short ones at the cone's edges fill the last wave.
+__device__ __forceinline__ int bp_zblock(int i, int n)
+{
+    const int c = (n - 1) / 2, off = (i + 1) >> 1;
+    return (i & 1) ? c + off : c - off;
+}
+
 // SV: the view table is copied to shared memory at block start (the
 // per-view loads at the head of each set-up chain then come from shared
 // memory instead of through L1).
@@ -236,7 +246,8 @@ __global__ void __launch_bounds__(256, MINB) backproject_kernel(
     constexpr int TW = VCBCT_BP_TILE, TH = 32 / TW, WX = 32 / TW;
     const int x = blockIdx.x * 32 + (threadIdx.y % WX) * TW + (threadIdx.x % TW);
     const int y = blockIdx.y * 8 + (threadIdx.y / WX) * TH + (threadIdx.x / TW);
-    const int z0 = blockIdx.z * ZB;
+    const int bz = bp_zblock(blockIdx.z, gridDim.z);
+    const int z0 = bz * ZB;
     const bool valid = x < f.N && y < f.N;
     const double R = (double)(f.N - 1) / 2.0;
     const bool inmask = valid && ((double)y - R) * ((double)y - R) + ((double)x - R) * ((double)x - R) <= R * R;
@@ -270,7 +281,7 @@ __global__ void __launch_bounds__(256, MINB) backproject_kernel(
     {
         const int tid = threadIdx.y * 32 + threadIdx.x;
         const int nwords = (f.V + 31) >> 5;
-        const int blk = (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+        const int blk = (bz * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
         for (int i = tid; i < nwords; i += 256) s_views[i] = __ldg(keep + (size_t)blk * nwords + i);
         if (SV) {
             const unsigned long long* src = reinterpret_cast<const unsigned long long*>(views);
