@@ -109,7 +109,7 @@ def test_fdk_chain_short_volume_within_one_lsb(cuda):
 
 
 @pytest.mark.parametrize("V,H,W,xshift", [(6, 40, 48, 0.0), (4, 8, 400, 0.0), (3, 100, 400, 16.0),
-                                          (2, 70, 256, 2.0), (3, 10, 50, 0.0),
+                                          (2, 70, 256, 2.0), (3, 10, 50, 0.0), (3, 20, 47, 1.0),
                                           # wider than one 512-column accumulator: column tiles
                                           (2, 12, 600, 0.0), (2, 9, 800, 8.0), (2, 5, 1030, 0.0)])
 def test_bf16x3_tensor_core_filter_matches_fp64(cuda, V, H, W, xshift):

@@ -131,14 +131,12 @@ __device__ __forceinline__ f32x2 fadd2_rd(f32x2 a, f32x2 b)  // rounded toward -
 // reference's edge rules and its weight quirk (the column weight is frac(U),
 // not frac(UUU), reconstructImage.cpp:80-83).
 // Register cap (minimum resident 256-thread blocks per SM) and slices per
-// thread.  The gathers are latency-bound, so occupancy pays, but the packed
-// f32x2 slice loop needs register pairs: at 6 blocks (40 registers) it
-// spills in the loop (1e8 local loads on 270x270x200 from 360 half-fan
-// views), at 5 (48 registers) it does not and is faster on B200 (3.30 vs
-// 3.36 ms, the volume bitwise the same).  With the scalar loop, 8 slices at
-// 6 blocks measured as fast as 16 at 5 (3.39 vs 3.37 ms) and 10-19 % faster
-// where more of the volume lies in the cone; 12, 20 slices and 16 at 4
-// blocks were slower.
+// thread.  The packed f32x2 slice loop needs register pairs: with the launch
+// constants in the parameter bank, 5 blocks (48 registers) and 6 (40) both
+// run without spills on 270x270x200 from 360 half-fan views, and 5 is faster
+// on B200 (3.05 vs 3.21 ms, the volume bitwise the same).  16 slices per
+// thread at 4 or 3 blocks measured slower (3.55 / 3.49 vs 3.30 ms): more
+// columns leave the interior loop at the cone's edges.
 #ifndef VCBCT_BP_MIN_BLOCKS
 #define VCBCT_BP_MIN_BLOCKS 5
 #endif
