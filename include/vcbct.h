@@ -418,6 +418,12 @@ typedef struct {
 
 void vcbct_fdk_default_geometry(vcbct_fdk_geometry* g);
 
+/* VCBCT_FILTER_BF16X3 splits -log p inside the GEMM and stores through TMA
+ * when the rows of the projections and of the output are 16-byte aligned
+ * (proj_width % 4 == 0 and 16-byte-aligned buffers; always so for the host
+ * path, which uses the object's own device buffers); otherwise it splits in
+ * a separate pass into a larger workspace.  The results agree within the
+ * filter's 1e-5 tolerance either way. */
 enum {
     VCBCT_FILTER_DIRECT_F32 = 0, /* FP32 direct Toeplitz product (parity path) */
     VCBCT_FILTER_BF16X3 = 1      /* tcgen05 BF16 3-term split GEMM, FP32 accumulate */
