@@ -485,11 +485,51 @@ struct PairSums {
     }
 };
 
+// The same with L in shared memory (this thread's column of a [M][kLStride]
+// array): L is touched once per 32 steps, and its registers are free for the
+// walk and the interval production.
+constexpr int kLStride = 256;
 template <int M>
-struct AccumU16 : PairSums<M> {
+struct PairSumsS {
+    static constexpr int NP = (M + 1) / 2;
+    float* Ls;
+    f32x2 P2[NP];
+    float lt = 1.0f;
+    __device__ __forceinline__ float Lget(int i) const { return Ls[i * kLStride]; }
+    __device__ __forceinline__ void clear()
+    {
+#pragma unroll
+        for (int i = 0; i < M; i++) Ls[i * kLStride] = 0.0f;
+#pragma unroll
+        for (int i = 0; i < NP; i++) P2[i] = 0ull;
+    }
+    __device__ __forceinline__ void fold()
+    {
+#pragma unroll
+        for (int i = 0; i < NP; i++) {
+            float a, b;
+            f2unpack(P2[i], a, b);
+            Ls[2 * i * kLStride] = fmaf(a, lt, Ls[2 * i * kLStride]);
+            if (2 * i + 1 < M) Ls[(2 * i + 1) * kLStride] = fmaf(b, lt, Ls[(2 * i + 1) * kLStride]);
+            P2[i] = 0ull;
+        }
+    }
+    __device__ __forceinline__ void zero_L()
+    {
+#pragma unroll
+        for (int i = 0; i < M; i++) Ls[i * kLStride] = 0.0f;
+    }
+};
+
+template <int M>
+struct AccumU16 : PairSumsS<M> {
     const uint4* __restrict__ vol;
     unsigned nseg;
-    __device__ __forceinline__ AccumU16(const uint4* v) : vol(v), nseg(0u) { this->clear(); }
+    __device__ __forceinline__ AccumU16(const uint4* v, float* ls) : vol(v), nseg(0u)
+    {
+        this->Ls = ls;
+        this->clear();
+    }
     // called by all 32 lanes together; p: this lane has a segment
     __device__ __forceinline__ void lanes(bool p, int idx, float len)
     {
@@ -502,7 +542,7 @@ struct AccumU16 : PairSums<M> {
         this->P2[0] = ffma2(u16pair(v.x), l2, this->P2[0]);
         this->P2[1] = ffma2(u16pair(v.y), l2, this->P2[1]);
         this->P2[2] = ffma2(u16pair(v.z), l2, this->P2[2]);
-        if (M > 6) this->P2[3 % PairSums<M>::NP] = ffma2(u16pair(v.w), l2, this->P2[3 % PairSums<M>::NP]);
+        if (M > 6) this->P2[3 % PairSumsS<M>::NP] = ffma2(u16pair(v.w), l2, this->P2[3 % PairSumsS<M>::NP]);
         nseg++;
     }
     // a segment of absolute length len (cm), straight into L
@@ -514,7 +554,7 @@ struct AccumU16 : PairSums<M> {
         for (int i = 0; i < M; i++) {
             float a, b;
             f2unpack(u16pair(w[i / 2]), a, b);
-            this->L[i] = fmaf((i & 1) ? b : a, len, this->L[i]);
+            this->Ls[i * kLStride] = fmaf((i & 1) ? b : a, len, this->Ls[i * kLStride]);
         }
         nseg++;
     }
@@ -1007,10 +1047,11 @@ __device__ __forceinline__ void forward_tile(const ForwardArgs& a, const float4*
         for (int i = 0; i < M; i++) L[i] = acc.L[i];
         nseg = acc.nseg;
     } else {
-        AccumU16<M> acc(a.vol_u16);
+        float* s_L = reinterpret_cast<float*>(s_iv + blockDim.y * kIvSlots) + threadIdx.y * 32 + lane;
+        AccumU16<M> acc(a.vol_u16, s_L);
         ray_integrals<AccumU16<M>, M>(P, R, valid, Klo, Khi, wbuf, acc);
 #pragma unroll
-        for (int i = 0; i < M; i++) L[i] = acc.L[i];
+        for (int i = 0; i < M; i++) L[i] = acc.Lget(i);
         nseg = acc.nseg;
     }
     if (COUNT) {
@@ -1049,9 +1090,16 @@ __device__ __forceinline__ IvRec* iv_buffer(float4* smem, int NEmax)
 // latency of its L2 gathers, so occupancy pays more than registers: 5 blocks
 // (48 registers, 40 warps per SM) measured 26 % faster on B200 than the
 // compiler's own choice (80 registers, 24 warps), although the rarely taken
-// paths then spill.
+// paths then spill; with the uint16 path's long-term sums L in shared memory
+// (six registers freed), 6 blocks (40 registers, 48 warps) run the
+// 512x512x200 / 360-view projection in 45.7 ms against 48.6 ms at 5 (7
+// blocks: 50.5 ms).
 #ifndef VCBCT_FWD_MIN_BLOCKS
-#define VCBCT_FWD_MIN_BLOCKS 5
+#define VCBCT_FWD_MIN_BLOCKS 6
+#endif
+// the FP32-volume path keeps its sums in registers: 5 blocks (48 registers)
+#ifndef VCBCT_FWD_MIN_BLOCKS_F32
+#define VCBCT_FWD_MIN_BLOCKS_F32 5
 #endif
 #if VCBCT_FWD_MIN_BLOCKS > 0
 #define VCBCT_FWD_BOUNDS __launch_bounds__(256, VCBCT_FWD_MIN_BLOCKS)
@@ -1059,7 +1107,8 @@ __device__ __forceinline__ IvRec* iv_buffer(float4* smem, int NEmax)
 #define VCBCT_FWD_BOUNDS __launch_bounds__(256)
 #endif
 template <int M, bool F32VOL, bool COUNT>
-__global__ void VCBCT_FWD_BOUNDS forward_kernel(ForwardArgs a)
+__global__ void __launch_bounds__(256, F32VOL ? VCBCT_FWD_MIN_BLOCKS_F32 : VCBCT_FWD_MIN_BLOCKS)
+    forward_kernel(ForwardArgs a)
 {
     extern __shared__ float4 smem[];
     float4* s_mu = smem;
@@ -1414,7 +1463,7 @@ static cudaError_t launch_fwd_t(const ForwardArgs& a, cudaStream_t st)
     dim3 block(32, cpb);
     dim3 grid((a.p.W + cpb - 1) / cpb, a.p.V, a.nbands > 0 ? a.nbands : (a.p.H + 31) / 32);
     size_t shm = ((size_t)2 * a.spec.NE + (a.spec.NE + 3) / 4) * sizeof(float4) +
-                 (size_t)cpb * kIvSlots * sizeof(IvRec);
+                 (size_t)cpb * kIvSlots * sizeof(IvRec) + (size_t)M * kLStride * sizeof(float);
     auto k = forward_kernel<M, F32VOL, COUNT>;
     if (shm > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
@@ -1430,7 +1479,7 @@ cudaError_t launch_persistent_batch(const FlatBatch& b, int NEmax, int nmat_max,
     if (b.begin[b.nitems] <= 0) return cudaSuccess;
     dim3 block(32, cols_per_block);
     size_t shm = ((size_t)2 * NEmax + (NEmax + 3) / 4) * sizeof(float4) +
-                 (size_t)cols_per_block * kIvSlots * sizeof(IvRec);
+                 (size_t)cols_per_block * kIvSlots * sizeof(IvRec) + (size_t)8 * kLStride * sizeof(float);
     // (the shared-memory attribute is set by batch_blocks_per_sm, before any
     // stream capture)
     cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st);
@@ -1447,7 +1496,7 @@ cudaError_t launch_flat_batch(const FlatBatch& b, int NEmax, int nmat_max, int c
     if (total > 0x7fffffffLL) return cudaErrorInvalidValue;
     dim3 block(32, cols_per_block);
     size_t shm = ((size_t)2 * NEmax + (NEmax + 3) / 4) * sizeof(float4) +
-                 (size_t)cols_per_block * kIvSlots * sizeof(IvRec);
+                 (size_t)cols_per_block * kIvSlots * sizeof(IvRec) + (size_t)8 * kLStride * sizeof(float);
     auto k = (nmat_max <= 6) ? flat_batch_kernel<6> : flat_batch_kernel<8>;
     // (the shared-memory attribute is set by batch_blocks_per_sm, before any
     // stream capture)
@@ -1458,7 +1507,7 @@ cudaError_t launch_flat_batch(const FlatBatch& b, int NEmax, int nmat_max, int c
 int batch_blocks_per_sm(int nmat_max, int cols_per_block, int NEmax)
 {
     size_t shm = ((size_t)2 * NEmax + (NEmax + 3) / 4) * sizeof(float4) +
-                 (size_t)cols_per_block * kIvSlots * sizeof(IvRec);
+                 (size_t)cols_per_block * kIvSlots * sizeof(IvRec) + (size_t)8 * kLStride * sizeof(float);
     int n = 0;
     auto k = (nmat_max <= 6) ? persistent_batch_kernel<6> : persistent_batch_kernel<8>;
     if (shm > 48 * 1024 && cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm) != cudaSuccess)
