@@ -47,8 +47,8 @@ METRIC = "MBFPA ray-voxel Gseg/s & FDK GUPS; batched vs plain; grad-step/fwd rat
 # DRAM traffic of one forward launch of this workload: ncu
 # dram__bytes_read.sum + dram__bytes_write.sum of the first launch of
 # `python -m measure.profile_cases forward_c2 1` (a one-pass capture
-# of the full-size launch): 3.25 GB read + 1.70 GB written.
-FORWARD_DRAM_BYTES = 4.95e9
+# of the full-size launch): 3.35 GB read + 2.34 GB written.
+FORWARD_DRAM_BYTES = 5.69e9
 
 
 def workload():

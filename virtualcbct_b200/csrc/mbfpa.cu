@@ -32,6 +32,7 @@
 
 #include <cfloat>
 #include <climits>
+#include <type_traits>
 
 namespace vcbct {
 
@@ -560,11 +561,16 @@ struct AccumU16 : PairSumsS<M> {
     }
 };
 
-template <int M>
-struct AccumF32 : PairSums<M> {
+template <int M, bool SL = false>
+struct AccumF32 : std::conditional_t<SL, PairSumsS<M>, PairSums<M>> {
+    using Base = std::conditional_t<SL, PairSumsS<M>, PairSums<M>>;
     const float4* __restrict__ vol;
     unsigned nseg;
-    __device__ __forceinline__ AccumF32(const float4* v) : vol(v), nseg(0u) { this->clear(); }
+    __device__ __forceinline__ AccumF32(const float4* v, float* ls = nullptr) : vol(v), nseg(0u)
+    {
+        if constexpr (SL) this->Ls = ls;
+        this->clear();
+    }
     __device__ __forceinline__ void lanes(bool p, int idx, float len)
     {
         if (p) (*this)(idx, len);
@@ -577,7 +583,7 @@ struct AccumF32 : PairSums<M> {
         this->P2[0] = ffma2(a.x, l2, this->P2[0]);
         this->P2[1] = ffma2(a.y, l2, this->P2[1]);
         this->P2[2] = ffma2(b.x, l2, this->P2[2]);
-        if (M > 6) this->P2[3 % PairSums<M>::NP] = ffma2(b.y, l2, this->P2[3 % PairSums<M>::NP]);
+        if (M > 6) this->P2[3 % Base::NP] = ffma2(b.y, l2, this->P2[3 % Base::NP]);
         nseg++;
     }
     // a segment of absolute length len (cm), straight into L
@@ -585,7 +591,10 @@ struct AccumF32 : PairSums<M> {
     {
         const float* p = reinterpret_cast<const float*>(vol + 2 * (size_t)idx);
 #pragma unroll
-        for (int i = 0; i < M; i++) this->L[i] = fmaf(__ldg(p + i), len, this->L[i]);
+        for (int i = 0; i < M; i++) {
+            if constexpr (SL) this->Ls[i * kLStride] = fmaf(__ldg(p + i), len, this->Ls[i * kLStride]);
+            else this->L[i] = fmaf(__ldg(p + i), len, this->L[i]);
+        }
         nseg++;
     }
 };
@@ -1040,14 +1049,14 @@ __device__ __forceinline__ void forward_tile(const ForwardArgs& a, const float4*
 
     float L[M];
     unsigned nseg = 0;
+    float* s_L = reinterpret_cast<float*>(s_iv + blockDim.y * kIvSlots) + threadIdx.y * 32 + lane;
     if (F32VOL) {
-        AccumF32<M> acc(a.vol_f32);
-        ray_integrals<AccumF32<M>, M>(P, R, valid, Klo, Khi, wbuf, acc);
+        AccumF32<M, true> acc(a.vol_f32, s_L);
+        ray_integrals<AccumF32<M, true>, M>(P, R, valid, Klo, Khi, wbuf, acc);
 #pragma unroll
-        for (int i = 0; i < M; i++) L[i] = acc.L[i];
+        for (int i = 0; i < M; i++) L[i] = acc.Lget(i);
         nseg = acc.nseg;
     } else {
-        float* s_L = reinterpret_cast<float*>(s_iv + blockDim.y * kIvSlots) + threadIdx.y * 32 + lane;
         AccumU16<M> acc(a.vol_u16, s_L);
         ray_integrals<AccumU16<M>, M>(P, R, valid, Klo, Khi, wbuf, acc);
 #pragma unroll
@@ -1090,16 +1099,12 @@ __device__ __forceinline__ IvRec* iv_buffer(float4* smem, int NEmax)
 // latency of its L2 gathers, so occupancy pays more than registers: 5 blocks
 // (48 registers, 40 warps per SM) measured 26 % faster on B200 than the
 // compiler's own choice (80 registers, 24 warps), although the rarely taken
-// paths then spill; with the uint16 path's long-term sums L in shared memory
-// (six registers freed), 6 blocks (40 registers, 48 warps) run the
-// 512x512x200 / 360-view projection in 45.7 ms against 48.6 ms at 5 (7
-// blocks: 50.5 ms).
+// paths then spill; with the long-term sums L in shared memory (six
+// registers freed), 6 blocks (40 registers, 48 warps) run the 512x512x200 /
+// 360-view projection in 45.7 ms against 48.6 ms at 5 (7 blocks: 50.5 ms),
+// and its FP32-volume form in 45.0 ms against 48.1 ms.
 #ifndef VCBCT_FWD_MIN_BLOCKS
 #define VCBCT_FWD_MIN_BLOCKS 6
-#endif
-// the FP32-volume path keeps its sums in registers: 5 blocks (48 registers)
-#ifndef VCBCT_FWD_MIN_BLOCKS_F32
-#define VCBCT_FWD_MIN_BLOCKS_F32 5
 #endif
 #if VCBCT_FWD_MIN_BLOCKS > 0
 #define VCBCT_FWD_BOUNDS __launch_bounds__(256, VCBCT_FWD_MIN_BLOCKS)
@@ -1107,7 +1112,7 @@ __device__ __forceinline__ IvRec* iv_buffer(float4* smem, int NEmax)
 #define VCBCT_FWD_BOUNDS __launch_bounds__(256)
 #endif
 template <int M, bool F32VOL, bool COUNT>
-__global__ void __launch_bounds__(256, F32VOL ? VCBCT_FWD_MIN_BLOCKS_F32 : VCBCT_FWD_MIN_BLOCKS)
+__global__ void __launch_bounds__(256, VCBCT_FWD_MIN_BLOCKS)
     forward_kernel(ForwardArgs a)
 {
     extern __shared__ float4 smem[];
