@@ -423,7 +423,8 @@ void vcbct_fdk_default_geometry(vcbct_fdk_geometry* g);
  * (proj_width % 4 == 0 and 16-byte-aligned buffers; always so for the host
  * path, which uses the object's own device buffers); otherwise it splits in
  * a separate pass into a larger workspace.  The results agree within the
- * filter's 1e-5 tolerance either way. */
+ * filter's 1e-5 tolerance either way.  Detectors narrower than 16 or wider
+ * than 4096 columns are filtered by the direct path. */
 enum {
     VCBCT_FILTER_DIRECT_F32 = 0, /* FP32 direct Toeplitz product (parity path) */
     VCBCT_FILTER_BF16X3 = 1      /* tcgen05 BF16 3-term split GEMM, FP32 accumulate */

@@ -66,7 +66,9 @@ void IR_ImageCBCT(const int ite, int reconSize, int reconSlices, double reconSca
  * table), so the reference's delete2DArray frees it. */
 double** prepareConstMap(int projWidth, double DETECTOR_PITCH_CM_AT_ISO_CENT);
 
-/* Release_recon_from_forward_pro_float_CM/filterSinogram.h:4-6 */
+/* Release_recon_from_forward_pro_float_CM/filterSinogram.h:4-6; filters with
+ * the tensor-core BF16x3 GEMM (VCBCT_FILTER=direct: the FP32 direct
+ * filter), both within 1e-5 of the FP64 filter's output scale. */
 void filterSinogram(int projHeight, int projWidth, int sngrmHeight, float*** projVolume,
                     float*** fltdVoxData, double** constMap, double* xshift, double* yshift,
                     double DETECTOR_PITCH_CM_AT_ISO_CENT);

@@ -1656,6 +1656,9 @@ extern "C" int vcbct_fdk_filter(vcbct_fdk* f, const float* proj, float* filtered
     }
     const float pitch = (float)(g.det_pitch_iso_cm * g.max_pic_num / g.proj_width);
     const float* w = f->have_wts ? f->wts.as<float>() : nullptr;
+    // the tensor-core tiles take 16 to 4096 detector columns; outside that
+    // the direct filter runs (the same result within the 1e-5 tolerance)
+    if (method == VCBCT_FILTER_BF16X3 && (g.proj_width < 16 || g.proj_width > 4096)) method = VCBCT_FILTER_DIRECT_F32;
     if (method == VCBCT_FILTER_DIRECT_F32) {
         VCBCT_CUDA_TRY(launch_filter_direct(din, dout, f->hT.as<float>(), f->fviews.as<FilterView>(), w,
                                             pitch, (float)g.sad_cm, g.n_views, g.proj_height,
@@ -1778,7 +1781,12 @@ extern "C" void vcbct_filterSinogram(int projHeight, int projWidth, int sngrmHei
     if (!rc) {
         f->g.n_views = sngrmHeight;
         f->fp.V = sngrmHeight;
-        rc = vcbct_fdk_filter(f, &projVolume[0][0][0], &fltdVoxData[0][0][0], 0, VCBCT_FILTER_DIRECT_F32, nullptr);
+        // the tensor-core filter unless VCBCT_FILTER=direct asks for the FP32
+        // direct one (both within 1e-5 of the FP64 filter's scale)
+        const char* fm = std::getenv("VCBCT_FILTER");
+        const int method =
+            (fm && std::strcmp(fm, "direct") == 0) ? VCBCT_FILTER_DIRECT_F32 : VCBCT_FILTER_BF16X3;
+        rc = vcbct_fdk_filter(f, &projVolume[0][0][0], &fltdVoxData[0][0][0], 0, method, nullptr);
     }
     if (rc) std::fprintf(stderr, "filterSinogram: %s\n", vcbct_last_error());
     vcbct_fdk_destroy(f);

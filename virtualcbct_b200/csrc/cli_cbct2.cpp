@@ -3,9 +3,10 @@
 // info file and flexmap, the float projections "<prefix>.<ext>"
 // [V][H][W], filters them (writing "fltsngrm.raw" as the reference does),
 // backprojects and writes the (short) volume [Z][N][N] to the
-// reconstruction file.  VCBCT_FILTER=bf16x3 selects the tensor-core filter;
-// the default is the FP32 direct filter of the reference's arithmetic.  Exit
-// status 0 on success, 1 on any error.
+// reconstruction file.  The filter is the tensor-core BF16x3 one (within
+// 1e-5 of the FP64 filter's scale, as the FP32 direct one is);
+// VCBCT_FILTER=direct selects the FP32 direct filter.  Exit status 0 on
+// success, 1 on any error.
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -74,7 +75,7 @@ int main(int argc, char** argv)
     vcbct_fdk* f = nullptr;
     if (vcbct_fdk_create(&g, d.angles_rad, d.xshift, d.yshift, &f)) return die("fdk");
     const char* fm = std::getenv("VCBCT_FILTER");
-    const int method = (fm && std::strcmp(fm, "bf16x3") == 0) ? VCBCT_FILTER_BF16X3 : VCBCT_FILTER_DIRECT_F32;
+    const int method = (fm && std::strcmp(fm, "direct") == 0) ? VCBCT_FILTER_DIRECT_F32 : VCBCT_FILTER_BF16X3;
     if (vcbct_fdk_filter(f, proj.data(), filt.data(), 0, method, nullptr)) {
         vcbct_fdk_destroy(f);
         return die("filterSinogram");
