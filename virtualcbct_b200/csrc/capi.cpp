@@ -690,7 +690,8 @@ static int projector_adjoint(vcbct_projector* p, const float* d_L, const float* 
     if (p->NE <= 0) return fail(VCBCT_ERR_STATE, "no spectrum set");
     cudaStream_t st = (cudaStream_t)stream;
     const auto& g = p->g;
-    // gradient planes of element pairs (ceil(nmat / 2) x 2 floats per voxel)
+    // gradient planes (ceil(nmat / 2) x 2 floats per voxel: element quads, then a
+    // pair for a last group of one or two elements)
     const size_t pk = (size_t)((g.num_material + 1) / 2) * 2 * g.recon_size * g.recon_size * g.recon_slices *
                       sizeof(float);
     VCBCT_CUDA_TRY(p->grad_pk.ensure(pk));

@@ -104,7 +104,8 @@ struct AdjointArgs {
     const float* grad_out;   // [V][H][W] d loss / d intensity
     const float* L_in;       // [V][H][W][nmat] path integrals of the forward, or
                              // nullptr: recompute them (first march)
-    float* grad_planes;      // [ceil(nmat/2)][N*N*Z][2] float accumulator, element pairs, z fastest
+    float* grad_planes;      // float accumulator, z fastest, ceil(nmat/2) x 2 floats per voxel: groups of
+                             // four elements [N*N*Z][4], the last a pair [N*N*Z][2] if it holds one or two
     int* err_flag;
     int cols_per_block;
     int y0, y1;              // scatter only into volume rows iy in [y0, y1) (y1 <= y0: all)

@@ -606,7 +606,8 @@ struct AccumF32 : std::conditional_t<SL, PairSumsS<M>, PairSums<M>> {
 // reduction per element and lane; the L2 applies them per sector).
 template <int M>
 struct Scatter {
-    float* __restrict__ grad;   // [ceil(nmat/2)][N*N*Z][2]: element pairs (2q, 2q+1) interleaved
+    float* __restrict__ grad;   // element groups: quads [N*N*Z][4] (elements 4q .. 4q+3), the last
+                                // group a pair [N*N*Z][2] when it holds one or two elements
     size_t plane;               // N*N*Z
     int nmat;
     float g[8];                 // zero beyond nmat
@@ -617,14 +618,20 @@ struct Scatter {
     __device__ __forceinline__ void first(int idx, float len)
     {
         if ((unsigned)idx - lo >= span) return;
-        // one 8-byte vector reduction per element pair: half the reduction
-        // instructions of per-element planes, and a warp's 32 lanes (about 11
-        // consecutive z cells) touch 3-4 sectors per pair plane
+        // one 16-byte vector reduction per group of four elements (8 bytes
+        // for a last group of one or two): a third fewer reduction requests
+        // than per element pair for six elements, the same sectors
 #pragma unroll
-        for (int q = 0; q < M / 2; q++)
-            if (2 * q < nmat)
-                atomicAdd(reinterpret_cast<float2*>(grad) + (size_t)q * plane + idx,
-                          make_float2(g[2 * q] * len, g[2 * q + 1] * len));
+        for (int q = 0; q < (M + 3) / 4; q++) {
+            const int e0 = 4 * q;
+            if (e0 >= nmat) break;
+            float* base = grad + (size_t)e0 * plane;  // earlier groups are full quads
+            if (nmat - e0 > 2)
+                atomicAdd(reinterpret_cast<float4*>(base) + idx,
+                          make_float4(g[e0] * len, g[e0 + 1] * len, g[(e0 + 2) % 8] * len, g[(e0 + 3) % 8] * len));
+            else
+                atomicAdd(reinterpret_cast<float2*>(base) + idx, make_float2(g[e0] * len, g[e0 + 1] * len));
+        }
     }
     __device__ __forceinline__ void lanes(bool p, int idx, float len)
     {
@@ -1416,11 +1423,13 @@ __global__ void unpack_grad_kernel(const float* __restrict__ src, int N, int Z, 
     const int m = blockIdx.z / zt;
     const int x0 = blockIdx.x * 32, y = blockIdx.y, z0 = (blockIdx.z % zt) * 32;
     const size_t NN = (size_t)N * N;
-    // element m is slot m % 2 of pair plane m / 2 (see Scatter)
-    const float* plane = src + (size_t)(m / 2) * NN * Z * 2 + (m % 2);
+    // element m is slot m % 4 of the group starting at element 4 (m / 4),
+    // four wide, or two for a last group of one or two elements (see Scatter)
+    const int e0 = (m / 4) * 4, wdt = nmat - e0 > 2 ? 4 : 2;
+    const float* plane = src + (size_t)e0 * NN * Z + (m % 4);
     for (int xx = threadIdx.y; xx < 32; xx += 8) {
         const int x = x0 + xx, z = z0 + threadIdx.x;
-        tile[threadIdx.x][xx] = (x < N && z < Z) ? plane[(((size_t)y * N + x) * Z + z) * 2] : 0.0f;
+        tile[threadIdx.x][xx] = (x < N && z < Z) ? plane[(((size_t)y * N + x) * Z + z) * wdt] : 0.0f;
     }
     __syncthreads();
     for (int zz = threadIdx.y; zz < 32; zz += 8) {
