@@ -177,6 +177,8 @@ constexpr uint32_t kHalfCol = 256;              // TMEM column of the second col
 constexpr int kAStages = 2;                     // A ring: the three planes of one K tile each
 constexpr uint32_t kAPlaneBytes = BM * BK * 2;  // one 128 x 64 bf16 plane, 16 KiB
 constexpr uint32_t kAStageBytes = 3 * kAPlaneBytes;
+// the fused epilogue stages 8 warps x 2 x 2 KB per column half in one A stage
+static_assert(kAStages == 2 && 8 * 4096 <= kAStageBytes, "epilogue staging in the A ring");
 constexpr uint32_t kPTileBytes = BM * BK * 4;   // fused form: one 128 x 64 FP32 tile of p, 32 KiB
 
 // B ring stages (one column half of one plane of one K tile each): the fused
@@ -189,7 +191,7 @@ __host__ __device__ constexpr int b_stages(bool fused) { return fused ? 3 : 4; }
 __host__ __device__ constexpr size_t gemm_smem_bytes(int NT, bool fused)
 {
     return (fused ? (size_t)kPTileBytes : 0) + (size_t)kAStages * kAStageBytes +
-           (size_t)b_stages(fused) * (NT / 2) * BK * 2 + 8 * (2 + 2 * kAStages + 2 * b_stages(fused) + 1) + 16;
+           (size_t)b_stages(fused) * (NT / 2) * BK * 2 + 8 * (2 + 2 * kAStages + 2 * b_stages(fused) + 2) + 16;
 }
 
 // Shared -> global tensor store of one box (clipped at the tensor's edges),
@@ -302,8 +304,9 @@ ramp_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant_
     uint64_t* a_empty = bars + 2 + kAStages;
     uint64_t* b_full = bars + 2 + 2 * kAStages;
     uint64_t* b_empty = bars + 2 + 2 * kAStages + SB;
-    uint64_t* accum = bars + 2 + 2 * kAStages + 2 * SB;
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(accum + 1);
+    uint64_t* accum = bars + 2 + 2 * kAStages + 2 * SB;  // every MMA of the tile done
+    uint64_t* accum0 = accum + 1;                        // those of column half 0 done
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(accum0 + 1);
 
     const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
     const int m0 = blockIdx.x * BM;
@@ -321,6 +324,7 @@ ramp_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant_
             mbar_init(&b_empty[s], 1);
         }
         mbar_init(accum, 1);
+        mbar_init(accum0, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     }
@@ -335,9 +339,9 @@ ramp_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant_
 
     if (warp == 0 && lane == 0) {
         // TMA producer.  Per K tile: the A operand (fused form: the FP32 tile
-        // of p; otherwise the three split A planes, one A stage), then the B
-        // planes 2, 1, 0, each as two column halves (six B stages) -- the
-        // order the consumers take them in.  Fused form: p tile n + 1 is
+        // of p; otherwise the three split A planes, one A stage), then column
+        // half 0 of B planes 2, 1, 0 and half 1 of the same (six B stages) --
+        // the order the consumers take them in.  Fused form: p tile n + 1 is
         // requested as soon as the converters have released tile n, polled
         // while the thread waits for B ring stages.
         int na = 0, nb = 0;  // stages (fused form: p tiles) issued
@@ -374,7 +378,7 @@ ramp_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant_
                     if (!ok) break;
                 }
                 if (FUSED && na < g.ktiles && mbar_try_wait(p_empty, (na - 1) & 1)) issue_p();
-                const int plane = 2 - q / 2, h = q % 2;
+                const int plane = 2 - q % 3, h = q / 3;
                 mbar_expect_tx(&b_full[s], bh_bytes);
                 tma_load_3d(bbuf + (size_t)s * bh_bytes, &tmB, &b_full[s], kt * BK, n0 + h * NH, plane);
                 nb = kb + 1;
@@ -396,11 +400,13 @@ ramp_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant_
         for (int k = nb - SB; k < nb; k++)
             if (k >= 0) mbar_wait(&b_full[k % SB], (k / SB) & 1, g.err);
     } else if (warp == 1 && lane == 0) {
-        // MMA issuer: per K tile and B plane j, each column half against A
-        // planes 2 - j .. 0, so the products (2,0) (1,1) (0,2) (1,0) (0,1)
-        // (0,0) are all formed, smaller terms of a tile before larger ones.
+        // MMA issuer: per K tile, column half 0 then 1, and per half B plane
+        // j against A planes 2 - j .. 0, so the products (2,0) (1,1) (0,2)
+        // (1,0) (0,1) (0,0) are all formed, smaller terms of a tile before
+        // larger ones.  Half 0 of the last K tile is committed on its own, so
+        // its epilogue starts while half 1's last MMAs run.
         const uint32_t idesc = idesc_bf16(BM, NH);
-        bool ok = true, fresh[2] = {true, true};
+        bool ok = true, fresh[2] = {true, true}, half0 = false;
         for (int kt = 0; kt < g.ktiles && ok; kt++) {
             const int sa = kt % kAStages;
             if (!(ok = mbar_wait(&a_full[sa], (kt / kAStages) & 1, g.err))) break;
@@ -409,7 +415,7 @@ ramp_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant_
                 const int kb = kt * 6 + q, s = kb % SB;
                 if (!(ok = mbar_wait(&b_full[s], (kb / SB) & 1, g.err))) break;
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                const int j = 2 - q / 2, h = q % 2;
+                const int j = 2 - q % 3, h = q / 3;
                 const uint32_t sb = smem_u32(bbuf + (size_t)s * bh_bytes);
                 const uint32_t dcol = taddr + (uint32_t)h * kHalfCol;
                 for (int i = 2 - j; i >= 0; i--) {
@@ -421,9 +427,14 @@ ramp_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant_
                     }
                 }
                 umma_commit(&b_empty[s]);
+                if (q == 2 && kt == g.ktiles - 1) {
+                    umma_commit(accum0);
+                    half0 = true;
+                }
             }
             umma_commit(&a_empty[sa]);
         }
+        if (!half0) umma_commit(accum0);  // (an error path: the waiters see the flag)
         umma_commit(accum);
     } else if (warp >= 2) {
         bool ok = true;
@@ -478,7 +489,7 @@ ramp_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant_
         const int grp = (warp - 2) / 4;
         const int half = grp >> 1, part = grp & 1;
         const int row = m0 + 32 * q + lane;
-        if (ok && warp_wait(accum, 0, g.err)) {
+        if (ok && warp_wait(half ? accum : accum0, 0, g.err)) {
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             float pos2 = 0.0f, xcs = 0.0f;
             if (row < g.M) {
@@ -492,17 +503,23 @@ ramp_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant_
             const float sad = g.sad, base2 = fmaf(pos2, pos2, sad * sad);
             if (FUSED) {
                 // Warp (q, half, part) drains TMEM lane quarter q of column
-                // half `half` (the logical columns half NH .. half NH + NH - 1),
-                // the 16-column chunks part, part + 2, ..., the next chunk's
-                // load in flight while this one is scaled and stored.  Each 32-row x 16-column chunk goes
-                // through a 2 KB staging buffer (two per warp, in the A ring,
-                // free once the last MMA has completed) in the layout of a
+                // half `half` (the logical columns half NH .. half NH + NH -
+                // 1), the 16-column chunks part, part + 2, ..., the next
+                // chunk's load in flight while this one is scaled and stored.
+                // Each 32-row x 16-column chunk goes through a 2 KB staging
+                // buffer (two per warp, in the A ring) in the layout of a
                 // CU_TENSOR_MAP_SWIZZLE_64B box (row r at 64 r bytes, 16-byte
                 // chunk j at j ^ ((r >> 1) & 3): conflict-free vector stores),
                 // and one TMA store writes it whole: full sectors, rows and
                 // columns past the detector clipped, instead of 32 rows
                 // touched by every warp store.
-                uint8_t* stage = abuf + (size_t)(warp - 2) * 4096;
+                // half 0 drains while half 1's last MMAs still read the A
+                // stage of the last K tile: its warps stage in the other A
+                // stage (its K tile's MMAs have completed), half 1's in that
+                // last stage once every MMA is done; 8 warps x 4 KB each
+                const int last_sa = (g.ktiles - 1) % kAStages;
+                const int ssel = half ? last_sa : kAStages - 1 - last_sa;
+                uint8_t* stage = abuf + (size_t)ssel * kAStageBytes + (size_t)((warp - 2) % 8) * 4096;
                 const int r0 = m0 + 32 * q;
                 const uint32_t tq = taddr + ((uint32_t)(32 * q) << 16) + (uint32_t)half * kHalfCol;
                 const int nch = NH / 16;
