@@ -363,25 +363,40 @@ __global__ void __launch_bounds__(256, MINB) backproject_kernel(
                 continue;
             }
             if (!lastc && full) {
-                // columns UU, UU + 1 of rows NZ, NZ1: one address per row and
-                // the second column at +4 bytes; all slices of the block exist
+                // some slices of the block project outside rows 0 .. H - 2:
+                // the same packed pairs, a slice off the detector (NZ outside
+                // 0 .. H - 1) adding an exact zero (its rows clamped, its
+                // weight 0; the sums are never -0, so acc + 0 = acc), the last
+                // row taking row weights (1, 0) as the scalar rule does
                 const float* pc = pv + UU;
+                const f32x2 dz2 = f2pack(dz, dz), zf2b = f2pack(Zf, Zf);
+                const f32x2 cw0_2 = f2pack(cw0, cw0), cw1_2 = f2pack(cw1, cw1);
+                const f32x2 big2 = f2pack(12582912.0f, 12582912.0f), one2 = f2pack(1.0f, 1.0f);
 #pragma unroll
-                for (int i = 0; i < ZB; i++) {
-                    const float zfrac = fmaf((float)i, dz, Zf);
-                    const float tq = __fadd_rd(zfrac, 12582912.0f);
-                    const float fl = tq - 12582912.0f;
-                    const int NZ = Zi + (__float_as_int(tq) - 0x4B400000);
-                    const float wz = zfrac - fl;
-                    if ((unsigned)NZ > (unsigned)(H - 1)) continue;
-                    const bool lastr = (NZ == H - 1);
-                    const float rw0 = lastr ? 1.0f : 1.0f - wz;
-                    const float rw1 = lastr ? 0.0f : wz;
-                    const float* r0p = pc + NZ * W;
-                    const float* r1p = lastr ? r0p : r0p + W;
-                    const float s0 = fmaf(cw1, __ldg(r0p + 1), cw0 * __ldg(r0p));
-                    const float s1 = fmaf(cw1, __ldg(r1p + 1), cw0 * __ldg(r1p));
-                    acc[i] = fmaf(fmaf(rw1, s1, rw0 * s0), w2, acc[i]);
+                for (int i = 0; i < ZB; i += 2) {
+                    const f32x2 zfrac = ffma2(f2pack((float)i, (float)(i + 1)), dz2, zf2b);
+                    const f32x2 tq = fadd2_rd(zfrac, big2);
+                    float wza, wzb, tqa, tqb;
+                    f2unpack(fsub2(zfrac, fsub2(tq, big2)), wza, wzb);
+                    f2unpack(tq, tqa, tqb);
+                    const int NZa = Zi + (__float_as_int(tqa) - 0x4B400000);
+                    const int NZb = Zi + (__float_as_int(tqb) - 0x4B400000);
+                    const bool ina = (unsigned)NZa <= (unsigned)(H - 1), inb = (unsigned)NZb <= (unsigned)(H - 1);
+                    const bool la = NZa == H - 1, lb = NZb == H - 1;
+                    const int ra = min(max(NZa, 0), H - 1), rb = min(max(NZb, 0), H - 1);
+                    const float* r0a = pc + ra * W;
+                    const float* r0b = pc + rb * W;
+                    const float* r1a = la || !ina ? r0a : r0a + W;
+                    const float* r1b = lb || !inb ? r0b : r0b + W;
+                    const f32x2 wz = f2pack(la ? 0.0f : wza, lb ? 0.0f : wzb);
+                    const f32x2 s0 = ffma2(cw1_2, f2pack(__ldg(r0a + 1), __ldg(r0b + 1)),
+                                           fmul2(cw0_2, f2pack(__ldg(r0a), __ldg(r0b))));
+                    const f32x2 s1 = ffma2(cw1_2, f2pack(__ldg(r1a + 1), __ldg(r1b + 1)),
+                                           fmul2(cw0_2, f2pack(__ldg(r1a), __ldg(r1b))));
+                    const f32x2 v = ffma2(wz, s1, fmul2(fsub2(one2, wz), s0));
+                    f32x2 a2 = f2pack(acc[i], acc[i + 1]);
+                    a2 = ffma2(v, f2pack(ina ? w2 : 0.0f, inb ? w2 : 0.0f), a2);
+                    f2unpack(a2, acc[i], acc[i + 1]);
                 }
                 continue;
             }
