@@ -161,3 +161,27 @@ def test_bf16x3_fused_and_split_a_operand_agree(cuda, redundancy):
     assert np.abs(fused - d64).max() <= 1e-5 * scale
     assert np.abs(split - d64).max() <= 1e-5 * scale
     assert np.abs(fused - split).max() <= 1e-5 * scale
+
+
+def test_bf16x3_unaligned_output_and_short_views(cuda):
+    """An output 4 bytes off alignment takes the unfused form (the fused one
+    stores through TMA); views of fewer than 8 rows take the per-row weight
+    loads of the fused converter.  Both against the FP64 filter of
+    w * (-log p) at 1e-5 of the scale."""
+    import torch
+    g, proj, ang, xs = _case(V=5, H=5, W=64, seed=21, xshift=3.0)
+    g = g.with_(redundancy=1)
+    w = redundancy_weights(g, xs)
+    f = Fdk(g, ang, xs, np.zeros(g.V))
+    pw = (proj.astype(np.float64) ** w[:, None, :].astype(np.float64)).astype(np.float32)
+    d64 = O.filter_sinogram(pw, xs, np.zeros(g.V), O.fdk_consts(g.piso), mode=1)
+    scale = np.abs(d64).max()
+    p = torch.from_numpy(proj).cuda()
+    fused = f.filter(p, method=FILTER_BF16X3).cpu().numpy()
+    store = torch.empty(proj.size + 1, dtype=torch.float32, device="cuda")
+    out = store[1:].view(proj.shape)
+    assert out.data_ptr() % 16 == 4
+    f.filter(p, out, method=FILTER_BF16X3)
+    split = out.cpu().numpy()
+    assert np.abs(fused - d64).max() <= 1e-5 * scale
+    assert np.abs(split - d64).max() <= 1e-5 * scale
