@@ -16,11 +16,13 @@
 // as two column halves (a ring of 3 or 4 stages), so each B plane of a K tile
 // is loaded once and multiplied by every A plane it pairs with; warp 1 issues
 // tcgen05.mma from a single thread into two 128 x NT/2 FP32 accumulators in
-// tensor memory (columns 0 and 256); warps 2-9 read them back (tcgen05.ld),
-// apply the cosine factor and store.
+// tensor memory (columns 0 and 256); warps 2-17 read them back (tcgen05.ld),
+// apply the cosine factor and store.  Each K tile is multiplied column half 0
+// first, so after the last one the warps of half 0 start their epilogue while
+// half 1's MMAs still run.
 //
 // The A operand, fused form (rows of p 16-byte aligned): warp 0 stages the
-// 128 x 64 FP32 tile of p in shared memory and warps 2-9, idle until the
+// 128 x 64 FP32 tile of p in shared memory and warps 2-17, idle until the
 // epilogue, turn it into the three swizzled bf16 planes of -ln p in a
 // 2-stage ring -- p is read from HBM once and no split copy is written.
 // Unfused form (other widths): split_a_kernel first writes the three A planes
@@ -235,11 +237,11 @@ __device__ __forceinline__ float2 ld_shared_f2(uint32_t addr)
 // the 128-byte-swizzled K-major tile a TMA load with
 // CU_TENSOR_MAP_SWIZZLE_128B would write (row r at r * 128 bytes, the 16-byte
 // chunk index XOR r % 8; buffers 1024-byte aligned).  Producer warp w makes
-// rows 16 w .. 16 w + 15, lane l the columns kt * 64 + 2 l, + 1 of each: one
-// 8-byte shared load and one 4-byte store per plane, conflict-free.
-// Redundancy weights: with wfast (H >= 16) the warp's rows hold at most two
-// views, whose weights the caller has loaded (wa before CTA row rsplit, wb
-// from it on); otherwise each row loads its own.
+// rows R w .. R w + R - 1 (R = BM / kEpiWarps = 8), lane l the columns
+// kt * 64 + 2 l, + 1 of each: one 8-byte shared load and one 4-byte store per
+// plane, conflict-free.  Redundancy weights: with wfast (H >= R) the warp's
+// rows hold at most two views, whose weights the caller has loaded (wa before
+// CTA row rsplit, wb from it on); otherwise each row loads its own.
 __device__ __forceinline__ void convert_a_tile(const GemmArgs& g, int m0, int kt, int pw, int lane,
                                                uint32_t ptile, uint32_t abuf, bool wfast, int rsplit, float2 wa,
                                                float2 wb)
@@ -442,8 +444,8 @@ ramp_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant_
             // the A planes of every K tile from the staged p tile,
             // double-buffered against the MMAs
             const int pw = warp - 2;
-            // the warp's rows m0 + 16 pw .. + 15 lie in views va and (from CTA
-            // row rsplit on) va + 1 when H >= 16
+            // the warp's rows m0 + 8 pw .. + 7 lie in views va and (from CTA
+            // row rsplit on) va + 1 when H >= 8
             const int rw = m0 + pw * (BM / kEpiWarps);
             const bool wfast = g.wts != nullptr && g.H >= BM / kEpiWarps;
             const int va = rw / g.H;
