@@ -47,8 +47,8 @@ METRIC = "MBFPA ray-voxel Gseg/s & FDK GUPS; batched vs plain; grad-step/fwd rat
 # DRAM traffic of one forward launch of this workload: ncu
 # dram__bytes_read.sum + dram__bytes_write.sum of the first launch of
 # `python -m measure.profile_cases forward_c2 1` (a one-pass capture
-# of the full-size launch): 3.35 GB read + 2.34 GB written.
-FORWARD_DRAM_BYTES = 5.69e9
+# of the full-size launch): 17.40 GB read + 6.48 GB written.
+FORWARD_DRAM_BYTES = 23.88e9
 
 
 def workload():
@@ -879,7 +879,7 @@ def run_ours(args, rank, world, local_rank):
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": w["name"], "segments_per_step": nseg, "parallelism": f"replica{world}",
-                   "l2": "inputs larger than L2 (packed volume 839 MB)"},
+                   "l2": "inputs larger than L2 (packed volume 1.68 GB)"},
         "e2e": {"value": e2e, "unit": "Gseg/s", "ms_per_step": ms_e2e,
                 "h2d_bytes_per_step": int(vol_np.nbytes), "d2h_bytes_per_step": int(out_np.nbytes)},
         "gpu_launches": args.steps * 1,

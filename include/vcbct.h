@@ -89,12 +89,15 @@ int vcbct_projector_set_spectrum(vcbct_projector* p, const float* attenuation,
 /* Element volume uint16 [Z][nmat][N][N] (the matVolume of projectionData.cpp),
  * from host memory (on_device = 0) or device memory (on_device = 1).  The
  * values are kept unaltered; the device copy is re-laid out once into the
- * z-fastest packed form the projector reads. */
+ * z-fastest packed form the projector reads (the values as floats, which
+ * represent every uint16 exactly). */
 int vcbct_projector_load_volume(vcbct_projector* p, const uint16_t* volume, int on_device,
                                 void* stream);
 
 /* Same, from float element volumes [Z][nmat][N][N] (densities x1000, the
- * differentiable path; no reference counterpart). */
+ * differentiable path; no reference counterpart).  Both loaders give the same
+ * packed form: a float volume holding integer values projects bit for bit as
+ * the uint16 volume of those values. */
 int vcbct_projector_load_volume_f32(vcbct_projector* p, const float* volume, int on_device,
                                     void* stream);
 
@@ -146,9 +149,9 @@ int vcbct_projector_count_segments(vcbct_projector* p, unsigned long long* total
 
 /* Adjoint (no reference counterpart; nearest analogue lengthproj.cpp:10-131):
  * given d(loss)/d(out) as float [V][H][W] on the device, accumulate
- * d(loss)/d(volume) into d_grad float [Z][nmat][N][N] (+=).  Requires a float
- * volume (vcbct_projector_load_volume_f32).  Per-ray spectral state is
- * recomputed, not stored. */
+ * d(loss)/d(volume) into d_grad float [Z][nmat][N][N] (+=).  Requires a
+ * loaded volume (either loader).  Per-ray spectral state is recomputed, not
+ * stored. */
 int vcbct_projector_adjoint(vcbct_projector* p, const float* d_grad_out, float* d_grad,
                             void* stream);
 /* The same pair with the per-ray element path integrals L[V][H][W][nmat]
@@ -162,8 +165,8 @@ int vcbct_projector_adjoint_state(vcbct_projector* p, const float* d_L, const fl
                                   float* d_grad, void* stream);
 
 /* Batched projection (no reference counterpart; the reference projects one
- * phantom per process run).  Items are projector objects holding a uint16
- * volume and a spectrum, each with its own device output [V][H][W]; the items
+ * phantom per process run).  Items are projector objects holding a volume
+ * and a spectrum, each with its own device output [V][H][W]; the items
  * may differ in volume size, view count and detector.  vcbct_batch_forward
  * projects all of them either in one persistent launch that balances the
  * uneven work through a global tile counter (the default), as per-item

@@ -1,6 +1,7 @@
 """Adjoint of the polychromatic projection with respect to the six float
 element volumes: against the FP64 gradient of the oracle and against central
-finite differences of the FP64 forward (h = 1e-3 on 64 random voxels)."""
+finite differences of the FP64 forward (h = 1e-3 on 64 random voxels); the
+two volume loaders against each other."""
 import numpy as np
 import pytest
 
@@ -28,6 +29,32 @@ def test_float_volume_forward_matches_oracle(cuda):
     out = p.forward().cpu().numpy()
     ref = O.mbfpa_forward(g, tabs, None, mu, pdf, 1000.0, volf=volf, exact=False, want=("d",))["d"]
     assert np.max(np.abs(out - ref) / ref) <= 1e-5
+
+
+def test_uint16_and_float_loaders_give_the_same_volume(cuda):
+    """Both loaders write the same packed form (float records): a uint16
+    volume and the float volume of the same values project bit for bit
+    alike, and the adjoint runs on either, with the same gradient."""
+    import torch
+    g, tabs, vol, _ = proj_case("ellipsoid", seed=3)
+    mu, pdf = spectrum()
+    pu, pf = Projector(g, *tabs), Projector(g, *tabs)
+    for p in (pu, pf):
+        p.set_spectrum(mu, pdf, 1000.0)
+    pu.load_volume(vol)
+    pf.load_volume_f32(torch.from_numpy(vol.astype(np.float32)).to(cuda))
+    ou, of = pu.forward(), pf.forward()
+    assert torch.equal(ou, of)
+    ref = O.mbfpa_forward(g, tabs, vol, mu, pdf, 1000.0, exact=False, want=("d",))["d"]
+    assert np.max(np.abs(ou.cpu().numpy() - ref) / ref) <= 1e-5
+    resid = torch.from_numpy(np.random.default_rng(7).normal(size=(g.V, g.H, g.W)).astype(np.float32)).to(cuda)
+    gu = torch.zeros((g.Z, g.nmat, g.N, g.N), dtype=torch.float32, device=cuda)
+    gf = torch.zeros_like(gu)
+    pu.adjoint(resid, gu)
+    pf.adjoint(resid, gf)
+    assert gu.abs().max() > 0
+    # float atomics may reduce in another order: equal to FP32 rounding
+    assert torch.allclose(gu, gf, rtol=1e-5, atol=1e-6 * gu.abs().max().item())
 
 
 @pytest.mark.parametrize("seed,zreg,keep", [(0, 0.3, True), (4, 0.3, False), (2, 0.0, True), (2, 0.0, False)])

@@ -1,7 +1,7 @@
 """State errors of live objects: a projector used before it has a volume or
-a spectrum, the adjoint on a uint16 volume, a batch given a float-volume
-projector, an unknown filter method, an invalid view range -- each a status
-and a message, with the object still usable afterwards."""
+a spectrum, the adjoint before a volume, a batch given a projector without a
+volume, an unknown filter method, an invalid view range -- each a status and
+a message, with the object still usable afterwards."""
 import ctypes as C
 
 import numpy as np
@@ -29,6 +29,9 @@ def test_projector_state_errors(cuda):
     out = torch.empty((g.V, g.H, g.W), dtype=torch.float32, device=cuda)
     rc, msg = _rc(L.vcbct_projector_forward, p._h, C.c_void_p(out.data_ptr()), 1, None)
     assert rc == STATE and "volume" in msg
+    grad = torch.zeros((g.Z, g.nmat, g.N, g.N), dtype=torch.float32, device=cuda)
+    rc, msg = _rc(L.vcbct_projector_adjoint, p._h, C.c_void_p(out.data_ptr()), C.c_void_p(grad.data_ptr()), None)
+    assert rc == STATE and "volume" in msg
     p.load_volume(vol)
     rc, msg = _rc(L.vcbct_projector_forward, p._h, C.c_void_p(out.data_ptr()), 1, None)
     assert rc == STATE and "spectrum" in msg
@@ -38,9 +41,6 @@ def test_projector_state_errors(cuda):
                   big.ctypes.data_as(C.POINTER(C.c_float)), 2000, 1000.0)
     assert rc == LIMIT
     p.set_spectrum(mu, pdf, 1000.0)
-    grad = torch.zeros((g.Z, g.nmat, g.N, g.N), dtype=torch.float32, device=cuda)
-    rc, msg = _rc(L.vcbct_projector_adjoint, p._h, C.c_void_p(out.data_ptr()), C.c_void_p(grad.data_ptr()), None)
-    assert rc == STATE and "float volume" in msg
     rc, _ = _rc(L.vcbct_projector_set_noise, p._h, 3, 1e4, 6e4, 0)
     assert rc == ARG
     proj = np.zeros((g.V, g.H, g.W), np.uint16)
@@ -58,10 +58,9 @@ def test_batch_and_fdk_state_errors(cuda):
     mu, pdf = spectrum()
     p = Projector(g, *tabs)
     p.set_spectrum(mu, pdf, 1000.0)
-    p.load_volume_f32(torch.from_numpy(vol.astype(np.float32)).to(cuda))
     b = Batch()
     out = torch.empty((g.V, g.H, g.W), dtype=torch.float32, device=cuda)
-    with pytest.raises(N.VcbctError, match="uint16"):
+    with pytest.raises(N.VcbctError, match="volume"):
         b.add(p, out)
     fg = FdkGeometry(W=48, H=40, V=6, N=27, Z=8, zstart=-3, step=0.5, scale=0.4)
     ang = np.deg2rad(-180.0001 + np.arange(6) * 60.0)

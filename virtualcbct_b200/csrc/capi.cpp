@@ -79,8 +79,7 @@ struct vcbct_projector {
     vcbct_proj_geometry g;
     ProjParams pp;
     DevBuf views;      // ViewGeom[V]
-    DevBuf vol_u16;    // packed
-    DevBuf vol_f32;    // packed
+    DevBuf vol_f32;    // packed, f32 form (uint16 volumes converted exactly)
     DevBuf stage;      // staging for host inputs / outputs
     DevBuf spec_mu;    // float4 [NE][2]
     DevBuf spec_pdf;   // float [NE]
@@ -175,7 +174,6 @@ extern "C" int vcbct_projector_destroy(vcbct_projector* p)
     if (p->band_stream) cudaStreamSynchronize(p->band_stream);
     if (p->pack_stream) cudaStreamSynchronize(p->pack_stream);
     p->views.release();
-    p->vol_u16.release();
     p->vol_f32.release();
     p->stage.release();
     p->spec_mu.release();
@@ -237,8 +235,9 @@ extern "C" int vcbct_projector_load_volume(vcbct_projector* p, const uint16_t* v
         VCBCT_CUDA_TRY(cudaMemcpyAsync(p->stage.p, vol, vol_elems(g) * sizeof(uint16_t), cudaMemcpyHostToDevice, st));
         src = p->stage.as<uint16_t>();
     }
-    VCBCT_CUDA_TRY(p->vol_u16.ensure(packed_u16_bytes(g.recon_size, g.recon_slices)));
-    VCBCT_CUDA_TRY(launch_pack_u16(src, g.recon_size, g.recon_slices, g.num_material, p->vol_u16.as<uint4>(), st));
+    VCBCT_CUDA_TRY(p->vol_f32.ensure(packed_f32_bytes(g.recon_size, g.recon_slices)));
+    VCBCT_CUDA_TRY(launch_pack_u16_f32_slab(src, g.recon_size, g.recon_slices, 0, g.recon_slices, g.num_material,
+                                            p->vol_f32.as<float4>(), st));
     p->have_u16 = 1;
     p->have_f32 = 0;
     return VCBCT_OK;
@@ -291,7 +290,7 @@ extern "C" int vcbct_projector_load_deck(vcbct_projector* p, const vcbct_proj_de
     for (cudaEvent_t& e : p->slab_copied)
         if (!e) VCBCT_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     VCBCT_CUDA_TRY(p->stage.ensure(2 * slab * sizeof(uint16_t)));
-    VCBCT_CUDA_TRY(p->vol_u16.ensure(packed_u16_bytes(g.recon_size, g.recon_slices)));
+    VCBCT_CUDA_TRY(p->vol_f32.ensure(packed_f32_bytes(g.recon_size, g.recon_slices)));
     std::vector<uint16_t> zeros(slice, 0);
     const uint16_t* prev = zeros.data();
     int bad = 0;
@@ -320,7 +319,8 @@ extern "C" int vcbct_projector_load_deck(vcbct_projector* p, const vcbct_proj_de
         uint16_t* dev = p->stage.as<uint16_t>() + (size_t)k * slab;
         VCBCT_CUDA_TRY(cudaMemcpyAsync(dev, host, (size_t)nz * slice * sizeof(uint16_t), cudaMemcpyHostToDevice, st));
         VCBCT_CUDA_TRY(cudaEventRecord(p->slab_copied[k], st));
-        VCBCT_CUDA_TRY(launch_pack_u16_slab(dev, g.recon_size, nz, z0, Z, g.num_material, p->vol_u16.as<uint4>(), st));
+        VCBCT_CUDA_TRY(
+            launch_pack_u16_f32_slab(dev, g.recon_size, nz, z0, Z, g.num_material, p->vol_f32.as<float4>(), st));
     }
     VCBCT_CUDA_TRY(cudaStreamSynchronize(st));
     p->have_u16 = 1;
@@ -337,8 +337,8 @@ static int make_fwd_args(vcbct_projector* p, ForwardArgs& a)
     a.p = p->pp;
     a.views = p->views.as<ViewGeom>();
     a.spec = SpectrumDev{p->spec_mu.as<float4>(), p->spec_pdf.as<float>(), p->NE};
-    a.vol_u16 = p->have_u16 ? p->vol_u16.as<uint4>() : nullptr;
-    a.vol_f32 = p->have_f32 ? p->vol_f32.as<float4>() : nullptr;
+    a.vol_u16 = nullptr;
+    a.vol_f32 = p->vol_f32.as<float4>();
     a.err_flag = reinterpret_cast<int*>(p->counter.as<char>() + 8);
     a.cols_per_block = p->cols_per_block;
     a.noise_kind = p->noise_kind;
@@ -506,13 +506,13 @@ static int project_host(vcbct_projector* p, const uint16_t* vol, float* out, cud
     const size_t slice = (size_t)g.recon_size * g.recon_size * g.num_material;
     const size_t nout = (size_t)V * H * W;
     VCBCT_CUDA_TRY(p->stage.ensure(vol_elems(g) * sizeof(uint16_t)));
-    VCBCT_CUDA_TRY(p->vol_u16.ensure(packed_u16_bytes(g.recon_size, Z)));
+    VCBCT_CUDA_TRY(p->vol_f32.ensure(packed_f32_bytes(g.recon_size, Z)));
     VCBCT_CUDA_TRY(p->grad_pk.ensure(nout * sizeof(float)));
     rc = grow_events(p->slab_ready, nslab);
     if (!rc) rc = grow_events(p->slab_copied_ev, nslab);
     if (!rc) rc = grow_events(p->band_done, nb);
     if (rc) return rc;
-    a.vol_u16 = p->vol_u16.as<uint4>();
+    a.vol_f32 = p->vol_f32.as<float4>();
     uint16_t* stage = p->stage.as<uint16_t>();
     float* dout = p->grad_pk.as<float>();
     // downloads per band overlap only into page-locked memory (a copy into
@@ -537,8 +537,8 @@ static int project_host(vcbct_projector* p, const uint16_t* vol, float* out, cud
                                        cudaMemcpyHostToDevice, p->up_stream));
         VCBCT_CUDA_TRY(cudaEventRecord(p->slab_copied_ev[issued], p->up_stream));
         VCBCT_CUDA_TRY(cudaStreamWaitEvent(p->pack_stream, p->slab_copied_ev[issued], 0));
-        VCBCT_CUDA_TRY(launch_pack_u16_slab(dev, g.recon_size, nz, z0, Z, g.num_material, p->vol_u16.as<uint4>(),
-                                            p->pack_stream));
+        VCBCT_CUDA_TRY(launch_pack_u16_f32_slab(dev, g.recon_size, nz, z0, Z, g.num_material,
+                                                p->vol_f32.as<float4>(), p->pack_stream));
         VCBCT_CUDA_TRY(cudaEventRecord(p->slab_ready[issued], p->pack_stream));
         pos[s] = issued++;
         return VCBCT_OK;
@@ -686,7 +686,7 @@ static int projector_adjoint(vcbct_projector* p, const float* d_L, const float* 
                              void* stream)
 {
     if (!p || !d_grad_out || !d_grad) return fail(VCBCT_ERR_ARG, "NULL argument");
-    if (!p->have_f32) return fail(VCBCT_ERR_STATE, "the adjoint needs a float volume (load_volume_f32)");
+    if (!p->have_u16 && !p->have_f32) return fail(VCBCT_ERR_STATE, "no volume loaded");
     if (p->NE <= 0) return fail(VCBCT_ERR_STATE, "no spectrum set");
     cudaStream_t st = (cudaStream_t)stream;
     const auto& g = p->g;
@@ -910,7 +910,7 @@ extern "C" int vcbct_batch_destroy(vcbct_batch* b)
 extern "C" int vcbct_batch_add(vcbct_batch* b, vcbct_projector* p, float* d_out)
 {
     if (!b || !p || !d_out) return fail(VCBCT_ERR_ARG, "NULL argument");
-    if (!p->have_u16) return fail(VCBCT_ERR_STATE, "batched projection needs a uint16 volume");
+    if (!p->have_u16 && !p->have_f32) return fail(VCBCT_ERR_STATE, "no volume loaded");
     if (p->NE <= 0) return fail(VCBCT_ERR_STATE, "no spectrum set");
     b->proj.push_back(p);
     b->outs.push_back(d_out);

@@ -1197,7 +1197,7 @@ __global__ void VCBCT_FWD_BOUNDS flat_batch_kernel(const __grid_constant__ FlatB
     const long long rest = w / b.ncolb[lo];
     const int v = (int)(rest % fa.p.V);
     const int rowt = (int)(rest / fa.p.V);
-    forward_tile<M, false, false>(fa, s_mu, s_pdf, iv_buffer(smem, fa.spec.NE), v, rowt, colb);
+    forward_tile<M, true, false>(fa, s_mu, s_pdf, iv_buffer(smem, fa.spec.NE), v, rowt, colb);
 }
 
 // Persistent batched forward projection: a grid of as many blocks as fit on
@@ -1242,7 +1242,7 @@ __global__ void VCBCT_FWD_BOUNDS persistent_batch_kernel(const __grid_constant__
         const long long rest = w / b.ncolb[lo];
         const int v = (int)(rest % b.fa[lo].p.V);
         const int rowt = (int)(rest / b.fa[lo].p.V);
-        forward_tile<M, false, false>(b.fa[lo], s_mu, s_pdf, s_iv, v, rowt, colb);
+        forward_tile<M, true, false>(b.fa[lo], s_mu, s_pdf, s_iv, v, rowt, colb);
         __syncthreads();
     }
 }
@@ -1357,9 +1357,12 @@ __global__ void __launch_bounds__(256, VCBCT_ADJ_MIN_BLOCKS) adjoint_kernel(Adjo
 // Reference layout [Z][nmat][N][N] -> packed z-fastest records.
 // grid (ceil(N/32), N, ceil(Z/32)), block (32, 8).
 // A slab of nz slices [zoff, zoff + nz) of a Z-slice volume: src holds the
-// slab [nz][nmat][N][N], dst the whole packed volume.
+// slab [nz][nmat][N][N], dst the whole packed volume.  F32REC: the values as
+// floats (exact for uint16) in two 16-byte records per voxel, the layout of
+// pack_f32_kernel; otherwise one 16-byte record of eight uint16.
+template <bool F32REC>
 __global__ void pack_u16_kernel(const uint16_t* __restrict__ src, int N, int nz, int zoff, int Z, int nmat,
-                                uint4* __restrict__ dst)
+                                void* __restrict__ dst)
 {
     __shared__ uint16_t tile[32][8][33];
     const int x0 = blockIdx.x * 32, y = blockIdx.y, z0 = blockIdx.z * 32;
@@ -1377,12 +1380,19 @@ __global__ void pack_u16_kernel(const uint16_t* __restrict__ src, int N, int nz,
         const int x = x0 + xx, z = z0 + threadIdx.x;
         if (x >= N || z >= nz) continue;
         const int zz = threadIdx.x;
-        uint4 r;
-        r.x = (uint32_t)tile[zz][0][xx] | ((uint32_t)tile[zz][1][xx] << 16);
-        r.y = (uint32_t)tile[zz][2][xx] | ((uint32_t)tile[zz][3][xx] << 16);
-        r.z = (uint32_t)tile[zz][4][xx] | ((uint32_t)tile[zz][5][xx] << 16);
-        r.w = (uint32_t)tile[zz][6][xx] | ((uint32_t)tile[zz][7][xx] << 16);
-        dst[((size_t)y * N + x) * Z + zoff + z] = r;
+        const size_t o = ((size_t)y * N + x) * Z + zoff + z;
+        if (F32REC) {
+            float4* p = static_cast<float4*>(dst) + 2 * o;
+            p[0] = make_float4(tile[zz][0][xx], tile[zz][1][xx], tile[zz][2][xx], tile[zz][3][xx]);
+            p[1] = make_float4(tile[zz][4][xx], tile[zz][5][xx], tile[zz][6][xx], tile[zz][7][xx]);
+        } else {
+            uint4 r;
+            r.x = (uint32_t)tile[zz][0][xx] | ((uint32_t)tile[zz][1][xx] << 16);
+            r.y = (uint32_t)tile[zz][2][xx] | ((uint32_t)tile[zz][3][xx] << 16);
+            r.z = (uint32_t)tile[zz][4][xx] | ((uint32_t)tile[zz][5][xx] << 16);
+            r.w = (uint32_t)tile[zz][6][xx] | ((uint32_t)tile[zz][7][xx] << 16);
+            static_cast<uint4*>(dst)[o] = r;
+        }
     }
 }
 
@@ -1444,15 +1454,15 @@ __global__ void unpack_grad_kernel(const float* __restrict__ src, int N, int Z, 
 cudaError_t launch_pack_u16(const uint16_t* src, int N, int Z, int nmat, uint4* dst, cudaStream_t st)
 {
     dim3 grid((N + 31) / 32, N, (Z + 31) / 32), block(32, 8);
-    pack_u16_kernel<<<grid, block, 0, st>>>(src, N, Z, 0, Z, nmat, dst);
+    pack_u16_kernel<false><<<grid, block, 0, st>>>(src, N, Z, 0, Z, nmat, dst);
     return cudaGetLastError();
 }
 
-cudaError_t launch_pack_u16_slab(const uint16_t* src, int N, int nz, int zoff, int Z, int nmat, uint4* dst,
-                                 cudaStream_t st)
+cudaError_t launch_pack_u16_f32_slab(const uint16_t* src, int N, int nz, int zoff, int Z, int nmat, float4* dst,
+                                     cudaStream_t st)
 {
     dim3 grid((N + 31) / 32, N, (nz + 31) / 32), block(32, 8);
-    pack_u16_kernel<<<grid, block, 0, st>>>(src, N, nz, zoff, Z, nmat, dst);
+    pack_u16_kernel<true><<<grid, block, 0, st>>>(src, N, nz, zoff, Z, nmat, dst);
     return cudaGetLastError();
 }
 

@@ -273,7 +273,7 @@ class Batch:
             pass
 
     def add(self, projector: Projector, out=None):
-        """Add a projector (uint16 volume and spectrum loaded); returns its
+        """Add a projector (volume and spectrum loaded); returns its
         device output tensor [V][H][W]."""
         import torch
         g = projector.geom
