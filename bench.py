@@ -853,12 +853,15 @@ def run_ours(args, rank, world, local_rank):
     # measured gather rooflines: the projector's and the backprojector's
     # access patterns replayed without arithmetic on this device
     from measure import probe_gather
-    probe_fwd = probe_gather(0) / 1e9
+    probe_fwd = probe_gather(3) / 1e9
+    probe_fwd_u16 = probe_gather(0) / 1e9
     probe_bp_smem = probe_gather(1) / 1e9
     probe_bp_l1 = probe_gather(2) / 1e9
     gather_roof = {
-        "mbfpa": {"pattern": "ray-front 16-B record gather (11-record runs, stride Z)",
-                  "peak_gseg_s": probe_fwd, "achieved_gseg_s": value, "frac": value / probe_fwd},
+        "mbfpa": {"pattern": "ray-front 32-B float record gather (11-record runs, stride Z), "
+                             "the records the projector reads",
+                  "peak_gseg_s": probe_fwd, "achieved_gseg_s": value, "frac": value / probe_fwd,
+                  "peak_gseg_s_16b_records": probe_fwd_u16, "frac_16b_records": value / probe_fwd_u16},
         "bp": {"pattern": "bilinear detector-tile gather", "peak_gups_shared": probe_bp_smem,
                "peak_gups_l1": probe_bp_l1,
                "achieved_gups": n_eff / (ms_bp * 1e-3) / 1e9,

@@ -29,10 +29,10 @@ def _lib():
 
 
 def probe_gather(kind: int, stream=None) -> float:
-    """Measured gather roofline on the current device: kind 0 = the forward
-    projector's ray-front pattern (lane-records/s); kind 1 / 2 = the
-    backprojector's bilinear pattern from shared memory / through L1 (voxel
-    updates/s)."""
+    """Measured gather roofline on the current device: kind 0 / 3 = the
+    forward projector's ray-front pattern over 16-byte uint16 / 32-byte float
+    records (lane-records/s); kind 1 / 2 = the backprojector's bilinear
+    pattern from shared memory / through L1 (voxel updates/s)."""
     L = _lib()
     r = C.c_double(0.0)
     sp = None if stream is None else C.c_void_p(stream.cuda_stream)

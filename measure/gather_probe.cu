@@ -22,6 +22,8 @@
 //    columns apart, successive slices 3.1 rows apart.  Rate unit: voxel
 //    updates (4 taps) per second.
 //  kind 2, the same BP pattern read from global memory through L1.
+//  kind 3, kind 0 with 32-byte records (8 floats, two 16-byte loads per lane
+//    and step; 1.68 GB): the float records the projector object keeps.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -41,6 +43,8 @@ __device__ __forceinline__ uint32_t hash32(uint32_t x)
     return x;
 }
 
+// HALVES: 16-byte loads per record (1: uint16 records, 2: float records)
+template <int HALVES>
 __global__ void __launch_bounds__(128) ray_front_probe(const uint4* __restrict__ vol, int rounds,
                                                        unsigned* __restrict__ sink)
 {
@@ -52,11 +56,17 @@ __global__ void __launch_bounds__(128) ray_front_probe(const uint4* __restrict__
         const uint32_t h = hash32(warp * 7919u + (uint32_t)r * 104729u);
         const int y = (int)(h % kProbeN);
         const int z0 = (int)((h >> 9) % (kProbeZ - kRun));
-        const uint4* p = vol + (size_t)y * kProbeN * kProbeZ + z0 + off;
+        // record index <= (N - 1) N Z + (Z - 2) + (kSteps - 1) Z < N N Z
+        const uint4* p = vol + ((size_t)y * kProbeN * kProbeZ + z0 + off) * HALVES;
 #pragma unroll 4
         for (int k = 0; k < kSteps; k++) {
-            const uint4 v = __ldg(p + (size_t)k * kProbeZ);
+            const uint4* q = p + (size_t)k * kProbeZ * HALVES;
+            const uint4 v = __ldg(q);
             acc += v.x ^ v.y ^ v.z;
+            if (HALVES == 2) {
+                const uint4 w = __ldg(q + 1);
+                acc += w.x ^ w.y;
+            }
         }
     }
     if (acc == 0x9e3779b9u) sink[0] = acc;  // keeps the loads; never true for zeroed data
@@ -110,14 +120,14 @@ int cuda_err(cudaError_t e, const char* what)
 // Message of the last failure (empty after a success).
 extern "C" const char* gather_probe_error(void) { return g_msg; }
 
-// Rate of probe `kind` (0, 1, 2; units above) on the current device, written
+// Rate of probe `kind` (0 .. 3; units above) on the current device, written
 // to *rate.  Returns 0, 1 for a bad argument, 2 for a CUDA failure.
 // Synchronous on `stream`; allocates and frees its own buffers.
 extern "C" int gather_probe_run(int kind, double* rate, void* stream)
 {
     g_msg[0] = 0;
-    if (!rate || kind < 0 || kind > 2) {
-        std::snprintf(g_msg, sizeof g_msg, "kind must be 0, 1 or 2");
+    if (!rate || kind < 0 || kind > 3) {
+        std::snprintf(g_msg, sizeof g_msg, "kind must be 0, 1, 2 or 3");
         return 1;
     }
     cudaStream_t st = (cudaStream_t)stream;
@@ -136,16 +146,18 @@ extern "C" int gather_probe_run(int kind, double* rate, void* stream)
     cudaError_t err = cudaSuccess;
     double units = 0.0;
     float ms = 0.0f;
-    if (kind == 0) {
-        const size_t bytes = (size_t)kProbeN * kProbeN * kProbeZ * sizeof(uint4);
+    if (kind == 0 || kind == 3) {
+        const int halves = kind == 3 ? 2 : 1;
+        const size_t bytes = (size_t)kProbeN * kProbeN * kProbeZ * sizeof(uint4) * halves;
         err = cudaMalloc(&buf, bytes);
         if (err == cudaSuccess) err = cudaMalloc(&sink, 64);
         if (err == cudaSuccess) err = cudaMemsetAsync(buf, 0, bytes, st);
         const int blocks = sms * 6, rounds = 32;  // 24 warps per SM, as the projector
         if (err == cudaSuccess) {
-            ray_front_probe<<<blocks, 128, 0, st>>>((const uint4*)buf, 1, (unsigned*)sink);
+            auto k = halves == 2 ? ray_front_probe<2> : ray_front_probe<1>;
+            k<<<blocks, 128, 0, st>>>((const uint4*)buf, 1, (unsigned*)sink);
             cudaEventRecord(e0, st);
-            ray_front_probe<<<blocks, 128, 0, st>>>((const uint4*)buf, rounds, (unsigned*)sink);
+            k<<<blocks, 128, 0, st>>>((const uint4*)buf, rounds, (unsigned*)sink);
             cudaEventRecord(e1, st);
             err = cudaEventSynchronize(e1);
         }

@@ -20,7 +20,7 @@ def test_probe_is_not_in_the_product_library():
 def test_probe_library_rejects_bad_kind():
     L = measure._lib()
     r = C.c_double()
-    assert L.gather_probe_run(3, C.byref(r), None) == 1
+    assert L.gather_probe_run(4, C.byref(r), None) == 1
     assert b"kind" in L.gather_probe_error()
     with pytest.raises(RuntimeError):
         measure.probe_gather(-1)
