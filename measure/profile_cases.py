@@ -9,9 +9,9 @@ kernel streams them, so a profiler capture of one to three launches ends in
 seconds:
 
   forward_c1     MBFPA forward, 20 cm water cylinder 512x512x100 x6 uint16,
-                 36 views, 400x400 detector, 90 bins (packed volume 419 MB)
+                 36 views, 400x400 detector, 90 bins (packed volume 839 MB)
   forward_c2     MBFPA forward of the 25 cm / 512x512x200 / 360-view half-fan
-                 workload (packed volume 839 MB; for one-pass launch lists)
+                 workload (packed volume 1.68 GB; for one-pass launch lists)
   filter_bf16x3  FDK ramp filter, BF16x3 tcgen05 GEMM, 360 views of 400x400
   filter_direct  FDK ramp filter, direct FP32 kernel, same projections
   backproject    FDK backprojection of 360 filtered 400x400 views to 270x270x200

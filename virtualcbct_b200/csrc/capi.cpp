@@ -74,6 +74,9 @@ using namespace vcbct;
 // Host-bound projections are computed in this many view chunks, each
 // downloaded while the next is computed.
 constexpr int kForwardChunks = 8;
+// view chunks of the last row band of a host-to-host projection
+constexpr int kTailChunks = 4;
+static_assert(kTailChunks <= kForwardChunks, "the tail chunks use the chunk events");
 
 struct vcbct_projector {
     vcbct_proj_geometry g;
@@ -543,14 +546,17 @@ static int project_host(vcbct_projector* p, const uint16_t* vol, float* out, cud
         pos[s] = issued++;
         return VCBCT_OK;
     };
-    auto download = [&](int b) -> int {
+    // band b's rows of views [v0, v1), once `done` has been reached
+    auto download_views = [&](int b, int v0, int v1, cudaEvent_t done) -> int {
         const int j1 = std::min(H, 32 * b + 32), r0 = H - j1, nr = j1 - 32 * b;  // rows H-1-j
         const size_t pitch = (size_t)H * W * sizeof(float);
-        VCBCT_CUDA_TRY(cudaStreamWaitEvent(p->copy_stream, p->band_done[b], 0));
-        VCBCT_CUDA_TRY(cudaMemcpy2DAsync(out + (size_t)r0 * W, pitch, dout + (size_t)r0 * W, pitch,
-                                         (size_t)nr * W * sizeof(float), V, cudaMemcpyDeviceToHost, p->copy_stream));
+        const size_t o = (size_t)v0 * H * W + (size_t)r0 * W;
+        VCBCT_CUDA_TRY(cudaStreamWaitEvent(p->copy_stream, done, 0));
+        VCBCT_CUDA_TRY(cudaMemcpy2DAsync(out + o, pitch, dout + o, pitch, (size_t)nr * W * sizeof(float), v1 - v0,
+                                         cudaMemcpyDeviceToHost, p->copy_stream));
         return VCBCT_OK;
     };
+    auto download = [&](int b) -> int { return download_views(b, 0, V, p->band_done[b]); };
     std::vector<char> done(nb, 0);
     std::vector<int> order;
     for (int step = 0; step < nb; step++) {
@@ -577,18 +583,29 @@ static int project_host(vcbct_projector* p, const uint16_t* vol, float* out, cud
                 wait = std::max(wait, pos[s]);
             }
         }
-        const cudaStream_t bs = cs[step & 1];
-        if (wait >= 0) VCBCT_CUDA_TRY(cudaStreamWaitEvent(bs, p->slab_ready[wait], 0));
-        ForwardArgs ab = a;
-        ab.out = dout;
-        ab.band0 = best;
-        ab.nbands = 1;
-        VCBCT_CUDA_TRY(launch_forward(ab, bs));
-        VCBCT_CUDA_TRY(cudaEventRecord(p->band_done[best], bs));
         order.push_back(best);
-        if (out_locked) {
-            rc = download(best);
-            if (rc) return rc;
+        // The last band goes in view chunks on alternating streams, each
+        // downloaded as soon as it is done: only the last chunk's rows are
+        // left to copy after the last launch.
+        const int nch = (step == nb - 1 && out_locked) ? std::min(kTailChunks, V) : 1;
+        for (int c = 0; c < nch; c++) {
+            const cudaStream_t bs = cs[(step + c) & 1];
+            if (wait >= 0) VCBCT_CUDA_TRY(cudaStreamWaitEvent(bs, p->slab_ready[wait], 0));
+            const int v0 = (int)((long long)V * c / nch), v1 = (int)((long long)V * (c + 1) / nch);
+            ForwardArgs ab = a;
+            ab.views = a.views + v0;
+            ab.view_offset = v0;
+            ab.p.V = v1 - v0;
+            ab.out = dout + (size_t)v0 * H * W;
+            ab.band0 = best;
+            ab.nbands = 1;
+            VCBCT_CUDA_TRY(launch_forward(ab, bs));
+            cudaEvent_t done = nch == 1 ? p->band_done[best] : p->chunk_done[c];
+            VCBCT_CUDA_TRY(cudaEventRecord(done, bs));
+            if (out_locked) {
+                rc = download_views(best, v0, v1, done);
+                if (rc) return rc;
+            }
         }
     }
     for (int s = 0; s < nslab; s++)  // slices no band reads still form the loaded volume
