@@ -20,6 +20,7 @@ CASES = [
     ("random", dict(seed=2, z_reg=1.7, H=70, Z=21)),            # off-centre source, ragged bands/slabs
     ("water", dict(N=128, Z=40, s=0.1, W=96, H=100, V=12, xshift=3.0)),
     ("random", dict(seed=4, N=96, Z=64, s=0.15, step=0.12, W=64, H=130, V=6, dpn=900.0)),  # steep cone
+    ("random", dict(seed=6, H=33, V=3)),                        # fewer views than the last band's chunks
 ]
 
 
@@ -54,7 +55,11 @@ def test_project_equals_load_and_forward(cuda, kind, kw, pinned):
     assert np.array_equal(again, ref)
 
 
-def test_project_twice_and_with_noise(cuda):
+@pytest.mark.parametrize("pinned", [True, False])
+def test_project_twice_and_with_noise(cuda, pinned):
+    """Noise counters follow the global view index, also in the last band's
+    view chunks (page-locked output)."""
+    import torch
     g, tabs, vol, _ = proj_case("random", seed=5, N=96, Z=30, W=64, H=72, V=8)
     vol2 = phantoms.random_volume(96, 30, seed=6, hi=500)
     mu, pdf = spectrum()
@@ -66,7 +71,8 @@ def test_project_twice_and_with_noise(cuda):
         p.load_volume(v)
         ref = np.empty((g.V, g.H, g.W), np.float32)
         p.forward(ref)
-        out = p.project(v)
+        out = torch.empty((g.V, g.H, g.W), dtype=torch.float32).pin_memory().numpy() if pinned else None
+        out = p.project(v, out)
         assert np.array_equal(out, ref)
         outs.append(out)
     assert np.array_equal(outs[0], outs[2]) and not np.array_equal(outs[0], outs[1])
