@@ -1396,6 +1396,28 @@ __global__ void pack_u16_kernel(const uint16_t* __restrict__ src, int N, int nz,
     }
 }
 
+// A thin slab (nz <= 8 slices) of uint16 -> float records: thread t of a
+// 256-thread block makes record (y, x0 + t / 8, zoff + t % 8), so a warp
+// writes four runs of 8 consecutive records (256 bytes each) and every lane
+// has work; the tiled kernel above gives a slab of 8 slices a quarter of its
+// lanes.  Reads go straight to global memory (the block's 32 x 8 values of
+// an element row share their sectors in L1).  grid (ceil(N/32), N).
+__global__ void __launch_bounds__(256) pack_u16_f32_thin_kernel(const uint16_t* __restrict__ src, int N, int nz,
+                                                                int zoff, int Z, int nmat, float4* __restrict__ dst)
+{
+    const int t = threadIdx.x;
+    const int z = t & 7, x = blockIdx.x * 32 + (t >> 3), y = blockIdx.y;
+    if (z >= nz || x >= N) return;
+    const size_t NN = (size_t)N * N;
+    const uint16_t* s = src + (size_t)z * nmat * NN + (size_t)y * N + x;
+    float e[8];
+#pragma unroll
+    for (int m = 0; m < 8; m++) e[m] = m < nmat ? (float)__ldg(s + (size_t)m * NN) : 0.0f;
+    float4* p = dst + 2 * (((size_t)y * N + x) * Z + zoff + z);
+    p[0] = make_float4(e[0], e[1], e[2], e[3]);
+    p[1] = make_float4(e[4], e[5], e[6], e[7]);
+}
+
 __global__ void pack_f32_kernel(const float* __restrict__ src, int N, int Z, int nmat,
                                 float4* __restrict__ dst)
 {
@@ -1461,6 +1483,10 @@ cudaError_t launch_pack_u16(const uint16_t* src, int N, int Z, int nmat, uint4* 
 cudaError_t launch_pack_u16_f32_slab(const uint16_t* src, int N, int nz, int zoff, int Z, int nmat, float4* dst,
                                      cudaStream_t st)
 {
+    if (nz <= 8) {
+        pack_u16_f32_thin_kernel<<<dim3((N + 31) / 32, N), 256, 0, st>>>(src, N, nz, zoff, Z, nmat, dst);
+        return cudaGetLastError();
+    }
     dim3 grid((N + 31) / 32, N, (nz + 31) / 32), block(32, 8);
     pack_u16_kernel<true><<<grid, block, 0, st>>>(src, N, nz, zoff, Z, nmat, dst);
     return cudaGetLastError();
