@@ -486,21 +486,23 @@ struct PairSums {
     }
 };
 
-// The same with L in shared memory (this thread's column of a [M][kLStride]
-// array): L is touched once per 32 steps, and its registers are free for the
-// walk and the interval production.
-constexpr int kLStride = 256;
+// The same with L in shared memory (this thread's column of an [M][threads
+// of the block] array): L is touched once per 32 steps, and its registers are
+// free for the walk and the interval production.  Sized by the block (not by
+// the largest block) so that the shared memory the resident blocks leave to
+// L1 is as large as it can be.
+__device__ __forceinline__ int ls_stride() { return (int)(blockDim.x * blockDim.y); }
 template <int M>
 struct PairSumsS {
     static constexpr int NP = (M + 1) / 2;
     float* Ls;
     f32x2 P2[NP];
     float lt = 1.0f;
-    __device__ __forceinline__ float Lget(int i) const { return Ls[i * kLStride]; }
+    __device__ __forceinline__ float Lget(int i) const { return Ls[i * ls_stride()]; }
     __device__ __forceinline__ void clear()
     {
 #pragma unroll
-        for (int i = 0; i < M; i++) Ls[i * kLStride] = 0.0f;
+        for (int i = 0; i < M; i++) Ls[i * ls_stride()] = 0.0f;
 #pragma unroll
         for (int i = 0; i < NP; i++) P2[i] = 0ull;
     }
@@ -510,15 +512,15 @@ struct PairSumsS {
         for (int i = 0; i < NP; i++) {
             float a, b;
             f2unpack(P2[i], a, b);
-            Ls[2 * i * kLStride] = fmaf(a, lt, Ls[2 * i * kLStride]);
-            if (2 * i + 1 < M) Ls[(2 * i + 1) * kLStride] = fmaf(b, lt, Ls[(2 * i + 1) * kLStride]);
+            Ls[2 * i * ls_stride()] = fmaf(a, lt, Ls[2 * i * ls_stride()]);
+            if (2 * i + 1 < M) Ls[(2 * i + 1) * ls_stride()] = fmaf(b, lt, Ls[(2 * i + 1) * ls_stride()]);
             P2[i] = 0ull;
         }
     }
     __device__ __forceinline__ void zero_L()
     {
 #pragma unroll
-        for (int i = 0; i < M; i++) Ls[i * kLStride] = 0.0f;
+        for (int i = 0; i < M; i++) Ls[i * ls_stride()] = 0.0f;
     }
 };
 
@@ -555,7 +557,7 @@ struct AccumU16 : PairSumsS<M> {
         for (int i = 0; i < M; i++) {
             float a, b;
             f2unpack(u16pair(w[i / 2]), a, b);
-            this->Ls[i * kLStride] = fmaf((i & 1) ? b : a, len, this->Ls[i * kLStride]);
+            this->Ls[i * ls_stride()] = fmaf((i & 1) ? b : a, len, this->Ls[i * ls_stride()]);
         }
         nseg++;
     }
@@ -592,7 +594,7 @@ struct AccumF32 : std::conditional_t<SL, PairSumsS<M>, PairSums<M>> {
         const float* p = reinterpret_cast<const float*>(vol + 2 * (size_t)idx);
 #pragma unroll
         for (int i = 0; i < M; i++) {
-            if constexpr (SL) this->Ls[i * kLStride] = fmaf(__ldg(p + i), len, this->Ls[i * kLStride]);
+            if constexpr (SL) this->Ls[i * ls_stride()] = fmaf(__ldg(p + i), len, this->Ls[i * ls_stride()]);
             else this->L[i] = fmaf(__ldg(p + i), len, this->L[i]);
         }
         nseg++;
@@ -1513,7 +1515,7 @@ static cudaError_t launch_fwd_t(const ForwardArgs& a, cudaStream_t st)
     dim3 block(32, cpb);
     dim3 grid((a.p.W + cpb - 1) / cpb, a.p.V, a.nbands > 0 ? a.nbands : (a.p.H + 31) / 32);
     size_t shm = ((size_t)2 * a.spec.NE + (a.spec.NE + 3) / 4) * sizeof(float4) +
-                 (size_t)cpb * kIvSlots * sizeof(IvRec) + (size_t)M * kLStride * sizeof(float);
+                 (size_t)cpb * kIvSlots * sizeof(IvRec) + (size_t)M * 32 * cpb * sizeof(float);
     auto k = forward_kernel<M, F32VOL, COUNT>;
     if (shm > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
@@ -1529,7 +1531,7 @@ cudaError_t launch_persistent_batch(const FlatBatch& b, int NEmax, int nmat_max,
     if (b.begin[b.nitems] <= 0) return cudaSuccess;
     dim3 block(32, cols_per_block);
     size_t shm = ((size_t)2 * NEmax + (NEmax + 3) / 4) * sizeof(float4) +
-                 (size_t)cols_per_block * kIvSlots * sizeof(IvRec) + (size_t)8 * kLStride * sizeof(float);
+                 (size_t)cols_per_block * kIvSlots * sizeof(IvRec) + (size_t)8 * 32 * cols_per_block * sizeof(float);
     // (the shared-memory attribute is set by batch_blocks_per_sm, before any
     // stream capture)
     cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st);
@@ -1546,7 +1548,7 @@ cudaError_t launch_flat_batch(const FlatBatch& b, int NEmax, int nmat_max, int c
     if (total > 0x7fffffffLL) return cudaErrorInvalidValue;
     dim3 block(32, cols_per_block);
     size_t shm = ((size_t)2 * NEmax + (NEmax + 3) / 4) * sizeof(float4) +
-                 (size_t)cols_per_block * kIvSlots * sizeof(IvRec) + (size_t)8 * kLStride * sizeof(float);
+                 (size_t)cols_per_block * kIvSlots * sizeof(IvRec) + (size_t)8 * 32 * cols_per_block * sizeof(float);
     auto k = (nmat_max <= 6) ? flat_batch_kernel<6> : flat_batch_kernel<8>;
     // (the shared-memory attribute is set by batch_blocks_per_sm, before any
     // stream capture)
@@ -1557,7 +1559,7 @@ cudaError_t launch_flat_batch(const FlatBatch& b, int NEmax, int nmat_max, int c
 int batch_blocks_per_sm(int nmat_max, int cols_per_block, int NEmax)
 {
     size_t shm = ((size_t)2 * NEmax + (NEmax + 3) / 4) * sizeof(float4) +
-                 (size_t)cols_per_block * kIvSlots * sizeof(IvRec) + (size_t)8 * kLStride * sizeof(float);
+                 (size_t)cols_per_block * kIvSlots * sizeof(IvRec) + (size_t)8 * 32 * cols_per_block * sizeof(float);
     int n = 0;
     auto k = (nmat_max <= 6) ? persistent_batch_kernel<6> : persistent_batch_kernel<8>;
     if (shm > 48 * 1024 && cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm) != cudaSuccess)
